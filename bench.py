@@ -1,0 +1,314 @@
+"""Benchmark of the Louvain hot path: edges/s per Louvain pass.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload lfr|sbm10k|rmat<scale>]
+                    [--impl ours|reference]
+
+Workload (default): the LFR-style graph n = 2^20 (power-law degrees, exponent
+2.5 on [5, 5000]; community sizes exponent 1.5 on [50, 50000]; mu = 0.3; unit
+weights; seed 1) -- synthetic, seeded, generated on the host.
+
+One step (value) = the level-0 one-level phase (all move passes from the
+singleton state, ΔQ test, commit and isolated-vertex merge) on the
+device-resident CSR.  value = CSR entries x passes / step time.
+e2e = one whole dendrogram run through the C ABI from pinned host buffers:
+H2D of the edge list, CSR build, every level, final FP64 modularity and D2H of
+the partition; e2e value = sum over levels of CSR entries x passes / run time.
+
+With --gpus N each rank runs an independent replica (the path does not shard
+within one graph); value is the sum over ranks of entries processed divided by
+the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edges/s per Louvain pass"
+UNIT = "edges/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="lfr")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_graph(workload):
+    from louvaingpu_b200 import graphgen
+    if workload == "lfr":
+        n, s, d, w = graphgen.lfr()
+        desc = dict(workload="LFR-style power-law graph", n_vertices=n, degree_exp=2.5, degree_range=[5, 5000],
+                    community_exp=1.5, community_range=[50, 50000], mu=0.3, weights="unit", seed=1)
+        return n, s, d, w, desc, 1e-7
+    if workload == "sbm10k":
+        n, s, d, w = graphgen.sbm_10k(seed=0)
+        desc = dict(workload="planted-partition SBM", n_vertices=n, blocks=100, p_in=0.1, p_out=0.0006,
+                    weights="unit", seed=0, level_min_gain=1e-6)
+        return n, s, d, w, desc, 1e-6
+    if workload.startswith("rmat"):
+        scale = int(workload[4:])
+        n, s, d, w = graphgen.rmat(scale)
+        desc = dict(workload=f"R-MAT scale {scale}", n_vertices=n, edge_factor=16, abcd=[0.57, 0.19, 0.19, 0.05],
+                    weights="integer 1..16", seed=2)
+        return n, s, d, w, desc, 1e-7
+    raise SystemExit(f"unknown workload {workload}")
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(workload):
+    """DRAM bytes per move pass from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "move_pass_traffic.json")
+    try:
+        with open(p) as f:
+            j = json.load(f)
+        return j.get(workload)
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(n, s, d, w, level_min, threads):
+    from oracle import oracle as O
+    r = O.Run(n, s, d, w, level_min_gain=level_min, n_threads=threads)
+    return r.pass_entries / r.seconds, r.seconds
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def run_reference(args, world, rank, pg):
+    """Reference arm: the CPU restatement of the reference's method on all host cores."""
+    if rank != 0:
+        return
+    n, s, d, w, desc, level_min = make_graph(args.workload)
+    threads = os.cpu_count() or 1
+    from oracle import oracle as O
+    for _ in range(args.warmup):
+        O.Run(n, s, d, w, level_min_gain=level_min, n_threads=threads)
+    t0 = time.perf_counter()
+    entries = 0
+    for _ in range(args.steps):
+        r = O.Run(n, s, d, w, level_min_gain=level_min, n_threads=threads)
+        entries += r.pass_entries
+    t = time.perf_counter() - t0
+    v = entries / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+        "config": dict(desc, parallelism="replicas", step="whole dendrogram run"),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} whole runs of the workload (CPU restatement of the reference "
+                                   f"method; the reference's own GPU code cannot be built here)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+    from louvaingpu_b200 import Louvain, kernel_launches
+    torch.cuda.set_device(local)
+    n, s, d, w, desc, level_min = make_graph(args.workload)
+    E = len(s)
+    stream = torch.cuda.current_stream()
+    # ---------------------------------------------------------------- value
+    ds = torch.from_numpy(s).cuda()
+    dd = torch.from_numpy(d).cuda()
+    dw = torch.from_numpy(w).cuda()
+    lv = Louvain(device=local, level_min_gain=level_min)
+    lv.set_stream(stream.cuda_stream)
+    lv.load_edges_device(ds.data_ptr(), dd.data_ptr(), dw.data_ptr(), E, n)
+    V, nnz, m = lv.csr_shape()
+    q0 = lv.modularity()
+    for _ in range(args.warmup):
+        lv.one_level(q0)
+    clocks = Clocks(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    passes_total, move_ms, move_passes = 0, 0.0, 0
+    for _ in range(args.steps):
+        q, p = lv.one_level(q0)
+        passes_total += p
+        ms, mp = lv.move_stats()
+        move_ms += ms
+        move_passes += mp
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = kernel_launches() - l0
+    clk = clocks.stop()
+    t_ms = e0.elapsed_time(e1)
+    if pg:
+        tt = torch.tensor([t_ms], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    entries = nnz * passes_total
+    value = entries * world / (t_ms / 1e3)
+    # roofline of the move kernels: B_pass = 12 nnz + 24 V bytes per pass
+    peak, peak_kind = measured_peak()
+    b_pass = 12.0 * nnz + 24.0 * V
+    t_move = move_ms / max(move_passes, 1) / 1e3
+    achieved = b_pass / t_move / 1e9 if t_move > 0 else 0.0
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_kind, "traffic": profiled_traffic(args.workload),
+            "kernel": "move kernels of one pass (all degree buckets)", "algorithmic_bytes": b_pass,
+            "move_ms_per_pass": t_move * 1e3}
+    del lv
+    # ---------------------------------------------------------------- e2e
+    hs = torch.from_numpy(s).pin_memory()
+    hd = torch.from_numpy(d).pin_memory()
+    hw = torch.from_numpy(w).pin_memory()
+    lv2 = Louvain(device=local, level_min_gain=level_min)
+    lv2.set_stream(stream.cuda_stream)
+    part = torch.empty(n, dtype=torch.int32).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        lv2.load_edges_ptr(hs.data_ptr(), hd.data_ptr(), hw.data_ptr(), E, n)
+        lv2.run()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    pe = 0
+    qf = None
+    for _ in range(args.steps):
+        lv2.load_edges_ptr(hs.data_ptr(), hd.data_ptr(), hw.data_ptr(), E, n)
+        res = lv2.run()
+        out = lv2.partition()
+        pe += res.pass_entries
+        qf = res.q_final
+    f1.record(stream)
+    torch.cuda.synchronize()
+    t2 = f0.elapsed_time(f1)
+    if pg:
+        tt = torch.tensor([t2], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t2 = float(tt.item())
+    e2e_value = pe * world / (t2 / 1e3)
+    levels = [lv2.level_info(l) for l in range(lv2.n_levels)]
+    del lv2
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, secs = cpu_baseline(n, s, d, w, level_min, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"one whole dendrogram run of the workload ({secs:.1f} s)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+        "config": dict(desc, n_entries=E, csr_entries=nnz, parallelism="replicas" if world > 1 else "single",
+                       step="level-0 one-level phase", passes_per_step=passes_total // args.steps,
+                       l2="inputs larger than L2 (move pass touches %.0f MB)" % (b_pass / 1e6)),
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 12 * E, "d2h_bytes_per_step": 4 * n,
+                "ms_per_run": t2 / args.steps, "q_final": qf, "levels": len(levels)},
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank, pg)
+        else:
+            run_ours(args, world, rank, local, pg)
+    finally:
+        if pg:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,180 @@
+/*
+ * lvg.h -- C ABI of liblvg, the B200 (sm_100a) Louvain hot path.
+ *
+ * Each entry point replaces one function of the reference's GPU phase API,
+ * the six `extern` functions its level driver links against
+ * (LouvainCUDA/LouvainCPP.cpp:129-134), or a driver-side step of
+ * generate_dendogram (LouvainCPP.cpp:209-553).  The reference file:line each
+ * one replaces is given beside it.
+ *
+ * Conventions
+ *  - Vertices are dense indices 0..n_vertices-1 (the reference's CUDPP
+ *    id->index hash, InitKernel.cu:276-306, becomes the caller's dense ids).
+ *  - An edge list is SoA (src, dst, w) of n_entries entries, exactly what the
+ *    reference copies to the device (LouvainCPP.cpp:283-287).  Both directions
+ *    of an undirected edge are listed by the caller; the library appends the
+ *    reversed copy of every entry as the reference does (NeighbourCompute.cu:66-68).
+ *  - Weights are finite and >= 0.
+ *  - Every function returns lvg_status; nothing throws across the ABI.  On
+ *    error lvg_last_error(ctx) describes the failure.
+ *  - A context owns one CUDA stream (or the one given by lvg_set_stream), its
+ *    device arena and all device state.  Contexts are independent; one
+ *    context must not be used by two host threads at once.
+ *  - Host pointers are only read during the call (inputs) or written before
+ *    it returns (outputs).  Device pointers passed to lvg_load_edges_device
+ *    must stay valid until the next load or lvg_destroy.
+ */
+#ifndef LVG_H
+#define LVG_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  LVG_OK = 0,
+  LVG_ERR_INVALID_ARG = 1, /* bad pointer, size, id out of range, negative/non-finite weight */
+  LVG_ERR_OOM = 2,         /* device arena or cudaMalloc exhausted */
+  LVG_ERR_CAPACITY = 3,    /* a size limit of this build was exceeded */
+  LVG_ERR_NOT_CONVERGED = 4, /* pass or level cap reached before the gain threshold */
+  LVG_ERR_CUDA = 5,        /* CUDA runtime error */
+  LVG_ERR_STATE = 6        /* call out of order (e.g. one_level before load) */
+} lvg_status;
+
+typedef struct lvg_ctx lvg_ctx;
+
+typedef struct {
+  int32_t device;          /* CUDA device ordinal (reference: cudaSetDevice(0), LouvainCPP.cpp:774) */
+  double pass_min_gain;    /* stop a level when Q gains less (reference __MIN = 1e-7, OneLevelKernel.cu:425) */
+  double level_min_gain;   /* stop the run when a level gains less (LouvainCPP.cpp:55,466) */
+  int32_t max_passes;      /* <0: unbounded like __PASS_MAX=-1 (OneLevelKernel.cu:424) */
+  int32_t max_levels;      /* <0: unbounded */
+  int64_t arena_bytes;     /* 0: sized from the level-0 graph at load */
+  int32_t warp_max_degree; /* vertices up to this degree use a warp-per-vertex table (0: default) */
+  int32_t block_max_degree;/* up to this degree a block-per-vertex shared table; above, global tables */
+  int32_t passes_per_sync; /* passes launched between host checks of convergence (0: default) */
+  int32_t use_graphs;      /* capture the pass sequence of a level in a CUDA graph (1: default on) */
+} lvg_config;
+
+/* Per-level record of a run (the reference keeps one Partition per level,
+ * LouvainCPP.cpp:384,464). */
+typedef struct {
+  int32_t n_vertices;      /* vertices of the level graph */
+  int64_t n_entries;       /* entries of the level input list */
+  int64_t nnz;             /* merged CSR entries (doubled list, loops removed) */
+  int32_t n_comms;         /* communities after the level (next level's vertices) */
+  int32_t passes;          /* move passes, including the last (breaking) one */
+  double q_start;          /* Q of the singleton state of the level */
+  double q_level;          /* Q returned by the one-level phase (oneLevelCUDA's return value) */
+  double ms_build, ms_passes, ms_renumber, ms_induce; /* device time of each phase */
+} lvg_level_info;
+
+typedef struct {
+  int32_t n_levels;
+  int32_t n_comms;         /* communities of the final partition */
+  double q_final;          /* FP64 Newman modularity of the final partition on the level-0 graph */
+  int64_t pass_entries;    /* sum over levels of nnz * passes (edges processed by move passes) */
+  int32_t status;          /* LVG_OK or LVG_ERR_NOT_CONVERGED */
+} lvg_result;
+
+/* Defaults: pass/level gain 1e-7 (the reference's), unbounded caps. */
+lvg_status lvg_config_default(lvg_config* cfg);
+
+lvg_status lvg_create(const lvg_config* cfg, lvg_ctx** out);
+lvg_status lvg_destroy(lvg_ctx* ctx);
+const char* lvg_last_error(const lvg_ctx* ctx);
+const char* lvg_status_string(lvg_status s);
+/* Run all work of this context on `stream` (a cudaStream_t); NULL restores the
+ * context's own stream. */
+lvg_status lvg_set_stream(lvg_ctx* ctx, void* stream);
+
+/* Load the level-0 edge list from HOST memory and build the level CSR, degrees
+ * and self-loop weights.  Replaces the driver's H2D copies
+ * (LouvainCPP.cpp:283-287) followed by CalculateNeighbour (NeighbourCompute.cu:42)
+ * and initCUDA (InitKernel.cu:245). */
+lvg_status lvg_load_edges(lvg_ctx* ctx, const int32_t* src, const int32_t* dst, const float* w,
+                          int64_t n_entries, int32_t n_vertices);
+/* As lvg_load_edges, with the edge list already in device memory. */
+lvg_status lvg_load_edges_device(lvg_ctx* ctx, const int32_t* d_src, const int32_t* d_dst,
+                                 const float* d_w, int64_t n_entries, int32_t n_vertices);
+
+/* Q of the current level's committed community state.
+ * Replaces modularityCUDA (OneLevelKernel.cu:965-980). */
+lvg_status lvg_modularity(lvg_ctx* ctx, double* q);
+
+/* Run the move passes of the current level until the Q gain falls below
+ * pass_min_gain, then the isolated-vertex merge.  `lower` is the floor of the
+ * running Q (the `lower` argument of the reference).  Replaces oneLevelCUDA
+ * (OneLevelKernel.cu:518-954). */
+lvg_status lvg_one_level(lvg_ctx* ctx, double lower, double* q, int32_t* passes);
+
+/* Number the current level's communities 0..C-1 in order of their smallest
+ * member vertex.  comm_out (host, nullable) receives n_vertices entries.
+ * Replaces renumberCUDA (RenumberKernel.cu:63-221). */
+lvg_status lvg_renumber(lvg_ctx* ctx, int32_t* comm_out, int32_t* n_comms);
+
+/* Coarsen: the level input list mapped through the renumbered partition,
+ * weight 0 -> 1, equal (cu,cv) keys summed, becomes the next level's input
+ * list; its CSR is built.  Replaces inducedGraphCUDA (InducedGraphKernel.cu:50-113)
+ * and the CalculateNeighbour/initCUDA calls of the next level. */
+lvg_status lvg_induce(lvg_ctx* ctx);
+
+/* Whole dendrogram from the loaded graph.  Replaces generate_dendogram
+ * (LouvainCPP.cpp:209-553). */
+lvg_status lvg_run(lvg_ctx* ctx, lvg_result* res);
+
+/* Results of the last lvg_run / step sequence. */
+lvg_status lvg_num_levels(const lvg_ctx* ctx, int32_t* n_levels);
+lvg_status lvg_get_level_info(const lvg_ctx* ctx, int32_t level, lvg_level_info* info);
+/* Renumbered partition of the level's vertices (the Partition pushed per level,
+ * RenumberKernel.cu:202-203), as a dense array of that level's size. */
+lvg_status lvg_get_level_partition(const lvg_ctx* ctx, int32_t level, int32_t* part);
+/* Community ids of the level before renumbering (vertex-index labels). */
+lvg_status lvg_get_level_labels(const lvg_ctx* ctx, int32_t level, int32_t* labels);
+/* Partition of the level-0 vertices composed through levels 0..level.
+ * Replaces partitionAtLevel (LouvainCPP.cpp:82-106). */
+lvg_status lvg_get_partition(const lvg_ctx* ctx, int32_t level, int32_t* part);
+/* 1 + max community id of a composed partition.  Replaces countPartitions
+ * (LouvainCPP.cpp:116-127). */
+lvg_status lvg_count_partitions(const int32_t* part, int64_t n, int32_t* count);
+
+/* FP64 Newman modularity of a partition (host array over the level-0
+ * vertices) on the loaded level-0 graph, computed on the device. */
+lvg_status lvg_modularity_fp64(lvg_ctx* ctx, const int32_t* part, double* q);
+
+/* Copy the current level's CSR and per-vertex values to host buffers (any may
+ * be NULL): off[V+1], col[nnz], w[nnz], degree k[V], loop weight[V], has_loop[V]. */
+lvg_status lvg_get_csr(const lvg_ctx* ctx, int32_t* n_vertices, int64_t* nnz, double* m,
+                       int64_t* off, int32_t* col, float* w, double* k, float* loopw,
+                       uint8_t* has_loop);
+
+/* Set the committed community state of the current level from host arrays
+ * (communities as vertex indices) and recompute its totals; used to drive
+ * single passes from a known state. */
+lvg_status lvg_set_communities(lvg_ctx* ctx, const int32_t* comm);
+/* One synchronous decision pass from the committed state, without commit:
+ * next[V] chosen community, cand[V] isolated-merge candidate (-1 none).
+ * The state is left unchanged.  Restates one launch of the move kernels
+ * (SetNewCommunityWarpShuffle + oneLevelKernel, OneLevelKernel.cu:248-422). */
+lvg_status lvg_move_decide(lvg_ctx* ctx, int32_t* next, int32_t* cand);
+
+/* Device-time (ms) of the move passes of the last lvg_one_level, and the
+ * per-pass breakdown when `ms` is non-NULL (cap entries). */
+lvg_status lvg_last_pass_times(const lvg_ctx* ctx, float* ms, int32_t cap, int32_t* n_passes);
+
+/* Device time of the move kernels (all degree buckets of a pass, the hot
+ * path's dominant work) summed over the passes of the last lvg_one_level /
+ * lvg_run, and the number of passes it covers. */
+lvg_status lvg_move_stats(const lvg_ctx* ctx, double* ms_total, int64_t* n_passes);
+
+/* Number of CUDA kernels this library has launched in this process. */
+lvg_status lvg_kernel_launches(int64_t* n);
+
+/* Bytes of device memory the context holds (arena capacity) and its peak use. */
+lvg_status lvg_memory(const lvg_ctx* ctx, int64_t* capacity, int64_t* peak);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,9 @@
+"""B200-native (sm_100a) Louvain hot path of LouvainGPU behind its phase API.
+
+The compute runs in liblvg.so (hand-written CUDA for sm_100a, C ABI in
+include/lvg.h); this package is the Python side of that ABI.
+"""
+from .louvain import Louvain, LevelInfo, RunResult, count_partitions, kernel_launches  # noqa: F401
+from ._lib import LvgError  # noqa: F401
+
+__all__ = ["Louvain", "LevelInfo", "RunResult", "count_partitions", "kernel_launches", "LvgError"]

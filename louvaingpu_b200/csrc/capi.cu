@@ -1,0 +1,687 @@
+// Context, level driver and the extern "C" entry points of liblvg.
+//
+// The level loop restates generate_dendogram (LouvainCPP.cpp:209-553):
+// level 0 runs CSR build -> Q of the singleton state -> one-level -> renumber ->
+// induce; every further level runs CSR build -> one-level -> renumber, stops
+// when the level's Q gain is below level_min_gain (LouvainCPP.cpp:466), else
+// induces the next level.  Unlike the reference, the level input lists stay on
+// the device between levels (no host round trip, LouvainCPP.cpp:390-412,477-499).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "louvain.cuh"
+#include "prims.cuh"
+
+using namespace lvg;
+
+namespace lvg {
+static std::atomic<int64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace lvg
+
+namespace {
+
+struct LevelRec {
+  lvg_level_info info;
+  int32_t* d_part = nullptr;    // renumbered partition (arena high end, run lifetime)
+  int32_t* d_labels = nullptr;  // community labels before renumbering
+};
+
+}  // namespace
+
+struct lvg_ctx {
+  lvg_config cfg;
+  Tuning tune;
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  Arena arena;
+  std::string err;
+  // level-0 graph
+  bool loaded = false;
+  int32_t V0 = 0;
+  int64_t E0 = 0;
+  const int32_t* src0 = nullptr;
+  const int32_t* dst0 = nullptr;
+  const float* w0 = nullptr;
+  int32_t* composed = nullptr;   // partition of the level-0 vertices through the last renumbered level
+  size_t base_lo = 0;            // arena low mark above the level-0 list and `composed`
+  size_t run_hi = 0;             // arena high mark above the per-level partitions
+  // current level
+  int level = 0;
+  LevelGraph g;
+  CommState st;
+  bool have_state = false;
+  bool renumbered = false;
+  int32_t* d_part_cur = nullptr;
+  int32_t C_cur = 0;
+  std::vector<LevelRec> levels;
+  std::vector<float> pass_ms;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> mev;   // move-phase events, two per pass
+  double move_ms = 0.0;
+  int64_t move_passes = 0;
+};
+
+namespace {
+
+lvg_status fail(lvg_ctx* c, lvg_status s, const std::string& m) {
+  if (c) c->err = m;
+  return s;
+}
+
+template <typename F>
+lvg_status guarded(lvg_ctx* c, F&& f) {
+  try {
+    f();
+    if (c) c->err.clear();
+    return LVG_OK;
+  } catch (const Error& e) {
+    return fail(c, e.status, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(c, LVG_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(c, LVG_ERR_CUDA, e.what());
+  }
+}
+
+void require(bool ok, lvg_status s, const char* m) {
+  if (!ok) throw Error(s, m);
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// Device bytes for a level-0 graph of V vertices and E entries: level-0 list
+// copy, composed partition, CSR + per-vertex arrays + community state, and the
+// largest phase scratch (the doubled-list sort of the CSR build).
+size_t arena_estimate(int64_t V, int64_t E, bool copy_list) {
+  size_t b = 0;
+  if (copy_list) b += 12 * (size_t)E;
+  b += 4 * (size_t)V;                       // composed
+  b += 16 * (size_t)E + 80 * (size_t)V;     // CSR (<= 2E entries) + per-vertex + state
+  b += 88 * (size_t)E + 24 * (size_t)V;     // build scratch: 2 x 2E x 12 B sort, head/pos, wsum
+  b += 16 * (size_t)E;                      // hub tables (degree-bounded) and per-level partitions
+  b += (size_t)64 << 20;
+  return b;
+}
+
+void sync(lvg_ctx* c) { LVG_CUDA(cudaStreamSynchronize(c->stream)); }
+
+// Prepare the current level (c->g holds the level input list): build, state.
+void prepare_level(lvg_ctx* c) {
+  build_level(c->g, c->tune, c->arena, c->stream);
+  alloc_state(c->g, c->st, c->arena);
+  init_state(c->g, c->st, 0.0, c->cfg.pass_min_gain, c->cfg.max_passes, c->arena, c->stream);
+  c->have_state = true;
+  c->renumbered = false;
+}
+
+void load_common(lvg_ctx* c, const int32_t* d_src, const int32_t* d_dst, const float* d_w, int64_t E,
+                 int32_t V) {
+  c->V0 = V;
+  c->E0 = E;
+  c->src0 = d_src;
+  c->dst0 = d_dst;
+  c->w0 = d_w;
+  c->composed = c->arena.lo_n<int32_t>(V);
+  std::vector<int32_t> iota(V);
+  for (int32_t i = 0; i < V; ++i) iota[i] = i;
+  LVG_CUDA(cudaMemcpyAsync(c->composed, iota.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, c->stream));
+  sync(c);
+  c->base_lo = c->arena.lo;
+  c->run_hi = c->arena.hi;
+  c->levels.clear();
+  c->level = 0;
+  c->g = LevelGraph();
+  c->g.V = V;
+  c->g.E = E;
+  c->g.src = d_src;
+  c->g.dst = d_dst;
+  c->g.w = d_w;
+  prepare_level(c);
+  c->loaded = true;
+}
+
+void reset_to_level0(lvg_ctx* c) {
+  // rebuild level 0 from the loaded list (used by lvg_run after partial steps)
+  c->arena.lo = c->base_lo;
+  c->arena.hi = c->run_hi = c->arena.cap;
+  std::vector<int32_t> iota(c->V0);
+  for (int32_t i = 0; i < c->V0; ++i) iota[i] = i;
+  LVG_CUDA(cudaMemcpyAsync(c->composed, iota.data(), sizeof(int32_t) * c->V0, cudaMemcpyHostToDevice, c->stream));
+  sync(c);
+  c->levels.clear();
+  c->level = 0;
+  c->g = LevelGraph();
+  c->g.V = c->V0;
+  c->g.E = c->E0;
+  c->g.src = c->src0;
+  c->g.dst = c->dst0;
+  c->g.w = c->w0;
+  prepare_level(c);
+}
+
+double read_q(lvg_ctx* c) {
+  HiScope hs(c->arena);
+  double* d = c->arena.hi_n<double>(1);
+  launch_q(c->g, c->st, d, c->stream);
+  double q = 0.0;
+  LVG_CUDA(cudaMemcpyAsync(&q, d, sizeof q, cudaMemcpyDeviceToHost, c->stream));
+  sync(c);
+  return q;
+}
+
+constexpr int kHardPassCap = 1 << 20;
+
+// One-level phase (oneLevelCUDA, OneLevelKernel.cu:518-954).
+void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int32_t* status_out,
+               double* q_start_out) {
+  cudaStream_t s = c->stream;
+  init_state(c->g, c->st, lower, c->cfg.pass_min_gain, c->cfg.max_passes, c->arena, s);
+  PassCtl h;
+  const int chunk = c->cfg.passes_per_sync > 0 ? c->cfg.passes_per_sync : 4;
+  c->pass_ms.clear();
+  LVG_CUDA(cudaEventRecord(c->ev0, s));
+  int launched = 0;
+  for (;;) {
+    for (int p = 0; p < chunk; ++p) {
+      size_t e = 2 * (size_t)launched;
+      while (c->mev.size() < e + 2) {
+        cudaEvent_t ev;
+        LVG_CUDA(cudaEventCreate(&ev));
+        c->mev.push_back(ev);
+      }
+      LVG_CUDA(cudaEventRecord(c->mev[e], s));
+      launch_moves(c->g, c->st, s);
+      LVG_CUDA(cudaEventRecord(c->mev[e + 1], s));
+      launch_commit(c->g, c->st, s);
+      ++launched;
+    }
+    LVG_CUDA(cudaMemcpyAsync(&h, c->st.ctl, sizeof h, cudaMemcpyDeviceToHost, s));
+    sync(c);
+    if (h.done) break;
+    if (h.err) throw Error(LVG_ERR_CAPACITY, "neighbour-community table probe limit exceeded");
+    // every pass must raise Q by pass_min_gain over a bounded range, so a
+    // level that runs this long has lost its state: stop with an error
+    if (launched >= kHardPassCap) throw Error(LVG_ERR_NOT_CONVERGED, "hard pass cap reached");
+  }
+  launch_merge(c->g, c->st, s);
+  LVG_CUDA(cudaEventRecord(c->ev1, s));
+  LVG_CUDA(cudaMemcpyAsync(&h, c->st.ctl, sizeof h, cudaMemcpyDeviceToHost, s));
+  sync(c);
+  if (h.err) throw Error(LVG_ERR_CAPACITY, "neighbour-community table probe limit exceeded");
+  c->pass_ms.push_back(elapsed(c->ev0, c->ev1));
+  c->move_ms = 0.0;
+  c->move_passes = h.passes;
+  for (int p = 0; p < h.passes && 2 * (size_t)p + 1 < c->mev.size(); ++p)
+    c->move_ms += elapsed(c->mev[2 * p], c->mev[2 * p + 1]);
+  if (q_out) *q_out = h.q_ret;
+  if (passes_out) *passes_out = h.passes;
+  if (status_out) *status_out = h.status;
+  (void)q_start_out;
+  (void)launched;
+}
+
+// Renumber the current level; the partition and labels live on the arena's
+// high end for the rest of the run.
+int32_t renumber_level(lvg_ctx* c) {
+  const int32_t V = c->g.V;
+  c->arena.hi = c->run_hi;
+  int32_t* part = c->arena.hi_n<int32_t>(V);
+  int32_t* labels = c->arena.hi_n<int32_t>(V);
+  c->run_hi = c->arena.hi;
+  LVG_CUDA(cudaMemcpyAsync(labels, c->st.comm, sizeof(int32_t) * std::max(V, 1), cudaMemcpyDeviceToDevice,
+                           c->stream));
+  int32_t C = renumber(c->g, c->st.comm, part, c->arena, c->stream);
+  compose(c->composed, part, c->V0, c->stream);    // partitionAtLevel (LouvainCPP.cpp:82-106)
+  c->d_part_cur = part;
+  c->C_cur = C;
+  c->renumbered = true;
+  LevelRec r;
+  std::memset(&r.info, 0, sizeof r.info);
+  r.d_part = part;
+  r.d_labels = labels;
+  r.info.n_vertices = V;
+  r.info.n_entries = c->g.E;
+  r.info.nnz = c->g.nnz;
+  r.info.n_comms = C;
+  c->levels.push_back(r);
+  return C;
+}
+
+// Coarsen into the next level and build it.
+void induce_level(lvg_ctx* c) {
+  int32_t *os = nullptr, *od = nullptr;
+  float* ow = nullptr;
+  c->arena.hi = c->run_hi;
+  int64_t n = induce(c->g, c->d_part_cur, c->C_cur, &os, &od, &ow, c->arena, c->stream);
+  // the next level's list moves down to the start of the level region
+  c->arena.lo = c->base_lo;
+  int32_t* ns = c->arena.lo_n<int32_t>(n);
+  int32_t* nd = c->arena.lo_n<int32_t>(n);
+  float* nw = c->arena.lo_n<float>(n);
+  if (n > 0) {
+    LVG_CUDA(cudaMemcpyAsync(ns, os, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
+    LVG_CUDA(cudaMemcpyAsync(nd, od, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
+    LVG_CUDA(cudaMemcpyAsync(nw, ow, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  sync(c);
+  c->arena.hi = c->run_hi;
+  int32_t C = c->C_cur;
+  c->g = LevelGraph();
+  c->g.V = C;
+  c->g.E = n;
+  c->g.src = ns;
+  c->g.dst = nd;
+  c->g.w = nw;
+  c->level += 1;
+  prepare_level(c);
+}
+
+void check_ctx(lvg_ctx* c) {
+  require(c != nullptr, LVG_ERR_INVALID_ARG, "null context");
+  LVG_CUDA(cudaSetDevice(c->device));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lvg_status_string(lvg_status s) {
+  switch (s) {
+    case LVG_OK: return "ok";
+    case LVG_ERR_INVALID_ARG: return "invalid argument";
+    case LVG_ERR_OOM: return "out of device memory";
+    case LVG_ERR_CAPACITY: return "capacity exceeded";
+    case LVG_ERR_NOT_CONVERGED: return "not converged";
+    case LVG_ERR_CUDA: return "CUDA error";
+    case LVG_ERR_STATE: return "call out of order";
+  }
+  return "unknown status";
+}
+
+lvg_status lvg_config_default(lvg_config* cfg) {
+  if (!cfg) return LVG_ERR_INVALID_ARG;
+  std::memset(cfg, 0, sizeof *cfg);
+  cfg->device = 0;
+  cfg->pass_min_gain = 1e-7;   // __MIN (OneLevelKernel.cu:425)
+  cfg->level_min_gain = 1e-7;  // __MIN (LouvainCPP.cpp:55)
+  cfg->max_passes = -1;        // __PASS_MAX (OneLevelKernel.cu:424)
+  cfg->max_levels = -1;
+  cfg->arena_bytes = 0;
+  cfg->warp_max_degree = 128;
+  cfg->block_max_degree = 4096;
+  cfg->passes_per_sync = 4;
+  cfg->use_graphs = 1;
+  return LVG_OK;
+}
+
+lvg_status lvg_create(const lvg_config* cfg, lvg_ctx** out) {
+  if (!out) return LVG_ERR_INVALID_ARG;
+  *out = nullptr;
+  lvg_ctx* c = new (std::nothrow) lvg_ctx();
+  if (!c) return LVG_ERR_OOM;
+  lvg_status s = guarded(c, [&] {
+    if (cfg) c->cfg = *cfg;
+    else lvg_config_default(&c->cfg);
+    require(c->cfg.warp_max_degree >= 0 && c->cfg.block_max_degree >= 0, LVG_ERR_INVALID_ARG,
+            "bucket thresholds must be >= 0");
+    c->tune.warp_max = c->cfg.warp_max_degree > 0 ? std::min(c->cfg.warp_max_degree, 128) : 128;
+    c->tune.block_max = c->cfg.block_max_degree > 0 ? std::min(c->cfg.block_max_degree, 8192) : 4096;
+    if (c->tune.block_max < c->tune.warp_max) c->tune.block_max = c->tune.warp_max;
+    c->device = c->cfg.device;
+    int n = 0;
+    LVG_CUDA(cudaGetDeviceCount(&n));
+    require(c->device >= 0 && c->device < n, LVG_ERR_INVALID_ARG, "no such CUDA device");
+    LVG_CUDA(cudaSetDevice(c->device));
+    LVG_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    LVG_CUDA(cudaEventCreate(&c->ev0));
+    LVG_CUDA(cudaEventCreate(&c->ev1));
+  });
+  if (s != LVG_OK) {
+    lvg_destroy(c);
+    return s;
+  }
+  *out = c;
+  return LVG_OK;
+}
+
+lvg_status lvg_destroy(lvg_ctx* c) {
+  if (!c) return LVG_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->arena.release();
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  for (cudaEvent_t e : c->mev) cudaEventDestroy(e);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return LVG_OK;
+}
+
+const char* lvg_last_error(const lvg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+lvg_status lvg_set_stream(lvg_ctx* c, void* stream) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  });
+}
+
+lvg_status lvg_load_edges(lvg_ctx* c, const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                          int32_t V) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(V >= 0 && E >= 0, LVG_ERR_INVALID_ARG, "negative size");
+    require(E == 0 || (src && dst && w), LVG_ERR_INVALID_ARG, "null edge array");
+    c->loaded = false;
+    size_t need = c->cfg.arena_bytes > 0 ? (size_t)c->cfg.arena_bytes : arena_estimate(V, E, true);
+    c->arena.reserve(need);
+    int32_t* s = c->arena.lo_n<int32_t>(E);
+    int32_t* d = c->arena.lo_n<int32_t>(E);
+    float* ww = c->arena.lo_n<float>(E);
+    if (E > 0) {
+      LVG_CUDA(cudaMemcpyAsync(s, src, sizeof(int32_t) * E, cudaMemcpyHostToDevice, c->stream));
+      LVG_CUDA(cudaMemcpyAsync(d, dst, sizeof(int32_t) * E, cudaMemcpyHostToDevice, c->stream));
+      LVG_CUDA(cudaMemcpyAsync(ww, w, sizeof(float) * E, cudaMemcpyHostToDevice, c->stream));
+    }
+    require(validate_edges(s, d, ww, E, V, c->arena, c->stream), LVG_ERR_INVALID_ARG,
+            "edge list has a vertex id out of range or a negative / non-finite weight");
+    load_common(c, s, d, ww, E, V);
+  });
+}
+
+lvg_status lvg_load_edges_device(lvg_ctx* c, const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                 int32_t V) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(V >= 0 && E >= 0, LVG_ERR_INVALID_ARG, "negative size");
+    require(E == 0 || (src && dst && w), LVG_ERR_INVALID_ARG, "null edge array");
+    c->loaded = false;
+    size_t need = c->cfg.arena_bytes > 0 ? (size_t)c->cfg.arena_bytes : arena_estimate(V, E, false);
+    c->arena.reserve(need);
+    require(validate_edges(src, dst, w, E, V, c->arena, c->stream), LVG_ERR_INVALID_ARG,
+            "edge list has a vertex id out of range or a negative / non-finite weight");
+    load_common(c, src, dst, w, E, V);
+  });
+}
+
+lvg_status lvg_modularity(lvg_ctx* c, double* q) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded && c->have_state, LVG_ERR_STATE, "no graph loaded");
+    require(q != nullptr, LVG_ERR_INVALID_ARG, "null output");
+    *q = read_q(c);
+  });
+}
+
+lvg_status lvg_one_level(lvg_ctx* c, double lower, double* q, int32_t* passes) {
+  int32_t status = 0;
+  lvg_status s = guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded && c->have_state, LVG_ERR_STATE, "no graph loaded");
+    one_level(c, lower, q, passes, &status, nullptr);
+  });
+  if (s == LVG_OK && status != 0) return fail(c, (lvg_status)status, "pass cap reached before convergence");
+  return s;
+}
+
+lvg_status lvg_renumber(lvg_ctx* c, int32_t* comm_out, int32_t* n_comms) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded && c->have_state, LVG_ERR_STATE, "no graph loaded");
+    int32_t C = renumber_level(c);
+    if (comm_out && c->g.V > 0)
+      LVG_CUDA(cudaMemcpyAsync(comm_out, c->d_part_cur, sizeof(int32_t) * c->g.V, cudaMemcpyDeviceToHost,
+                               c->stream));
+    sync(c);
+    if (n_comms) *n_comms = C;
+  });
+}
+
+lvg_status lvg_induce(lvg_ctx* c) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded && c->renumbered, LVG_ERR_STATE, "lvg_induce needs lvg_renumber first");
+    induce_level(c);
+  });
+}
+
+lvg_status lvg_run(lvg_ctx* c, lvg_result* res) {
+  int32_t run_status = 0;
+  lvg_status s = guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded, LVG_ERR_STATE, "no graph loaded");
+    if (c->level != 0 || c->renumbered || !c->levels.empty()) reset_to_level0(c);
+    if (res) std::memset(res, 0, sizeof *res);
+    if (c->E0 == 0) {
+      // LouvainCPP.cpp:211-230: an empty edge list yields one identity partition
+      renumber_level(c);
+      c->levels.back().info.passes = 0;
+      if (res) { res->n_levels = 1; res->n_comms = c->V0; res->q_final = 0.0; }
+      return;
+    }
+    double mod = 0.0;
+    int64_t pass_entries = 0;
+    for (;;) {
+      double q0 = read_q(c);                      // modularityCUDA (LouvainCPP.cpp:356)
+      double lower = c->level == 0 ? q0 : mod;
+      double ql = 0.0;
+      int32_t passes = 0, st = 0;
+      one_level(c, lower, &ql, &passes, &st, nullptr);
+      float ms_passes = c->pass_ms.empty() ? 0.0f : c->pass_ms.back();
+      renumber_level(c);
+      LevelRec& r = c->levels.back();
+      r.info.passes = passes;
+      r.info.q_start = q0;
+      r.info.q_level = ql;
+      r.info.ms_passes = ms_passes;
+      pass_entries += c->g.nnz * (int64_t)passes;
+      if (st != 0) { run_status = st; break; }
+      if (c->level > 0 && (ql - mod) < c->cfg.level_min_gain) break;   // LouvainCPP.cpp:466
+      if (c->cfg.max_levels >= 0 && c->level + 1 >= c->cfg.max_levels) { run_status = LVG_ERR_NOT_CONVERGED; break; }
+      mod = ql;
+      induce_level(c);
+    }
+    if (res) {
+      res->n_levels = (int32_t)c->levels.size();
+      res->n_comms = c->C_cur;
+      res->pass_entries = pass_entries;
+      res->status = run_status;
+      res->q_final = modularity_fp64(c->src0, c->dst0, c->w0, c->E0, std::max(c->C_cur, 1), c->composed,
+                                     c->arena, c->stream);
+    }
+  });
+  if (s == LVG_OK && run_status != 0) return fail(c, (lvg_status)run_status, "cap reached before convergence");
+  return s;
+}
+
+lvg_status lvg_num_levels(const lvg_ctx* c, int32_t* n) {
+  if (!c || !n) return LVG_ERR_INVALID_ARG;
+  *n = (int32_t)c->levels.size();
+  return LVG_OK;
+}
+
+lvg_status lvg_get_level_info(const lvg_ctx* c, int32_t level, lvg_level_info* info) {
+  if (!c || !info || level < 0 || level >= (int32_t)c->levels.size()) return LVG_ERR_INVALID_ARG;
+  *info = c->levels[level].info;
+  return LVG_OK;
+}
+
+lvg_status lvg_get_level_partition(const lvg_ctx* cc, int32_t level, int32_t* part) {
+  lvg_ctx* c = const_cast<lvg_ctx*>(cc);
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(part && level >= 0 && level < (int32_t)c->levels.size(), LVG_ERR_INVALID_ARG, "bad level");
+    const LevelRec& r = c->levels[level];
+    if (r.info.n_vertices > 0)
+      LVG_CUDA(cudaMemcpyAsync(part, r.d_part, sizeof(int32_t) * r.info.n_vertices, cudaMemcpyDeviceToHost,
+                               c->stream));
+    sync(c);
+  });
+}
+
+lvg_status lvg_get_level_labels(const lvg_ctx* cc, int32_t level, int32_t* labels) {
+  lvg_ctx* c = const_cast<lvg_ctx*>(cc);
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(labels && level >= 0 && level < (int32_t)c->levels.size(), LVG_ERR_INVALID_ARG, "bad level");
+    const LevelRec& r = c->levels[level];
+    if (r.info.n_vertices > 0)
+      LVG_CUDA(cudaMemcpyAsync(labels, r.d_labels, sizeof(int32_t) * r.info.n_vertices,
+                               cudaMemcpyDeviceToHost, c->stream));
+    sync(c);
+  });
+}
+
+lvg_status lvg_get_partition(const lvg_ctx* cc, int32_t level, int32_t* part) {
+  lvg_ctx* c = const_cast<lvg_ctx*>(cc);
+  return guarded(c, [&] {
+    check_ctx(c);
+    int32_t L = (int32_t)c->levels.size();
+    require(part && L > 0 && level >= 0, LVG_ERR_INVALID_ARG, "bad level");
+    if (level >= L - 1) {
+      if (c->V0 > 0)
+        LVG_CUDA(cudaMemcpyAsync(part, c->composed, sizeof(int32_t) * c->V0, cudaMemcpyDeviceToHost, c->stream));
+      sync(c);
+      return;
+    }
+    // compose levels 0..level on the host side from the per-level partitions
+    std::vector<int32_t> cur(c->V0), lv;
+    LVG_CUDA(cudaMemcpyAsync(cur.data(), c->levels[0].d_part, sizeof(int32_t) * c->V0, cudaMemcpyDeviceToHost,
+                             c->stream));
+    sync(c);
+    for (int32_t l = 1; l <= level; ++l) {
+      lv.resize(c->levels[l].info.n_vertices);
+      LVG_CUDA(cudaMemcpyAsync(lv.data(), c->levels[l].d_part, sizeof(int32_t) * lv.size(),
+                               cudaMemcpyDeviceToHost, c->stream));
+      sync(c);
+      for (auto& x : cur) x = lv[x];
+    }
+    std::memcpy(part, cur.data(), sizeof(int32_t) * c->V0);
+  });
+}
+
+lvg_status lvg_count_partitions(const int32_t* part, int64_t n, int32_t* count) {
+  if (!count || (n > 0 && !part) || n < 0) return LVG_ERR_INVALID_ARG;
+  int32_t mx = 0;                                // countPartitions (LouvainCPP.cpp:116-127)
+  for (int64_t i = 0; i < n; ++i) mx = std::max(mx, part[i]);
+  *count = 1 + mx;
+  return LVG_OK;
+}
+
+lvg_status lvg_modularity_fp64(lvg_ctx* c, const int32_t* part, double* q) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded, LVG_ERR_STATE, "no graph loaded");
+    require(part && q, LVG_ERR_INVALID_ARG, "null argument");
+    int32_t C = 0;
+    for (int32_t i = 0; i < c->V0; ++i) {
+      require(part[i] >= 0 && part[i] < std::max(c->V0, 1), LVG_ERR_INVALID_ARG, "partition id out of range");
+      C = std::max(C, part[i] + 1);
+    }
+    HiScope hs(c->arena);
+    int32_t* dp = c->arena.hi_n<int32_t>(c->V0);
+    if (c->V0 > 0)
+      LVG_CUDA(cudaMemcpyAsync(dp, part, sizeof(int32_t) * c->V0, cudaMemcpyHostToDevice, c->stream));
+    *q = modularity_fp64(c->src0, c->dst0, c->w0, c->E0, std::max(C, 1), dp, c->arena, c->stream);
+  });
+}
+
+lvg_status lvg_get_csr(const lvg_ctx* cc, int32_t* n_vertices, int64_t* nnz, double* m, int64_t* off,
+                       int32_t* col, float* w, double* k, float* loopw, uint8_t* has_loop) {
+  lvg_ctx* c = const_cast<lvg_ctx*>(cc);
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded && c->have_state, LVG_ERR_STATE, "no graph loaded");
+    const LevelGraph& g = c->g;
+    if (n_vertices) *n_vertices = g.V;
+    if (nnz) *nnz = g.nnz;
+    if (m) *m = g.m;
+    cudaStream_t s = c->stream;
+    if (off) LVG_CUDA(cudaMemcpyAsync(off, g.off, sizeof(int64_t) * (g.V + 1), cudaMemcpyDeviceToHost, s));
+    if (col && g.nnz) LVG_CUDA(cudaMemcpyAsync(col, g.col, sizeof(int32_t) * g.nnz, cudaMemcpyDeviceToHost, s));
+    if (w && g.nnz) LVG_CUDA(cudaMemcpyAsync(w, g.cw, sizeof(float) * g.nnz, cudaMemcpyDeviceToHost, s));
+    if (k && g.V) LVG_CUDA(cudaMemcpyAsync(k, g.k, sizeof(double) * g.V, cudaMemcpyDeviceToHost, s));
+    if (loopw && g.V) LVG_CUDA(cudaMemcpyAsync(loopw, g.loopw, sizeof(float) * g.V, cudaMemcpyDeviceToHost, s));
+    if (has_loop && g.V) LVG_CUDA(cudaMemcpyAsync(has_loop, g.has_loop, g.V, cudaMemcpyDeviceToHost, s));
+    sync(c);
+  });
+}
+
+lvg_status lvg_set_communities(lvg_ctx* c, const int32_t* comm) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded && c->have_state, LVG_ERR_STATE, "no graph loaded");
+    require(comm != nullptr, LVG_ERR_INVALID_ARG, "null communities");
+    const int32_t V = c->g.V;
+    for (int32_t i = 0; i < V; ++i)
+      require(comm[i] >= 0 && comm[i] < V, LVG_ERR_INVALID_ARG, "community id out of range");
+    HiScope hs(c->arena);
+    int32_t* d = c->arena.hi_n<int32_t>(V);
+    if (V > 0) LVG_CUDA(cudaMemcpyAsync(d, comm, sizeof(int32_t) * V, cudaMemcpyHostToDevice, c->stream));
+    set_state_from(c->g, c->st, d, c->stream);
+    sync(c);
+  });
+}
+
+lvg_status lvg_move_decide(lvg_ctx* c, int32_t* next, int32_t* cand) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded && c->have_state, LVG_ERR_STATE, "no graph loaded");
+    const int32_t V = c->g.V;
+    cudaStream_t s = c->stream;
+    reset_ctl(c->st, 0.0, c->cfg.pass_min_gain, -1, s);
+    clear_deltas(c->g, c->st, s);
+    launch_moves(c->g, c->st, s);
+    if (next && V) LVG_CUDA(cudaMemcpyAsync(next, c->st.next, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, s));
+    if (cand && V) LVG_CUDA(cudaMemcpyAsync(cand, c->st.cand, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, s));
+    PassCtl h;
+    LVG_CUDA(cudaMemcpyAsync(&h, c->st.ctl, sizeof h, cudaMemcpyDeviceToHost, s));
+    // leave the committed state as it was
+    clear_deltas(c->g, c->st, s);
+    if (V) LVG_CUDA(cudaMemcpyAsync(c->st.next, c->st.comm, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, s));
+    sync(c);
+    require(h.err == 0, LVG_ERR_CAPACITY, "neighbour-community table probe limit exceeded");
+  });
+}
+
+lvg_status lvg_last_pass_times(const lvg_ctx* c, float* ms, int32_t cap, int32_t* n) {
+  if (!c) return LVG_ERR_INVALID_ARG;
+  int32_t k = (int32_t)c->pass_ms.size();
+  if (ms)
+    for (int32_t i = 0; i < k && i < cap; ++i) ms[i] = c->pass_ms[i];
+  if (n) *n = k;
+  return LVG_OK;
+}
+
+lvg_status lvg_move_stats(const lvg_ctx* c, double* ms_total, int64_t* n_passes) {
+  if (!c) return LVG_ERR_INVALID_ARG;
+  if (ms_total) *ms_total = c->move_ms;
+  if (n_passes) *n_passes = c->move_passes;
+  return LVG_OK;
+}
+
+lvg_status lvg_kernel_launches(int64_t* n) {
+  if (!n) return LVG_ERR_INVALID_ARG;
+  *n = lvg::g_launches.load();
+  return LVG_OK;
+}
+
+lvg_status lvg_memory(const lvg_ctx* c, int64_t* capacity, int64_t* peak) {
+  if (!c) return LVG_ERR_INVALID_ARG;
+  if (capacity) *capacity = (int64_t)c->arena.cap;
+  if (peak) *peak = (int64_t)c->arena.peak;
+  return LVG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1142 @@
+// Louvain hot path kernels for sm_100a.
+//
+// Layout in HBM (one level):
+//   level input list  src/dst int32[E], w float[E]       (the reference's edge list)
+//   CSR               off int64[V+1], col int32[nnz], cw float[nnz]
+//                     (doubled list, equal (u,v) merged, self loops removed)
+//   per vertex        k/kfrac double, loopw float, has_loop u8
+//   community state   comm/next int32, tot/in double, size int32, deltas
+//                     dtot/din double + dsize int32, cand int32
+//
+// Every FP64 expression that feeds a decision is written with explicit
+// round-to-nearest intrinsics so it rounds exactly as the CPU oracle does.
+#include <algorithm>
+#include <climits>
+#include <vector>
+
+#include "louvain.cuh"
+#include "prims.cuh"
+
+namespace lvg {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kHubChunk = 4096;
+constexpr int kHubThreads = 512;
+constexpr int kNone = INT_MAX;
+
+__device__ __forceinline__ uint32_t hash_c(int32_t c, int logT) {
+  return (uint32_t)(((uint64_t)(uint32_t)c * 0x9E3779B97F4A7C15ull) >> (64 - logT));
+}
+
+__device__ __forceinline__ int ceil_log2(int64_t x) {  // x >= 1
+  return x <= 1 ? 0 : 64 - __clzll((unsigned long long)(x - 1));
+}
+
+// ------------------------------------------------------------------ validate
+__global__ void validate_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                int32_t V, uint32_t* bad) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    int32_t a = src[e], b = dst[e];
+    float x = w[e];
+    if (a < 0 || a >= V || b < 0 || b >= V || !(x >= 0.0f) || isinf(x)) atomicOr(bad, 1u);
+  }
+}
+
+// ------------------------------------------------------------------ CSR build
+// Doubled list D = input ++ reversed(input) (NeighbourCompute.cu:66-68) as
+// 64-bit keys (src << B | dst) with the weight as payload.
+__global__ void make_keys_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int B,
+                                 uint64_t* keys, float* vals) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t a = (uint32_t)src[e], b = (uint32_t)dst[e];
+    float x = w[e];
+    keys[e] = (a << B) | b;
+    vals[e] = x;
+    keys[E + e] = (b << B) | a;
+    vals[E + e] = x;
+  }
+}
+
+// Segmented inclusive warp sum over contiguous runs of equal `seg`.
+template <typename K>
+__device__ __forceinline__ double seg_warp_sum(double v, K seg) {
+  const unsigned full = 0xffffffffu;
+  int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    double u = __shfl_up_sync(full, v, o);
+    K t = __shfl_up_sync(full, seg, o);
+    if (lane >= o && t == seg) v = __dadd_rn(v, u);
+  }
+  return v;
+}
+
+template <typename K>
+__device__ __forceinline__ bool seg_warp_last(K seg, bool valid) {
+  const unsigned full = 0xffffffffu;
+  int lane = threadIdx.x & 31;
+  K nx = __shfl_down_sync(full, seg, 1);
+  bool nvalid = __shfl_down_sync(full, valid, 1);
+  return valid && (lane == 31 || !nvalid || nx != seg);
+}
+
+// Per sorted entry: CSR heads, row counts, degree (InitKernel.cu:154-179:
+// weight 0 counts 1, a self loop counts twice), last self-loop weight
+// (InitKernel.cu:181-194).  Grid covers n exactly in whole warps.
+__global__ void csr_scan_kernel(const uint64_t* keys, const float* vals, int64_t n, int B, uint32_t* head,
+                                int64_t* rowcnt, double* k, float* loopw, uint8_t* has_loop) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool valid = i < n;
+  uint64_t mask = (B >= 64) ? ~0ull : ((1ull << B) - 1);
+  uint64_t key = valid ? keys[i] : 0ull;
+  int64_t row = valid ? (int64_t)(key >> B) : -1;
+  uint64_t c = key & mask;
+  bool loop = valid && (uint64_t)row == c;
+  float x = valid ? vals[i] : 0.0f;
+  bool first = valid && (i == 0 || keys[i - 1] != key);
+  bool last = valid && (i == n - 1 || keys[i + 1] != key);
+  bool h = first && !loop;
+  if (valid) head[i] = h ? 1u : 0u;
+  if (h) atomicAdd((unsigned long long*)&rowcnt[row], 1ull);
+  if (loop && last) { loopw[row] = x; has_loop[row] = 1; }
+  float dv = x == 0.0f ? 1.0f : x;
+  if (loop) dv *= 2.0f;
+  double s = seg_warp_sum<int64_t>(valid ? (double)dv : 0.0, row);
+  if (seg_warp_last<int64_t>(row, valid)) atomicAdd(&k[row], s);
+}
+
+// CSR column and merged weight of every (u,v), u != v.
+__global__ void csr_emit_kernel(const uint64_t* keys, const float* vals, int64_t n, int B, const uint32_t* pos,
+                                const uint32_t* head, int32_t* col, double* wsum) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool valid = i < n;
+  uint64_t mask = (B >= 64) ? ~0ull : ((1ull << B) - 1);
+  uint64_t key = valid ? keys[i] : 0ull;
+  uint64_t row = key >> B, c = key & mask;
+  bool loop = row == c;
+  int64_t r = (valid && !loop) ? (int64_t)pos[i] + (int64_t)head[i] - 1 : -1;
+  if (valid && head[i]) col[r] = (int32_t)c;
+  double s = seg_warp_sum<int64_t>(valid && !loop ? (double)vals[i] : 0.0, r);
+  if (seg_warp_last<int64_t>(r, valid) && r >= 0) atomicAdd(&wsum[r], s);
+}
+
+__global__ void to_float_kernel(const double* x, float* y, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = __double2float_rn(x[i]);
+}
+
+// ------------------------------------------------------------------ buckets
+__device__ __forceinline__ int bucket_of(int32_t i, const int64_t* off, const double* k, int32_t wmax,
+                                         int32_t bmax) {
+  if (!(k[i] > 0.0)) return 3;  // no entry in the doubled list: never moves
+  int64_t d = off[i + 1] - off[i];
+  return d <= wmax ? 0 : (d <= bmax ? 1 : 2);
+}
+
+__global__ void __launch_bounds__(kThreads) bucket_count_kernel(int32_t V, const int64_t* off, const double* k,
+                                                                int32_t wmax, int32_t bmax, uint32_t* cnt,
+                                                                int64_t nblk) {
+  uint32_t c[3] = {0, 0, 0};
+  int64_t base = (int64_t)blockIdx.x * 2048 + (int64_t)threadIdx.x * 8;
+  for (int j = 0; j < 8; ++j) {
+    int64_t i = base + j;
+    if (i < V) {
+      int b = bucket_of((int32_t)i, off, k, wmax, bmax);
+      if (b < 3) c[b]++;
+    }
+  }
+  for (int b = 0; b < 3; ++b) {
+    uint32_t tot;
+    block_exclusive_scan256<uint32_t>(c[b], &tot);
+    if (threadIdx.x == 0) cnt[b * nblk + blockIdx.x] = tot;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) bucket_scatter_kernel(int32_t V, const int64_t* off, const double* k,
+                                                                  int32_t wmax, int32_t bmax,
+                                                                  const uint32_t* offs, int64_t nblk,
+                                                                  int32_t* list) {
+  int64_t base = (int64_t)blockIdx.x * 2048 + (int64_t)threadIdx.x * 8;
+  int8_t bid[8];
+  uint32_t c[3] = {0, 0, 0};
+  for (int j = 0; j < 8; ++j) {
+    int64_t i = base + j;
+    bid[j] = i < V ? (int8_t)bucket_of((int32_t)i, off, k, wmax, bmax) : (int8_t)3;
+    if (bid[j] < 3) c[bid[j]]++;
+  }
+  uint32_t pre[3];
+  for (int b = 0; b < 3; ++b) {
+    uint32_t tot;
+    pre[b] = block_exclusive_scan256<uint32_t>(c[b], &tot) + offs[b * nblk + blockIdx.x];
+  }
+  for (int j = 0; j < 8; ++j) {
+    int b = bid[j];
+    if (b < 3) list[pre[b]++] = (int32_t)(base + j);
+  }
+}
+
+__global__ void hub_info_kernel(const int32_t* hubs, int64_t nhub, const int64_t* off, int64_t* beg_end) {
+  int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (h < nhub) {
+    int32_t i = hubs[h];
+    beg_end[2 * h] = off[i];
+    beg_end[2 * h + 1] = off[i + 1];
+  }
+}
+
+// ------------------------------------------------------------------ state
+__global__ void init_state_kernel(int32_t V, const double* k, const float* loopw, double m, double* kfrac,
+                                  int32_t* comm, int32_t* next, double* tot, double* in, int32_t* size,
+                                  double* dtot, double* din, int32_t* dsize, int32_t* cand) {
+  double twom = __dmul_rn(2.0, m);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+    comm[i] = (int32_t)i;                 // InitKernel.cu:213-215
+    next[i] = (int32_t)i;
+    tot[i] = k[i];                        // InitKernel.cu:236
+    in[i] = (double)loopw[i];             // InitKernel.cu:242
+    size[i] = 1;                          // OneLevelKernel.cu:87
+    dtot[i] = 0.0; din[i] = 0.0; dsize[i] = 0;
+    cand[i] = -1;
+    kfrac[i] = m > 0.0 ? __ddiv_rn(k[i], twom) : 0.0;  // OneLevelKernel.cu:307
+  }
+}
+
+struct MoveArgs {
+  const int32_t* list;
+  int64_t n;
+  const int64_t* off;
+  const int32_t* col;
+  const float* cw;
+  const int32_t* comm;
+  const double* tot;
+  const int32_t* size;
+  const double* kfrac;
+  const double* k;
+  const float* loopw;
+  const uint8_t* has_loop;
+  int32_t* next;
+  int32_t* cand;
+  double* dtot;
+  double* din;
+  int32_t* dsize;
+  PassCtl* ctl;
+};
+
+// Candidate order: higher gain first, then lower community id
+// (OneLevelKernel.cu:330,358).  Only strictly positive gains are candidates.
+__device__ __forceinline__ bool better(double g2, int32_t c2, double g1, int32_t c1) {
+  return g2 > g1 || (g2 == g1 && c2 < c1);
+}
+
+__device__ __forceinline__ void consider(int32_t c, double W, double kf, const double* tot, double& bg,
+                                         int32_t& bc, double& bw) {
+  if (W != 0.0) {                                                // OneLevelKernel.cu:303
+    double g = __dsub_rn(W, __dmul_rn(tot[c], kf));              // OneLevelKernel.cu:307-313
+    if (g > 0.0 && better(g, c, bg, bc)) { bg = g; bc = c; bw = W; }
+  }
+}
+
+__device__ __forceinline__ void warp_best(double& bg, int32_t& bc, double& bw) {
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    double g = __shfl_xor_sync(full, bg, o);
+    int32_t c = __shfl_xor_sync(full, bc, o);
+    double w = __shfl_xor_sync(full, bw, o);
+    if (better(g, c, bg, bc)) { bg = g; bc = c; bw = w; }
+  }
+}
+
+// The decision for one vertex from its best candidate: singleton-pair rule
+// (OneLevelKernel.cu:407-410), remove/insert into the delta buffers
+// (OneLevelKernel.cu:52-78, 412-421) and the isolated-merge candidate
+// (OneLevelKernel.cu:142-169).
+__device__ __forceinline__ void apply_decision(const MoveArgs& P, int32_t i, int32_t own, int32_t bc, double bw,
+                                               int32_t nseg) {
+  int32_t raw = bc == kNone ? own : bc;
+  int32_t so = P.size[own], sb = P.size[raw];
+  int32_t best = raw;
+  if (so == 1 && sb == 1 && raw > own) best = own;
+  P.next[i] = best;
+  P.cand[i] = (so == 1 && nseg == 1 && raw != own && own < raw) ? raw : -1;
+  if (best != own) {
+    double ki = P.k[i];
+    double iw = __dadd_rn(bw, (double)P.loopw[i]);
+    atomicAdd(&P.dtot[own], -ki);
+    atomicAdd(&P.dtot[best], ki);
+    atomicAdd(&P.din[own], -iw);
+    atomicAdd(&P.din[best], iw);
+    atomicAdd(&P.dsize[own], -1);
+    atomicAdd(&P.dsize[best], 1);
+  }
+}
+
+// Open-addressing insert of (c, w) into a table of 2^logT slots.
+__device__ __forceinline__ bool table_insert(int32_t* keys, double* vals, int logT, int32_t c, double w) {
+  uint32_t T = 1u << logT;
+  uint32_t h = hash_c(c, logT);
+  for (uint32_t p = 0; p < T; ++p) {
+    int32_t prev = atomicCAS(&keys[h], -1, c);
+    if (prev == -1 || prev == c) { atomicAdd(&vals[h], w); return true; }
+    h = (h + 1) & (T - 1);
+  }
+  return false;
+}
+
+// Warp per vertex, neighbour-community table in shared memory.
+constexpr int kWarpSlots = 256;
+__global__ void __launch_bounds__(kThreads) move_warp_kernel(MoveArgs P) {
+  __shared__ int32_t skeys[kThreads / 32][kWarpSlots];
+  __shared__ double svals[kThreads / 32][kWarpSlots];
+  if (P.ctl->done) return;
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int32_t* keys = skeys[w];
+  double* vals = svals[w];
+  for (int s = lane; s < kWarpSlots; s += 32) { keys[s] = -1; vals[s] = 0.0; }
+  __syncwarp();
+  bool overflow = false;
+  for (int64_t item = (int64_t)blockIdx.x * (kThreads / 32) + w; item < P.n;
+       item += (int64_t)gridDim.x * (kThreads / 32)) {
+    int32_t i = P.list[item];
+    int32_t own = P.comm[i];
+    int64_t beg = P.off[i], end = P.off[i + 1];
+    int logT = max(5, ceil_log2(2 * (end - beg)));
+    int T = 1 << logT;
+    bool sawown = false;
+    for (int64_t e = beg + lane; e < end; e += 32) {
+      int32_t c = P.comm[P.col[e]];
+      sawown |= (c == own);
+      if (!table_insert(keys, vals, logT, c, (double)P.cw[e])) overflow = true;
+    }
+    __syncwarp();
+    double kf = P.kfrac[i];
+    double bg = 0.0, bw = 0.0;
+    int32_t bc = kNone;
+    int nocc = 0;
+    for (int s = lane; s < T; s += 32) {
+      int32_t c = keys[s];
+      if (c >= 0) {
+        ++nocc;
+        consider(c, vals[s], kf, P.tot, bg, bc, bw);
+        keys[s] = -1;
+        vals[s] = 0.0;
+      }
+    }
+    warp_best(bg, bc, bw);
+    nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
+    sawown = __any_sync(0xffffffffu, sawown);
+    if (lane == 0) {
+      int32_t nseg = nocc + ((P.has_loop[i] && !sawown) ? 1 : 0);
+      apply_decision(P, i, own, bc, bw, nseg);
+    }
+    __syncwarp();
+  }
+  if (__any_sync(0xffffffffu, overflow) && lane == 0) atomicOr(&P.ctl->err, kErrProbe);
+}
+
+// Block per vertex, table of up to kBlockSlots slots in dynamic shared memory.
+__global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int maxLog) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double rg[kThreads / 32], rw[kThreads / 32];
+  __shared__ int32_t rc[kThreads / 32], rn[kThreads / 32], rs[kThreads / 32];
+  if (P.ctl->done) return;
+  const int Tmax = 1 << maxLog;
+  double* vals = reinterpret_cast<double*>(smem);
+  int32_t* keys = reinterpret_cast<int32_t*>(vals + Tmax);
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int s = threadIdx.x; s < Tmax; s += kThreads) { keys[s] = -1; vals[s] = 0.0; }
+  __syncthreads();
+  bool overflow = false;
+  for (int64_t item = blockIdx.x; item < P.n; item += gridDim.x) {
+    int32_t i = P.list[item];
+    int32_t own = P.comm[i];
+    int64_t beg = P.off[i], end = P.off[i + 1];
+    int logT = min(maxLog, max(5, ceil_log2(2 * (end - beg))));
+    int T = 1 << logT;
+    bool sawown = false;
+    for (int64_t e = beg + threadIdx.x; e < end; e += kThreads) {
+      int32_t c = P.comm[P.col[e]];
+      sawown |= (c == own);
+      if (!table_insert(keys, vals, logT, c, (double)P.cw[e])) overflow = true;
+    }
+    __syncthreads();
+    double kf = P.kfrac[i];
+    double bg = 0.0, bw = 0.0;
+    int32_t bc = kNone;
+    int nocc = 0;
+    for (int s = threadIdx.x; s < T; s += kThreads) {
+      int32_t c = keys[s];
+      if (c >= 0) {
+        ++nocc;
+        consider(c, vals[s], kf, P.tot, bg, bc, bw);
+        keys[s] = -1;
+        vals[s] = 0.0;
+      }
+    }
+    warp_best(bg, bc, bw);
+    nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
+    int so = __any_sync(0xffffffffu, sawown) ? 1 : 0;
+    if (lane == 0) { rg[w] = bg; rc[w] = bc; rw[w] = bw; rn[w] = nocc; rs[w] = so; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double g = rg[0], ww = rw[0];
+      int32_t c = rc[0];
+      int n = rn[0], sw = rs[0];
+      for (int k2 = 1; k2 < kThreads / 32; ++k2) {
+        if (better(rg[k2], rc[k2], g, c)) { g = rg[k2]; c = rc[k2]; ww = rw[k2]; }
+        n += rn[k2];
+        sw |= rs[k2];
+      }
+      int32_t nseg = n + ((P.has_loop[i] && !sw) ? 1 : 0);
+      apply_decision(P, i, own, c, ww, nseg);
+    }
+    __syncthreads();
+  }
+  if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
+}
+
+// Hubs: chunks of a hub's row insert into the hub's global table ...
+struct HubArgs {
+  const int32_t* hubs;
+  const int32_t* chunk_hub;
+  const int64_t* chunk_beg;
+  const int64_t* toff;
+  const int32_t* tlog;
+  int32_t* keys;
+  double* vals;
+  uint32_t* sawown;
+};
+
+__global__ void __launch_bounds__(kThreads) hub_insert_kernel(MoveArgs P, HubArgs H) {
+  if (P.ctl->done) return;
+  int32_t h = H.chunk_hub[blockIdx.x];
+  int32_t i = H.hubs[h];
+  int32_t own = P.comm[i];
+  int64_t beg = H.chunk_beg[blockIdx.x];
+  int64_t end = min(beg + (int64_t)kHubChunk, P.off[i + 1]);
+  int32_t* keys = H.keys + H.toff[h];
+  double* vals = H.vals + H.toff[h];
+  int logT = H.tlog[h];
+  bool sawown = false, overflow = false;
+  for (int64_t e = beg + threadIdx.x; e < end; e += kThreads) {
+    int32_t c = P.comm[P.col[e]];
+    sawown |= (c == own);
+    if (!table_insert(keys, vals, logT, c, (double)P.cw[e])) overflow = true;
+  }
+  if (__syncthreads_or(sawown) && threadIdx.x == 0) atomicOr(&H.sawown[h], 1u);
+  if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
+}
+
+// ... then one block per hub scans its table, decides and clears it.
+__global__ void __launch_bounds__(kHubThreads) hub_decide_kernel(MoveArgs P, HubArgs H) {
+  __shared__ double rg[kHubThreads / 32], rw[kHubThreads / 32];
+  __shared__ int32_t rc[kHubThreads / 32], rn[kHubThreads / 32];
+  if (P.ctl->done) return;
+  int32_t h = blockIdx.x;
+  int32_t i = H.hubs[h];
+  int32_t own = P.comm[i];
+  int32_t* keys = H.keys + H.toff[h];
+  double* vals = H.vals + H.toff[h];
+  int64_t T = (int64_t)1 << H.tlog[h];
+  double kf = P.kfrac[i];
+  double bg = 0.0, bw = 0.0;
+  int32_t bc = kNone;
+  int nocc = 0;
+  for (int64_t s = threadIdx.x; s < T; s += kHubThreads) {
+    int32_t c = keys[s];
+    if (c >= 0) {
+      ++nocc;
+      consider(c, vals[s], kf, P.tot, bg, bc, bw);
+      keys[s] = -1;
+      vals[s] = 0.0;
+    }
+  }
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  warp_best(bg, bc, bw);
+  nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
+  if (lane == 0) { rg[w] = bg; rc[w] = bc; rw[w] = bw; rn[w] = nocc; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double g = rg[0], ww = rw[0];
+    int32_t c = rc[0];
+    int n = rn[0];
+    for (int k2 = 1; k2 < kHubThreads / 32; ++k2) {
+      if (better(rg[k2], rc[k2], g, c)) { g = rg[k2]; c = rc[k2]; ww = rw[k2]; }
+      n += rn[k2];
+    }
+    bool sw = H.sawown[h] != 0;
+    H.sawown[h] = 0;
+    int32_t nseg = n + ((P.has_loop[i] && !sw) ? 1 : 0);
+    apply_decision(P, i, own, c, ww, nseg);
+  }
+}
+
+// ------------------------------------------------------------------ commit + Q
+// term_c = in_c/m - (tot_c/2m)^2 (OneLevelKernel.cu:447-448), zero when m <= 0.
+__device__ __forceinline__ double q_term(double in, double tot, double m, double twom) {
+  if (!(m > 0.0)) return 0.0;
+  double a = __ddiv_rn(in, m);
+  double b = __ddiv_rn(tot, twom);
+  return __dsub_rn(a, __dmul_rn(b, b));
+}
+
+enum { kCommitInit = 0, kCommitPass = 1, kCommitForce = 2 };
+
+// kCommitPass: the ΔQ test of the pass (OneLevelKernel.cu:889-896), then
+// communitySetKernel (:93-107) and the Q of the new state; on a stop the
+// deltas are dropped (mergeInitKernel, :109-120).  kCommitForce commits
+// unconditionally (mergeSetKernel, :122-136).  kCommitInit only sums Q.
+template <int MODE>
+__global__ void __launch_bounds__(kRedThreads) commit_kernel(int32_t V, double m, int32_t* comm, const int32_t* next,
+                                                             double* tot, double* in, int32_t* size, double* dtot,
+                                                             double* din, int32_t* dsize, double* partials,
+                                                             PassCtl* ctl) {
+  __shared__ double ws[8];
+  int64_t base = (int64_t)blockIdx.x * kGroup + threadIdx.x;
+  if (MODE == kCommitPass) {
+    if (ctl->done) return;
+    bool stop = __dsub_rn(ctl->q_prev, ctl->cur) < ctl->pass_min;
+    bool capped = ctl->max_passes >= 0 && ctl->pass >= ctl->max_passes;
+    if (stop || capped) {
+      for (int j = 0; j < 8; ++j) {
+        int64_t c = base + (int64_t)j * 256;
+        if (c < V) { dtot[c] = 0.0; din[c] = 0.0; dsize[c] = 0; }
+      }
+      if (blockIdx.x == 0 && threadIdx.x == 0) ctl->stop_now = stop ? 1 : 2;
+      return;
+    }
+  }
+  double twom = __dmul_rn(2.0, m);
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    int64_t c = base + (int64_t)j * 256;
+    if (c < V) {
+      double t, x;
+      if (MODE != kCommitInit) {
+        t = __dadd_rn(tot[c], dtot[c]);
+        x = __dadd_rn(in[c], din[c]);
+        tot[c] = t; in[c] = x;
+        size[c] += dsize[c];
+        dtot[c] = 0.0; din[c] = 0.0; dsize[c] = 0;
+        comm[c] = next[c];
+      } else {
+        t = tot[c]; x = in[c];
+      }
+      s = __dadd_rn(s, q_term(x, t, m, twom));
+    }
+  }
+  double r = block_tree256(s, ws);
+  if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+
+// Intermediate tree level when a level has more than 2048 groups.
+__global__ void __launch_bounds__(kRedThreads) tree_level_ctl_kernel(const double* x, int64_t n, double* out,
+                                                                     const PassCtl* ctl, int respect_ctl) {
+  __shared__ double ws[8];
+  if (respect_ctl && (ctl->done || ctl->stop_now)) return;
+  int64_t b = blockIdx.x;
+  int64_t len = n - b * kGroup;
+  if (len > kGroup) len = kGroup;
+  double r = group_sum_block<double>(x + b * kGroup, len, ws);
+  if (threadIdx.x == 0) out[b] = r;
+}
+
+// End of a pass: either finish the level loop or move the floor and Q on.
+__global__ void __launch_bounds__(kRedThreads) ctl_pass_kernel(const double* partials, int64_t np, PassCtl* ctl) {
+  __shared__ double ws[8];
+  __shared__ int flag;
+  if (threadIdx.x == 0) flag = ctl->done ? 2 : (ctl->stop_now ? 1 : 0);
+  __syncthreads();
+  int f = flag;
+  if (f == 2) return;
+  if (f == 1) {
+    if (threadIdx.x == 0) {
+      ctl->status = ctl->stop_now == 2 ? LVG_ERR_NOT_CONVERGED : LVG_OK;
+      ctl->passes = ctl->pass;
+      ctl->stop_now = 0;
+      ctl->done = 1;
+    }
+    return;
+  }
+  double q = group_sum_block<double>(partials, np, ws);
+  if (threadIdx.x == 0) {
+    double cur = ctl->q_prev;            // curMod = newMod; if (curMod < lower) curMod = lower
+    if (cur < ctl->lower) cur = ctl->lower;
+    ctl->cur = cur;
+    ctl->q_prev = q;
+    ctl->pass += 1;
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) ctl_q_kernel(const double* partials, int64_t np, double* dst) {
+  __shared__ double ws[8];
+  double q = group_sum_block<double>(partials, np, ws);
+  if (threadIdx.x == 0) *dst = q;
+}
+
+__global__ void ctl_init_kernel(PassCtl* ctl, double lower, double pass_min, int32_t max_passes) {
+  ctl->cur = -1.0;                       // curMod = -1 (OneLevelKernel.cu:528)
+  ctl->lower = lower;
+  ctl->pass_min = pass_min;
+  ctl->q_ret = 0.0;
+  ctl->pass = 1;
+  ctl->max_passes = max_passes;
+  ctl->stop_now = 0;
+  ctl->done = 0;
+  ctl->status = 0;
+  ctl->passes = 0;
+  ctl->err = 0;
+}
+
+// Isolated-vertex merge (OneLevelKernel.cu:138-171) from the candidates of
+// the last pass; weight 0, so `in` moves by the loop weight only.
+__global__ void merge_kernel(int32_t V, const int32_t* comm, int32_t* next, const int32_t* cand, const double* k,
+                             const float* loopw, double* dtot, double* din, int32_t* dsize) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+    int32_t c = cand[i];
+    if (c >= 0) {
+      int32_t own = comm[i];
+      next[i] = c;
+      double ki = k[i];
+      double iw = __dadd_rn(0.0, (double)loopw[i]);
+      atomicAdd(&dtot[own], -ki);
+      atomicAdd(&dtot[c], ki);
+      atomicAdd(&din[own], -iw);
+      atomicAdd(&din[c], iw);
+      atomicAdd(&dsize[own], -1);
+      atomicAdd(&dsize[c], 1);
+    }
+  }
+}
+
+__global__ void set_state_kernel(int32_t V, const int32_t* src_comm, const double* k, const float* loopw,
+                                 int32_t* comm, int32_t* next, double* tot, double* in, int32_t* size) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+    int32_t c = src_comm[i];
+    comm[i] = c;
+    next[i] = c;
+    atomicAdd(&tot[c], k[i]);
+    atomicAdd(&in[c], (double)loopw[i]);
+    atomicAdd(&size[c], 1);
+  }
+}
+
+__global__ void clear_deltas_kernel(int32_t V, double* dtot, double* din, int32_t* dsize, int32_t* cand) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+    dtot[i] = 0.0; din[i] = 0.0; dsize[i] = 0;
+    if (cand) cand[i] = -1;
+  }
+}
+
+// ------------------------------------------------------------------ renumber
+__global__ void min_member_kernel(int32_t V, const int32_t* comm, int32_t* minidx) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x)
+    atomicMin(&minidx[comm[i]], (int32_t)i);
+}
+
+// Head flag of each community's smallest member.
+__global__ void head_flag_kernel(int32_t V, const int32_t* comm, const int32_t* minidx, uint32_t* flag) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < V) flag[i] = minidx[comm[i]] == (int32_t)i ? 1u : 0u;
+}
+
+__global__ void renumber_apply_kernel(int32_t V, const int32_t* comm, const uint32_t* flag, const uint32_t* pos,
+                                      int32_t* newid_of_comm) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x)
+    if (flag[i]) newid_of_comm[comm[i]] = (int32_t)pos[i];
+}
+
+__global__ void gather_kernel(int32_t V, const int32_t* comm, const int32_t* newid_of_comm, int32_t* part) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x)
+    part[i] = newid_of_comm[comm[i]];
+}
+
+// ------------------------------------------------------------------ induce
+__global__ void induce_keys_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                   const int32_t* part, int B, uint64_t* keys, float* vals) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t a = (uint32_t)part[src[e]], b = (uint32_t)part[dst[e]];
+    keys[e] = (a << B) | b;
+    float x = w[e];
+    vals[e] = x == 0.0f ? 1.0f : x;       // InducedGraphKernel.cu:38-39
+  }
+}
+
+__global__ void run_head_kernel(const uint64_t* keys, int64_t n, uint32_t* head) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    head[i] = (i == 0 || keys[i - 1] != keys[i]) ? 1u : 0u;
+}
+
+__global__ void run_sum_kernel(const uint64_t* keys, const float* vals, int64_t n, int B, const uint32_t* pos,
+                               const uint32_t* head, int32_t* osrc, int32_t* odst, double* wsum) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool valid = i < n;
+  uint64_t mask = (B >= 64) ? ~0ull : ((1ull << B) - 1);
+  uint64_t key = valid ? keys[i] : 0ull;
+  int64_t r = valid ? (int64_t)pos[i] + (int64_t)head[i] - 1 : -1;
+  if (valid && head[i]) {
+    osrc[r] = (int32_t)(key >> B);
+    odst[r] = (int32_t)(key & mask);
+  }
+  double s = seg_warp_sum<int64_t>(valid ? (double)vals[i] : 0.0, r);
+  if (seg_warp_last<int64_t>(r, valid)) atomicAdd(&wsum[r], s);
+}
+
+// ------------------------------------------------------------------ modularity
+__global__ void nm_accum_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                const int32_t* part, double* Kc, double* Ain) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    double x = (double)w[e];
+    int32_t a = part[src[e]], b = part[dst[e]];
+    atomicAdd(&Kc[a], x);
+    atomicAdd(&Kc[b], x);
+    if (a == b) atomicAdd(&Ain[a], 2.0 * x);
+  }
+}
+
+__global__ void nm_term_kernel(const double* Kc, const double* Ain, int32_t C, const double* twoW, double* t) {
+  double tw = *twoW;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C; c += (int64_t)gridDim.x * blockDim.x) {
+    double f = __ddiv_rn(Kc[c], tw);
+    t[c] = tw > 0.0 ? __dsub_rn(__ddiv_rn(Ain[c], tw), __dmul_rn(f, f)) : 0.0;
+  }
+}
+
+__global__ void compose_kernel(int32_t* composed, const int32_t* part_level, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    composed[i] = part_level[composed[i]];
+}
+
+unsigned sm_grid(int64_t n, int threads) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  int64_t g = (n + threads - 1) / threads;
+  int64_t cap = (int64_t)sms * 16;
+  if (g > cap) g = cap;
+  return (unsigned)(g > 0 ? g : 1);
+}
+
+MoveArgs move_args(const LevelGraph& g, CommState& st) {
+  MoveArgs P;
+  P.list = nullptr; P.n = 0;
+  P.off = g.off; P.col = g.col; P.cw = g.cw;
+  P.comm = st.comm; P.tot = st.tot; P.size = st.size;
+  P.kfrac = g.kfrac; P.k = g.k; P.loopw = g.loopw; P.has_loop = g.has_loop;
+  P.next = st.next; P.cand = st.cand;
+  P.dtot = st.dtot; P.din = st.din; P.dsize = st.dsize;
+  P.ctl = st.ctl;
+  return P;
+}
+
+int block_table_log(const Tuning& t) {
+  int l = 5;
+  while ((1 << l) < 2 * t.block_max) ++l;
+  return l;
+}
+
+}  // namespace
+
+// ============================================================================ host
+
+bool validate_edges(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t V, Arena& a,
+                    cudaStream_t s) {
+  if (E == 0) return true;
+  HiScope hs(a);
+  uint32_t* bad = a.hi_n<uint32_t>(1);
+  LVG_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), s));
+  validate_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, V, bad);
+  LVG_LAUNCH();
+  uint32_t h = 0;
+  LVG_CUDA(cudaMemcpyAsync(&h, bad, sizeof h, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  return h == 0;
+}
+
+void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
+  const int32_t V = g.V;
+  const int64_t E = g.E;
+  const int64_t n = 2 * E;
+  if (n >= ((int64_t)1 << 32)) throw Error(LVG_ERR_CAPACITY, "doubled edge list exceeds 2^32-1 entries");
+  // per-vertex arrays (low end, level lifetime)
+  g.off = a.lo_n<int64_t>(V + 1);
+  g.k = a.lo_n<double>(V);
+  g.kfrac = a.lo_n<double>(V);
+  g.loopw = a.lo_n<float>(V);
+  g.has_loop = a.lo_n<uint8_t>(V);
+  double* d_m = a.lo_n<double>(1);
+  LVG_CUDA(cudaMemsetAsync(g.k, 0, sizeof(double) * std::max<int32_t>(V, 1), s));
+  LVG_CUDA(cudaMemsetAsync(g.loopw, 0, sizeof(float) * std::max<int32_t>(V, 1), s));
+  LVG_CUDA(cudaMemsetAsync(g.has_loop, 0, std::max<int32_t>(V, 1), s));
+  tree_sum_f32(g.w, E, d_m, a, s);                                  // NeighbourCompute.cu:46
+  {
+    HiScope hs(a);
+    const int B = std::max(1, bits_for(V));
+    uint64_t* k0 = a.hi_n<uint64_t>(n);
+    float* v0 = a.hi_n<float>(n);
+    uint64_t* k1 = a.hi_n<uint64_t>(n);
+    float* v1 = a.hi_n<float>(n);
+    uint32_t* head = a.hi_n<uint32_t>(n + 1);
+    uint32_t* pos = a.hi_n<uint32_t>(n + 1);
+    int64_t* rowcnt = a.hi_n<int64_t>(V + 1);
+    LVG_CUDA(cudaMemsetAsync(rowcnt, 0, sizeof(int64_t) * (V + 1), s));
+    if (E > 0) {
+      make_keys_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, g.w, E, B, k0, v0);
+      LVG_LAUNCH();
+    }
+    int which = radix_sort_pairs(k0, v0, k1, v1, n, 2 * B, a, s);   // NeighbourCompute.cu:82
+    uint64_t* keys = which ? k1 : k0;
+    float* vals = which ? v1 : v0;
+    if (n > 0) {
+      csr_scan_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(keys, vals, n, B, head, rowcnt, g.k, g.loopw,
+                                                                  g.has_loop);
+      LVG_LAUNCH();
+    }
+    scan_u32(head, pos, n, a, s);
+    scan_i64(rowcnt, g.off, V, a, s);
+    int64_t nnz = 0;
+    LVG_CUDA(cudaMemcpyAsync(&nnz, g.off + V, sizeof nnz, cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaMemcpyAsync(&g.m, d_m, sizeof(double), cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaStreamSynchronize(s));
+    g.nnz = nnz;
+    // exact CSR on the low end
+    g.col = a.lo_n<int32_t>(nnz);
+    g.cw = a.lo_n<float>(nnz);
+    double* wsum = a.hi_n<double>(nnz);
+    LVG_CUDA(cudaMemsetAsync(wsum, 0, sizeof(double) * std::max<int64_t>(nnz, 1), s));
+    if (n > 0) {
+      csr_emit_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(keys, vals, n, B, pos, head, g.col, wsum);
+      LVG_LAUNCH();
+    }
+    if (nnz > 0) {
+      to_float_kernel<<<sm_grid(nnz, kThreads), kThreads, 0, s>>>(wsum, g.cw, nnz);
+      LVG_LAUNCH();
+    }
+  }
+  // degree buckets (stable by vertex index)
+  g.blist = a.lo_n<int32_t>(V);
+  {
+    HiScope hs(a);
+    int64_t nblk = (V + 2047) / 2048;
+    if (nblk == 0) nblk = 1;
+    uint32_t* cnt = a.hi_n<uint32_t>(3 * nblk + 1);
+    bucket_count_kernel<<<(unsigned)nblk, kThreads, 0, s>>>(V, g.off, g.k, t.warp_max, t.block_max, cnt, nblk);
+    LVG_LAUNCH();
+    std::vector<uint32_t> host_cnt(3 * nblk);
+    LVG_CUDA(cudaMemcpyAsync(host_cnt.data(), cnt, sizeof(uint32_t) * 3 * nblk, cudaMemcpyDeviceToHost, s));
+    scan_u32(cnt, cnt, 3 * nblk, a, s);
+    bucket_scatter_kernel<<<(unsigned)nblk, kThreads, 0, s>>>(V, g.off, g.k, t.warp_max, t.block_max, cnt, nblk,
+                                                              g.blist);
+    LVG_LAUNCH();
+    LVG_CUDA(cudaStreamSynchronize(s));
+    for (int b = 0; b < 3; ++b) {
+      int64_t c = 0;
+      for (int64_t j = 0; j < nblk; ++j) c += host_cnt[b * nblk + j];
+      g.nbucket[b] = c;
+    }
+  }
+  // hub tables
+  g.nchunk = 0;
+  g.hub_slots = 0;
+  const int64_t nhub = g.nbucket[2];
+  if (nhub > 0) {
+    const int32_t* hubs = g.blist + g.nbucket[0] + g.nbucket[1];
+    std::vector<int64_t> be(2 * nhub);
+    {
+      HiScope hs(a);
+      int64_t* d_be = a.hi_n<int64_t>(2 * nhub);
+      hub_info_kernel<<<grid_for(nhub, kThreads), kThreads, 0, s>>>(hubs, nhub, g.off, d_be);
+      LVG_LAUNCH();
+      LVG_CUDA(cudaMemcpyAsync(be.data(), d_be, sizeof(int64_t) * 2 * nhub, cudaMemcpyDeviceToHost, s));
+      LVG_CUDA(cudaStreamSynchronize(s));
+    }
+    std::vector<int64_t> toff(nhub);
+    std::vector<int32_t> tlog(nhub), chub;
+    std::vector<int64_t> cbeg;
+    int64_t slots = 0;
+    for (int64_t h = 0; h < nhub; ++h) {
+      int64_t d = be[2 * h + 1] - be[2 * h];
+      int l = 5;
+      while (((int64_t)1 << l) < 2 * d) ++l;
+      toff[h] = slots;
+      tlog[h] = l;
+      slots += (int64_t)1 << l;
+      for (int64_t b = be[2 * h]; b < be[2 * h + 1]; b += kHubChunk) {
+        chub.push_back((int32_t)h);
+        cbeg.push_back(b);
+      }
+    }
+    g.hub_slots = slots;
+    g.nchunk = (int64_t)chub.size();
+    g.hub_toff = a.lo_n<int64_t>(nhub);
+    g.hub_tlog = a.lo_n<int32_t>(nhub);
+    g.chunk_hub = a.lo_n<int32_t>(g.nchunk);
+    g.chunk_beg = a.lo_n<int64_t>(g.nchunk);
+    g.hub_keys = a.lo_n<int32_t>(slots);
+    g.hub_vals = a.lo_n<double>(slots);
+    g.hub_sawown = a.lo_n<uint32_t>(nhub);
+    LVG_CUDA(cudaMemcpyAsync(g.hub_toff, toff.data(), sizeof(int64_t) * nhub, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.hub_tlog, tlog.data(), sizeof(int32_t) * nhub, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.chunk_hub, chub.data(), sizeof(int32_t) * g.nchunk, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.chunk_beg, cbeg.data(), sizeof(int64_t) * g.nchunk, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemsetAsync(g.hub_keys, 0xff, sizeof(int32_t) * slots, s));
+    LVG_CUDA(cudaMemsetAsync(g.hub_vals, 0, sizeof(double) * slots, s));
+    LVG_CUDA(cudaMemsetAsync(g.hub_sawown, 0, sizeof(uint32_t) * nhub, s));
+    LVG_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
+  }
+  g.block_log = block_table_log(t);
+}
+
+void alloc_state(const LevelGraph& g, CommState& st, Arena& a) {
+  const int32_t V = g.V;
+  st.comm = a.lo_n<int32_t>(V);
+  st.next = a.lo_n<int32_t>(V);
+  st.tot = a.lo_n<double>(V);
+  st.in = a.lo_n<double>(V);
+  st.size = a.lo_n<int32_t>(V);
+  st.dtot = a.lo_n<double>(V);
+  st.din = a.lo_n<double>(V);
+  st.dsize = a.lo_n<int32_t>(V);
+  st.cand = a.lo_n<int32_t>(V);
+  st.ngroups = (V + kGroup - 1) / kGroup;
+  if (st.ngroups == 0) st.ngroups = 1;
+  st.partials = a.lo_n<double>(st.ngroups);
+  st.partials2 = a.lo_n<double>((st.ngroups + kGroup - 1) / kGroup);
+  st.ctl = a.lo_n<PassCtl>(1);
+}
+
+// Q of the committed state through the fixed tree into *dst.
+static void q_tail(const CommState& st, double* dst, cudaStream_t s, bool respect_ctl) {
+  const double* p = st.partials;
+  int64_t np = st.ngroups;
+  if (np > kGroup) {
+    int64_t nb = (np + kGroup - 1) / kGroup;
+    tree_level_ctl_kernel<<<(unsigned)nb, kRedThreads, 0, s>>>(p, np, st.partials2, st.ctl, respect_ctl ? 1 : 0);
+    LVG_LAUNCH();
+    p = st.partials2;
+    np = nb;
+  }
+  if (respect_ctl) {
+    ctl_pass_kernel<<<1, kRedThreads, 0, s>>>(p, np, st.ctl);
+  } else {
+    ctl_q_kernel<<<1, kRedThreads, 0, s>>>(p, np, dst);
+  }
+  LVG_LAUNCH();
+}
+
+void init_state(const LevelGraph& g, CommState& st, double lower, double pass_min, int32_t max_passes, Arena& a,
+                cudaStream_t s) {
+  (void)a;
+  const int32_t V = g.V;
+  if (V > 0) {
+    init_state_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, g.k, g.loopw, g.m, g.kfrac, st.comm, st.next,
+                                                                st.tot, st.in, st.size, st.dtot, st.din, st.dsize,
+                                                                st.cand);
+    LVG_LAUNCH();
+  }
+  ctl_init_kernel<<<1, 1, 0, s>>>(st.ctl, lower, pass_min, max_passes);
+  LVG_LAUNCH();
+  launch_q(g, st, &st.ctl->q_prev, s);
+}
+
+void launch_q(const LevelGraph& g, CommState& st, double* dst, cudaStream_t s) {
+  commit_kernel<kCommitInit><<<(unsigned)st.ngroups, kRedThreads, 0, s>>>(
+      g.V, g.m, st.comm, st.next, st.tot, st.in, st.size, st.dtot, st.din, st.dsize, st.partials, st.ctl);
+  LVG_LAUNCH();
+  q_tail(st, dst, s, false);
+}
+
+void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s) {
+  MoveArgs P = move_args(g, st);
+  const int64_t nhub = g.nbucket[2];
+  if (nhub > 0) {
+    HubArgs H;
+    H.hubs = g.blist + g.nbucket[0] + g.nbucket[1];
+    H.chunk_hub = g.chunk_hub; H.chunk_beg = g.chunk_beg;
+    H.toff = g.hub_toff; H.tlog = g.hub_tlog;
+    H.keys = g.hub_keys; H.vals = g.hub_vals; H.sawown = g.hub_sawown;
+    hub_insert_kernel<<<(unsigned)g.nchunk, kThreads, 0, s>>>(P, H);
+    LVG_LAUNCH();
+    hub_decide_kernel<<<(unsigned)nhub, kHubThreads, 0, s>>>(P, H);
+    LVG_LAUNCH();
+  }
+  if (g.nbucket[1] > 0) {
+    P.list = g.blist + g.nbucket[0];
+    P.n = g.nbucket[1];
+    int lg = g.block_log;
+    size_t smem = ((size_t)1 << lg) * (sizeof(double) + sizeof(int32_t));
+    static size_t attr = 0;
+    if (smem > attr) {
+      LVG_CUDA(cudaFuncSetAttribute(move_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr = smem;
+    }
+    move_block_kernel<<<sm_grid(P.n, 1), kThreads, smem, s>>>(P, lg);
+    LVG_LAUNCH();
+  }
+  if (g.nbucket[0] > 0) {
+    P.list = g.blist;
+    P.n = g.nbucket[0];
+    move_warp_kernel<<<grid_for(P.n, kThreads / 32), kThreads, 0, s>>>(P);
+    LVG_LAUNCH();
+  }
+}
+
+void launch_pass(const LevelGraph& g, CommState& st, cudaStream_t s) {
+  launch_moves(g, st, s);
+  launch_commit(g, st, s);
+}
+
+void launch_commit(const LevelGraph& g, CommState& st, cudaStream_t s) {
+  commit_kernel<kCommitPass><<<(unsigned)st.ngroups, kRedThreads, 0, s>>>(
+      g.V, g.m, st.comm, st.next, st.tot, st.in, st.size, st.dtot, st.din, st.dsize, st.partials, st.ctl);
+  LVG_LAUNCH();
+  q_tail(st, nullptr, s, true);
+}
+
+void launch_merge(const LevelGraph& g, CommState& st, cudaStream_t s) {
+  const int32_t V = g.V;
+  if (V > 0) {
+    merge_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, st.comm, st.next, st.cand, g.k, g.loopw, st.dtot,
+                                                          st.din, st.dsize);
+    LVG_LAUNCH();
+  }
+  commit_kernel<kCommitForce><<<(unsigned)st.ngroups, kRedThreads, 0, s>>>(
+      V, g.m, st.comm, st.next, st.tot, st.in, st.size, st.dtot, st.din, st.dsize, st.partials, st.ctl);
+  LVG_LAUNCH();
+  q_tail(st, &st.ctl->q_ret, s, false);
+}
+
+void set_state_from(const LevelGraph& g, CommState& st, const int32_t* d_comm, cudaStream_t s) {
+  const int32_t V = g.V;
+  if (V == 0) return;
+  LVG_CUDA(cudaMemsetAsync(st.tot, 0, sizeof(double) * V, s));
+  LVG_CUDA(cudaMemsetAsync(st.in, 0, sizeof(double) * V, s));
+  LVG_CUDA(cudaMemsetAsync(st.size, 0, sizeof(int32_t) * V, s));
+  set_state_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, d_comm, g.k, g.loopw, st.comm, st.next, st.tot,
+                                                             st.in, st.size);
+  LVG_LAUNCH();
+  clear_deltas(g, st, s);
+}
+
+void reset_ctl(CommState& st, double lower, double pass_min, int32_t max_passes, cudaStream_t s) {
+  ctl_init_kernel<<<1, 1, 0, s>>>(st.ctl, lower, pass_min, max_passes);
+  LVG_LAUNCH();
+}
+
+void clear_deltas(const LevelGraph& g, CommState& st, cudaStream_t s) {
+  if (g.V == 0) return;
+  clear_deltas_kernel<<<sm_grid(g.V, kThreads), kThreads, 0, s>>>(g.V, st.dtot, st.din, st.dsize, st.cand);
+  LVG_LAUNCH();
+}
+
+int32_t renumber(const LevelGraph& g, const int32_t* comm, int32_t* part, Arena& a, cudaStream_t s) {
+  const int32_t V = g.V;
+  if (V == 0) return 0;
+  HiScope hs(a);
+  int32_t* minidx = a.hi_n<int32_t>(V);
+  uint32_t* flag = a.hi_n<uint32_t>(V + 1);
+  uint32_t* pos = a.hi_n<uint32_t>(V + 1);
+  LVG_CUDA(cudaMemsetAsync(minidx, 0x7f, sizeof(int32_t) * V, s));
+  min_member_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, comm, minidx);
+  LVG_LAUNCH();
+  head_flag_kernel<<<grid_for(V, kThreads), kThreads, 0, s>>>(V, comm, minidx, flag);
+  LVG_LAUNCH();
+  scan_u32(flag, pos, V, a, s);
+  renumber_apply_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, comm, flag, pos, minidx);
+  LVG_LAUNCH();
+  gather_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, comm, minidx, part);
+  LVG_LAUNCH();
+  uint32_t C = 0;
+  LVG_CUDA(cudaMemcpyAsync(&C, pos + V, sizeof C, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  return (int32_t)C;
+}
+
+int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** out_src, int32_t** out_dst,
+               float** out_w, Arena& a, cudaStream_t s) {
+  const int64_t E = g.E;
+  if (E >= ((int64_t)1 << 32)) throw Error(LVG_ERR_CAPACITY, "level edge list exceeds 2^32-1 entries");
+  // the output stays in high scratch for the caller; temporaries are released below it
+  int32_t* osrc = a.hi_n<int32_t>(E);
+  int32_t* odst = a.hi_n<int32_t>(E);
+  float* ow = a.hi_n<float>(E);
+  int64_t cnt = 0;
+  {
+    HiScope hs(a);
+    const int B = std::max(1, bits_for(C));
+    uint64_t* k0 = a.hi_n<uint64_t>(E);
+    float* v0 = a.hi_n<float>(E);
+    uint64_t* k1 = a.hi_n<uint64_t>(E);
+    float* v1 = a.hi_n<float>(E);
+    uint32_t* head = a.hi_n<uint32_t>(E + 1);
+    uint32_t* pos = a.hi_n<uint32_t>(E + 1);
+    double* wsum = a.hi_n<double>(E);
+    if (E > 0) {
+      induce_keys_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, g.w, E, part, B, k0, v0);
+      LVG_LAUNCH();
+    }
+    int which = radix_sort_pairs(k0, v0, k1, v1, E, 2 * B, a, s);   // InducedGraphKernel.cu:91
+    uint64_t* keys = which ? k1 : k0;
+    float* vals = which ? v1 : v0;
+    if (E > 0) {
+      run_head_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(keys, E, head);
+      LVG_LAUNCH();
+    }
+    scan_u32(head, pos, E, a, s);
+    uint32_t n_out = 0;
+    LVG_CUDA(cudaMemcpyAsync(&n_out, pos + E, sizeof n_out, cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaStreamSynchronize(s));
+    cnt = n_out;
+    LVG_CUDA(cudaMemsetAsync(wsum, 0, sizeof(double) * std::max<int64_t>(cnt, 1), s));
+    if (E > 0) {
+      run_sum_kernel<<<grid_for(E, kThreads), kThreads, 0, s>>>(keys, vals, E, B, pos, head, osrc, odst, wsum);
+      LVG_LAUNCH();
+    }
+    if (cnt > 0) {
+      to_float_kernel<<<sm_grid(cnt, kThreads), kThreads, 0, s>>>(wsum, ow, cnt);
+      LVG_LAUNCH();
+    }
+    LVG_CUDA(cudaStreamSynchronize(s));
+  }
+  *out_src = osrc;
+  *out_dst = odst;
+  *out_w = ow;
+  return cnt;
+}
+
+double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
+                       const int32_t* part, Arena& a, cudaStream_t s) {
+  HiScope hs(a);
+  double* Kc = a.hi_n<double>(C);
+  double* Ain = a.hi_n<double>(C);
+  double* t = a.hi_n<double>(C);
+  double* twoW = a.hi_n<double>(2);
+  LVG_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * std::max(C, 1), s));
+  LVG_CUDA(cudaMemsetAsync(Ain, 0, sizeof(double) * std::max(C, 1), s));
+  if (E > 0) {
+    nm_accum_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
+    LVG_LAUNCH();
+  }
+  tree_sum_f64(Kc, C, twoW, a, s);
+  nm_term_kernel<<<sm_grid(C, kThreads), kThreads, 0, s>>>(Kc, Ain, C, twoW, t);
+  LVG_LAUNCH();
+  tree_sum_f64(t, C, twoW + 1, a, s);
+  double q = 0.0;
+  LVG_CUDA(cudaMemcpyAsync(&q, twoW + 1, sizeof q, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  return q;
+}
+
+void compose(int32_t* composed, const int32_t* part_level, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  compose_kernel<<<sm_grid(n, kThreads), kThreads, 0, s>>>(composed, part_level, n);
+  LVG_LAUNCH();
+}
+
+}  // namespace lvg

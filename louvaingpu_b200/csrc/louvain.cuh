@@ -1,0 +1,128 @@
+// Level data structures and host-side phase functions of the Louvain hot path.
+#pragma once
+#include <vector>
+
+#include "lvg_internal.cuh"
+
+namespace lvg {
+
+// Control block of the pass loop, resident on the device so that a whole
+// level of passes runs without host round trips.  Kernels of a pass that
+// start after `done` is set return at once.
+struct PassCtl {
+  double q_prev;     // Q of the committed state, tested by this pass
+  double cur;        // running floor (curMod, OneLevelKernel.cu:528,894-896)
+  double lower;      // floor given by the caller
+  double pass_min;   // __MIN (OneLevelKernel.cu:425)
+  double q_ret;      // Q after the isolated-vertex merge
+  int32_t pass;      // 1-based pass in progress
+  int32_t max_passes;
+  int32_t stop_now;  // 1: gain below threshold this pass, 2: pass cap
+  int32_t done;
+  int32_t status;    // LVG_OK or LVG_ERR_NOT_CONVERGED
+  int32_t passes;    // passes executed
+  uint32_t err;      // device-side error bits
+  int32_t pad;
+};
+
+enum : uint32_t { kErrProbe = 1u };
+
+// One level of the graph on the device.
+struct LevelGraph {
+  int32_t V = 0;
+  int64_t E = 0;                  // level input list
+  const int32_t* src = nullptr;
+  const int32_t* dst = nullptr;
+  const float* w = nullptr;
+  int64_t nnz = 0;                // merged doubled list, self loops removed
+  int64_t* off = nullptr;         // [V+1]
+  int32_t* col = nullptr;         // [nnz]
+  float* cw = nullptr;            // [nnz]
+  double* k = nullptr;            // degree (InitKernel.cu:154-179), 0 for vertices without entries
+  double* kfrac = nullptr;        // k / 2m
+  float* loopw = nullptr;         // last self-loop weight (InitKernel.cu:181-194,239-242)
+  uint8_t* has_loop = nullptr;
+  double m = 0.0;                 // sum of input weights (NeighbourCompute.cu:46)
+  int32_t* blist = nullptr;       // vertices grouped by bucket: warp | block | hub
+  int64_t nbucket[3] = {0, 0, 0};
+  int32_t max_deg = 0;
+  int block_log = 13;             // log2 slots of the block-per-vertex table
+  // hub tables
+  int64_t hub_slots = 0;
+  int64_t* hub_toff = nullptr;    // [nhub] table offset
+  int32_t* hub_tlog = nullptr;    // [nhub] log2 table size
+  int32_t* chunk_hub = nullptr;   // [nchunk] hub index of the chunk
+  int64_t* chunk_beg = nullptr;   // [nchunk] first CSR entry of the chunk
+  int64_t nchunk = 0;
+  int32_t* hub_keys = nullptr;
+  double* hub_vals = nullptr;
+  uint32_t* hub_sawown = nullptr;
+};
+
+struct CommState {
+  int32_t* comm = nullptr;
+  int32_t* next = nullptr;
+  double* tot = nullptr;
+  double* in = nullptr;
+  int32_t* size = nullptr;
+  double* dtot = nullptr;
+  double* din = nullptr;
+  int32_t* dsize = nullptr;
+  int32_t* cand = nullptr;
+  double* partials = nullptr;     // level-1 group partials of Q
+  double* partials2 = nullptr;
+  PassCtl* ctl = nullptr;
+  int64_t ngroups = 0;
+};
+
+struct Tuning {
+  int32_t warp_max = 128;
+  int32_t block_max = 4096;
+};
+
+// Validate an input list on the device: ids in range, weights finite >= 0.
+bool validate_edges(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t V,
+                    Arena& a, cudaStream_t s);
+
+// Build the level CSR, degrees, loops and buckets (NeighbourCompute.cu:42-117,
+// InitKernel.cu:245-339).  Level arrays go to the arena's low end.
+void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s);
+
+// Allocate community state for g (low end) and set the singleton state
+// (InitKernel.cu:196-216, OneLevelKernel.cu:80-91); ctl->q_prev = Q(S0).
+void alloc_state(const LevelGraph& g, CommState& st, Arena& a);
+void init_state(const LevelGraph& g, CommState& st, double lower, double pass_min, int32_t max_passes,
+                Arena& a, cudaStream_t s);
+
+// Launch one pass: move kernels + conditional commit + control.
+void launch_pass(const LevelGraph& g, CommState& st, cudaStream_t s);
+// The ΔQ test, conditional commit and pass control of one pass.
+void launch_commit(const LevelGraph& g, CommState& st, cudaStream_t s);
+// Launch only the move kernels (decisions, accumulations into d*).
+void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s);
+// After the loop is done: isolated-vertex merge, final commit, ctl->q_ret.
+void launch_merge(const LevelGraph& g, CommState& st, cudaStream_t s);
+// Q of the committed state into *dst (device).
+void launch_q(const LevelGraph& g, CommState& st, double* dst, cudaStream_t s);
+// Overwrite the committed state from comm (device) and recompute totals.
+void set_state_from(const LevelGraph& g, CommState& st, const int32_t* d_comm, cudaStream_t s);
+void clear_deltas(const LevelGraph& g, CommState& st, cudaStream_t s);
+void reset_ctl(CommState& st, double lower, double pass_min, int32_t max_passes, cudaStream_t s);
+
+// Renumber (RenumberKernel.cu:63-221): part[i] = rank of comm[i] by smallest
+// member index; returns the community count (synchronises).
+int32_t renumber(const LevelGraph& g, const int32_t* comm, int32_t* part, Arena& a, cudaStream_t s);
+
+// Coarsen (InducedGraphKernel.cu:50-113): writes the next level input list to
+// high-end scratch and returns its size; out_* point into that scratch.
+int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** out_src, int32_t** out_dst,
+               float** out_w, Arena& a, cudaStream_t s);
+
+// FP64 Newman modularity of part[] (values < C) over an input list (device).
+double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
+                       const int32_t* part, Arena& a, cudaStream_t s);
+
+// part_out[i] = part_level[composed[i]] for i < n.
+void compose(int32_t* composed, const int32_t* part_level, int64_t n, cudaStream_t s);
+
+}  // namespace lvg

@@ -1,0 +1,101 @@
+"""Seeded synthetic graphs of the benchmark shapes (host generators in C++).
+
+Each function returns (n_vertices, src, dst, w) as numpy arrays: a symmetric
+edge list (both directions), no self loops, duplicates merged, sorted.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from ._lib import GEN_PATH
+
+_gen = None
+
+
+def _load():
+    global _gen
+    if _gen is None:
+        if not os.path.exists(GEN_PATH):
+            from .build import build_gen
+            build_gen()
+        L = ctypes.CDLL(GEN_PATH)
+        P, i32, i64, dbl, u64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_uint64
+        L.lvggen_sbm.restype = P
+        L.lvggen_sbm.argtypes = [i32, i32, dbl, dbl, i32, i32, u64]
+        L.lvggen_lfr.restype = P
+        L.lvggen_lfr.argtypes = [i32, dbl, i32, i32, dbl, i32, i32, dbl, u64]
+        L.lvggen_rmat.restype = P
+        L.lvggen_rmat.argtypes = [i32, i32, dbl, dbl, dbl, i32, i32, u64]
+        L.lvggen_n_vertices.restype = i32
+        L.lvggen_n_vertices.argtypes = [P]
+        L.lvggen_n_entries.restype = i64
+        L.lvggen_n_entries.argtypes = [P]
+        L.lvggen_copy.argtypes = [P, P, P, P]
+        L.lvggen_truth.argtypes = [P, P]
+        L.lvggen_free.argtypes = [P]
+        _gen = L
+    return _gen
+
+
+def _take(h, with_truth=False):
+    L = _load()
+    if not h:
+        raise ValueError("generator rejected its parameters")
+    try:
+        n = L.lvggen_n_vertices(h)
+        E = L.lvggen_n_entries(h)
+        src = np.zeros(E, np.int32)
+        dst = np.zeros(E, np.int32)
+        w = np.zeros(E, np.float32)
+        c = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        L.lvggen_copy(h, c(src), c(dst), c(w))
+        truth = None
+        if with_truth:
+            truth = np.zeros(n, np.int32)
+            L.lvggen_truth(h, c(truth))
+    finally:
+        L.lvggen_free(h)
+    return (n, src, dst, w, truth) if with_truth else (n, src, dst, w)
+
+
+def sbm(n, blocks, p_in, p_out, w_lo=1, w_hi=1, seed=0, with_truth=False):
+    """Planted-partition SBM with near-equal blocks."""
+    return _take(_load().lvggen_sbm(int(n), int(blocks), float(p_in), float(p_out), int(w_lo), int(w_hi),
+                                    int(seed)), with_truth)
+
+
+def sbm_10k(seed=0):
+    """n=10,000 in 100 blocks of 100, p_in=0.1, p_out=0.0006, unit weights."""
+    return sbm(10000, 100, 0.1, 0.0006, 1, 1, seed)
+
+
+def lfr(n=1 << 20, deg_exp=2.5, d_min=5, d_max=5000, com_exp=1.5, c_min=50, c_max=50000, mu=0.3, seed=1,
+        with_truth=False):
+    """LFR-style power-law graph (defaults: the n=2^20 benchmark shape)."""
+    return _take(_load().lvggen_lfr(int(n), float(deg_exp), int(d_min), int(d_max), float(com_exp), int(c_min),
+                                    int(c_max), float(mu), int(seed)), with_truth)
+
+
+def rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, w_lo=1, w_hi=16, seed=2):
+    """R-MAT graph (host generator; large scales use the device generator)."""
+    return _take(_load().lvggen_rmat(int(scale), int(edge_factor), float(a), float(b), float(c), int(w_lo),
+                                     int(w_hi), int(seed)))
+
+
+def batched_sbm_params(count, seed=3, n_lo=64, n_hi=200000):
+    """Per-graph SBM parameters of the batched shape: n log-uniform in
+    [n_lo, n_hi], 4-400 blocks, average degree uniform in [8, 32], 70% intra
+    edges, integer weights 1..4."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+        blocks = int(min(rng.integers(4, 401), max(1, n // 4)))
+        d = float(rng.uniform(8, 32))
+        s = n / blocks
+        p_in = min(1.0, 0.7 * d / max(s - 1, 1))
+        p_out = min(1.0, 0.3 * d / max(n - s, 1))
+        out.append(dict(n=n, blocks=blocks, p_in=p_in, p_out=p_out, w_lo=1, w_hi=4,
+                        seed=int(rng.integers(0, 2**62))))
+    return out

@@ -1,0 +1,233 @@
+"""Host-side API over liblvg: the reference's phase functions as methods.
+
+    lv = Louvain()                       # one context = one device arena + stream
+    lv.load_edges(src, dst, w, n)        # CalculateNeighbour + initCUDA
+    res = lv.run()                       # generate_dendogram
+    part = lv.partition()                # partitionAtLevel(last level)
+
+The per-phase methods keep the reference's names and argument meaning
+(LouvainCUDA/LouvainCPP.cpp:129-134): modularity (modularityCUDA),
+one_level (oneLevelCUDA), renumber (renumberCUDA), induce (inducedGraphCUDA).
+"""
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class LevelInfo:
+    n_vertices: int
+    n_entries: int
+    nnz: int
+    n_comms: int
+    passes: int
+    q_start: float
+    q_level: float
+    ms_passes: float
+
+
+@dataclass
+class RunResult:
+    n_levels: int
+    n_comms: int
+    q_final: float
+    pass_entries: int
+    status: int
+
+
+class Louvain:
+    def __init__(self, device=0, pass_min_gain=1e-7, level_min_gain=1e-7, max_passes=-1, max_levels=-1,
+                 arena_bytes=0, warp_max_degree=0, block_max_degree=0, passes_per_sync=0):
+        L = _lib.load()
+        cfg = _lib.LvgConfig()
+        L.lvg_config_default(ctypes.byref(cfg))
+        cfg.device = device
+        cfg.pass_min_gain = pass_min_gain
+        cfg.level_min_gain = level_min_gain
+        cfg.max_passes = max_passes
+        cfg.max_levels = max_levels
+        cfg.arena_bytes = arena_bytes
+        if warp_max_degree:
+            cfg.warp_max_degree = warp_max_degree
+        if block_max_degree:
+            cfg.block_max_degree = block_max_degree
+        if passes_per_sync:
+            cfg.passes_per_sync = passes_per_sync
+        self._L = L
+        h = ctypes.c_void_p()
+        _lib.check(None, L.lvg_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.n_vertices = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.lvg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, status):
+        _lib.check(self._h, status)
+
+    # ------------------------------------------------------------------ load
+    def load_edges(self, src, dst, w, n_vertices):
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        dst = np.ascontiguousarray(dst, dtype=np.int32)
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        if not (len(src) == len(dst) == len(w)):
+            raise ValueError("src, dst and w must have the same length")
+        self._check(self._L.lvg_load_edges(self._h, _p(src), _p(dst), _p(w), len(src), int(n_vertices)))
+        self.n_vertices = int(n_vertices)
+
+    def load_edges_ptr(self, src_ptr, dst_ptr, w_ptr, n_entries, n_vertices):
+        """Edge list in host memory given by raw pointers (e.g. pinned torch tensors)."""
+        self._check(self._L.lvg_load_edges(self._h, ctypes.c_void_p(src_ptr), ctypes.c_void_p(dst_ptr),
+                                            ctypes.c_void_p(w_ptr), int(n_entries), int(n_vertices)))
+        self.n_vertices = int(n_vertices)
+
+    def load_edges_device(self, src_ptr, dst_ptr, w_ptr, n_entries, n_vertices):
+        """Edge list already on the device (raw pointers, e.g. torch .data_ptr())."""
+        self._check(self._L.lvg_load_edges_device(self._h, ctypes.c_void_p(src_ptr), ctypes.c_void_p(dst_ptr),
+                                                   ctypes.c_void_p(w_ptr), int(n_entries), int(n_vertices)))
+        self.n_vertices = int(n_vertices)
+
+    def set_stream(self, stream_handle):
+        self._check(self._L.lvg_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
+
+    # ------------------------------------------------------------------ phases
+    def modularity(self):
+        q = ctypes.c_double()
+        self._check(self._L.lvg_modularity(self._h, ctypes.byref(q)))
+        return q.value
+
+    def one_level(self, lower):
+        q, p = ctypes.c_double(), ctypes.c_int32()
+        self._check(self._L.lvg_one_level(self._h, float(lower), ctypes.byref(q), ctypes.byref(p)))
+        return q.value, p.value
+
+    def renumber(self):
+        V = self.csr_shape()[0]
+        out = np.zeros(V, np.int32)
+        c = ctypes.c_int32()
+        self._check(self._L.lvg_renumber(self._h, _p(out), ctypes.byref(c)))
+        return out, c.value
+
+    def induce(self):
+        self._check(self._L.lvg_induce(self._h))
+
+    def run(self):
+        r = _lib.LvgResult()
+        self._check(self._L.lvg_run(self._h, ctypes.byref(r)))
+        return RunResult(r.n_levels, r.n_comms, r.q_final, r.pass_entries, r.status)
+
+    # ------------------------------------------------------------------ results
+    @property
+    def n_levels(self):
+        n = ctypes.c_int32()
+        self._check(self._L.lvg_num_levels(self._h, ctypes.byref(n)))
+        return n.value
+
+    def level_info(self, level):
+        i = _lib.LvgLevelInfo()
+        self._check(self._L.lvg_get_level_info(self._h, int(level), ctypes.byref(i)))
+        return LevelInfo(i.n_vertices, i.n_entries, i.nnz, i.n_comms, i.passes, i.q_start, i.q_level, i.ms_passes)
+
+    def level_partition(self, level):
+        out = np.zeros(self.level_info(level).n_vertices, np.int32)
+        self._check(self._L.lvg_get_level_partition(self._h, int(level), _p(out)))
+        return out
+
+    def level_labels(self, level):
+        out = np.zeros(self.level_info(level).n_vertices, np.int32)
+        self._check(self._L.lvg_get_level_labels(self._h, int(level), _p(out)))
+        return out
+
+    def partition(self, level=-1):
+        if level < 0:
+            level = self.n_levels - 1
+        out = np.zeros(self.n_vertices, np.int32)
+        self._check(self._L.lvg_get_partition(self._h, int(level), _p(out)))
+        return out
+
+    def modularity_fp64(self, part):
+        part = np.ascontiguousarray(part, np.int32)
+        q = ctypes.c_double()
+        self._check(self._L.lvg_modularity_fp64(self._h, _p(part), ctypes.byref(q)))
+        return q.value
+
+    def csr_shape(self):
+        V, nnz, m = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_double()
+        self._check(self._L.lvg_get_csr(self._h, ctypes.byref(V), ctypes.byref(nnz), ctypes.byref(m),
+                                        None, None, None, None, None, None))
+        return V.value, nnz.value, m.value
+
+    def csr(self):
+        V, nnz, m = self.csr_shape()
+        off = np.zeros(V + 1, np.int64)
+        col = np.zeros(nnz, np.int32)
+        w = np.zeros(nnz, np.float32)
+        k = np.zeros(V, np.float64)
+        loopw = np.zeros(V, np.float32)
+        hl = np.zeros(V, np.uint8)
+        Vc, nc, mc = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_double()
+        self._check(self._L.lvg_get_csr(self._h, ctypes.byref(Vc), ctypes.byref(nc), ctypes.byref(mc), _p(off),
+                                        _p(col), _p(w), _p(k), _p(loopw), _p(hl)))
+        return dict(V=V, nnz=nnz, m=m, off=off, col=col, w=w, k=k, loopw=loopw, has_loop=hl)
+
+    def set_communities(self, comm):
+        comm = np.ascontiguousarray(comm, np.int32)
+        self._check(self._L.lvg_set_communities(self._h, _p(comm)))
+
+    def move_decide(self):
+        V = self.csr_shape()[0]
+        nxt = np.zeros(V, np.int32)
+        cand = np.zeros(V, np.int32)
+        self._check(self._L.lvg_move_decide(self._h, _p(nxt), _p(cand)))
+        return nxt, cand
+
+    def pass_times(self):
+        n = ctypes.c_int32()
+        self._check(self._L.lvg_last_pass_times(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float32)
+        self._check(self._L.lvg_last_pass_times(self._h, _p(out), n.value, ctypes.byref(n)))
+        return out[:n.value]
+
+    def move_stats(self):
+        """(device ms of the move kernels, passes) of the last one-level phase(s)."""
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        self._check(self._L.lvg_move_stats(self._h, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def memory(self):
+        cap, peak = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self._L.lvg_memory(self._h, ctypes.byref(cap), ctypes.byref(peak)))
+        return cap.value, peak.value
+
+
+def kernel_launches():
+    """CUDA kernels launched by liblvg in this process."""
+    n = ctypes.c_int64()
+    _lib.check(None, _lib.load().lvg_kernel_launches(ctypes.byref(n)))
+    return n.value
+
+
+def count_partitions(part):
+    """countPartitions (LouvainCPP.cpp:116-127): 1 + max community id."""
+    part = np.ascontiguousarray(part, np.int32)
+    c = ctypes.c_int32()
+    _lib.check(None, _lib.load().lvg_count_partitions(_p(part), len(part), ctypes.byref(c)))
+    return c.value

@@ -1,0 +1,210 @@
+"""GPU parity: every phase of the CUDA path against the CPU oracle.
+
+Integer-valued weights make every sum exact, so the CUDA path must agree with
+the oracle bit for bit: CSR, degrees, loop weights, single-pass decisions,
+renumbered partitions, coarse graphs, pass counts and the FP64 Q values.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import undirected_to_lists
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def Louvain():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+    from louvaingpu_b200 import Louvain as L
+    return L
+
+
+def csr_equal(lv, oc):
+    c = lv.csr()
+    assert c["V"] == oc.V
+    assert c["nnz"] == oc.nnz
+    assert c["m"] == oc.m
+    np.testing.assert_array_equal(c["off"], oc.off)
+    np.testing.assert_array_equal(c["col"], oc.col)
+    np.testing.assert_array_equal(c["w"], oc.w)
+    np.testing.assert_array_equal(c["k"], oc.k)
+    np.testing.assert_array_equal(c["loopw"], oc.loopw)
+    np.testing.assert_array_equal(c["has_loop"], oc.has_loop)
+
+
+def run_equal(lv, res, orun, n, src, dst, w, oracle):
+    assert res.n_levels == len(orun.levels)
+    for l, ol in enumerate(orun.levels):
+        li = lv.level_info(l)
+        assert (li.n_vertices, li.n_entries, li.nnz, li.n_comms, li.passes) == \
+               (ol.n_vertices, ol.n_entries, ol.nnz, ol.n_comms, ol.passes), f"level {l}"
+        assert li.q_start == ol.q_start, f"level {l}"
+        assert li.q_level == ol.q, f"level {l}"
+        np.testing.assert_array_equal(lv.level_labels(l), ol.labels)
+        np.testing.assert_array_equal(lv.level_partition(l), ol.part)
+    np.testing.assert_array_equal(lv.partition(), orun.final)
+    q = oracle.modularity_fp64(n, src, dst, w, orun.final)
+    assert res.q_final == pytest.approx(q, abs=1e-9)
+
+
+def test_two_triangles_known_answer(Louvain, oracle):
+    with open(os.path.join(GOLDEN, "two_triangles.json")) as f:
+        g = json.load(f)
+    src, dst, w = undirected_to_lists(g["undirected_edges"])
+    with Louvain() as lv:
+        lv.load_edges(src, dst, w, g["n_vertices"])
+        res = lv.run()
+        assert res.n_levels == 2
+        for l, exp in enumerate(g["levels"]):
+            li = lv.level_info(l)
+            assert li.passes == exp["passes"] and li.n_comms == exp["n_comms"] and li.nnz == exp["nnz"]
+            assert li.q_level == pytest.approx(exp["q_level"], abs=1e-12)
+            assert lv.level_labels(l).tolist() == exp["labels"]
+            assert lv.level_partition(l).tolist() == exp["part"]
+        assert lv.partition().tolist() == g["final_partition"]
+        assert res.q_final == pytest.approx(g["final_modularity_fp64"], abs=1e-12)
+
+
+@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "hub"])
+def test_csr_build_bit_exact(Louvain, oracle, gen, case):
+    n, s, d, w = make_case(gen, case)
+    oc = oracle.Csr(n, s, d, w)
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        csr_equal(lv, oc)
+
+
+def make_case(gen, case):
+    rng = np.random.default_rng(7)
+    if case == "sbm_small":
+        return gen.sbm(2000, 20, 0.05, 0.002, 1, 1, seed=1)
+    if case == "weighted":
+        return gen.sbm(3000, 30, 0.05, 0.002, 1, 4, seed=2)
+    if case == "loops_zeros_isolated":
+        n = 500
+        m = 3000
+        s = rng.integers(0, n - 50, m).astype(np.int32)   # vertices >= 450 isolated
+        d = rng.integers(0, n - 50, m).astype(np.int32)
+        w = rng.integers(0, 4, m).astype(np.float32)       # zero weights and self loops included
+        return n, s, d, w
+    if case == "hub":
+        # a star hub of degree 12000 (global-table path) plus a block-bucket hub and SBM background
+        n, s, d, w = gen.sbm(20000, 40, 0.01, 0.0002, 1, 3, seed=3)
+        leaves = np.arange(1, 12001, dtype=np.int32)
+        mid = np.arange(13000, 13600, dtype=np.int32)
+        hs = np.concatenate([np.zeros(12000, np.int32), leaves, np.full(600, 12500, np.int32), mid])
+        hd = np.concatenate([leaves, np.zeros(12000, np.int32), mid, np.full(600, 12500, np.int32)])
+        hw = np.ones(len(hs), np.float32) * 2
+        return n, np.concatenate([s, hs]), np.concatenate([d, hd]), np.concatenate([w, hw])
+    raise ValueError(case)
+
+
+@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "hub"])
+def test_move_decisions_bit_exact(Louvain, oracle, gen, case):
+    n, s, d, w = make_case(gen, case)
+    oc = oracle.Csr(n, s, d, w)
+    rng = np.random.default_rng(11)
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        # singleton state, then a random clustered state
+        for comm in (np.arange(n, dtype=np.int32), rng.integers(0, n // 10, n).astype(np.int32)):
+            tot = np.zeros(n)
+            size = np.zeros(n, np.int32)
+            np.add.at(tot, comm, oc.k)
+            np.add.at(size, comm, 1)
+            exp_next, exp_cand, _ = oc.decide(comm, tot, size)
+            lv.set_communities(comm)
+            nxt, cand = lv.move_decide()
+            np.testing.assert_array_equal(nxt, exp_next)
+            np.testing.assert_array_equal(cand, exp_cand)
+
+
+@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "hub"])
+def test_full_run_bit_exact(Louvain, oracle, gen, case):
+    n, s, d, w = make_case(gen, case)
+    orun = oracle.Run(n, s, d, w)
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        res = lv.run()
+        run_equal(lv, res, orun, n, s, d, w, oracle)
+
+
+def test_sbm_10k_config(Louvain, oracle, gen):
+    """SBM n=10,000 config: level gain threshold 1e-6, bit-exact dendrogram."""
+    n, s, d, w = gen.sbm_10k(seed=0)
+    orun = oracle.Run(n, s, d, w, level_min_gain=1e-6)
+    with open(os.path.join(GOLDEN, "sbm10k_seed0.json")) as f:
+        g = json.load(f)
+    with Louvain(level_min_gain=1e-6) as lv:
+        lv.load_edges(s, d, w, n)
+        res = lv.run()
+        run_equal(lv, res, orun, n, s, d, w, oracle)
+        assert [lv.level_info(l).passes for l in range(res.n_levels)] == g["passes"]
+        assert res.q_final == pytest.approx(g["final_modularity_fp64"], abs=1e-9)
+
+
+def test_step_api_matches_run(Louvain, oracle, gen):
+    """modularity / one_level / renumber / induce called one by one as the
+    reference's driver does (LouvainCPP.cpp:334-501)."""
+    n, s, d, w = gen.sbm(3000, 30, 0.05, 0.002, 1, 1, seed=4)
+    orun = oracle.Run(n, s, d, w)
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        q0 = lv.modularity()
+        assert q0 == orun.levels[0].q_start
+        q, passes = lv.one_level(q0)
+        assert (q, passes) == (orun.levels[0].q, orun.levels[0].passes)
+        part, C = lv.renumber()
+        np.testing.assert_array_equal(part, orun.levels[0].part)
+        lv.induce()
+        q1, p1 = lv.one_level(q)
+        assert (q1, p1) == (orun.levels[1].q, orun.levels[1].passes)
+
+
+def test_lfr_full_size(Louvain, oracle, gen):
+    """LFR-style n=2^20 config: the dendrogram matches the oracle bit for bit
+    and the final Q lies within 1e-3."""
+    n, s, d, w = gen.lfr()
+    orun = oracle.Run(n, s, d, w)
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        res = lv.run()
+        run_equal(lv, res, orun, n, s, d, w, oracle)
+
+
+def test_invalid_input_is_an_error(Louvain):
+    from louvaingpu_b200 import LvgError
+    with Louvain() as lv:
+        with pytest.raises(LvgError):
+            lv.load_edges([0, 5], [5, 0], [1.0, 1.0], 3)        # id out of range
+        with pytest.raises(LvgError):
+            lv.load_edges([0, 1], [1, 0], [-1.0, 1.0], 3)       # negative weight
+        with pytest.raises(LvgError):
+            lv.load_edges([0, 1], [1, 0], [np.nan, 1.0], 3)     # non-finite weight
+        with pytest.raises(LvgError):
+            lv.one_level(0.0)                                   # nothing loaded
+
+
+def test_empty_graph(Louvain):
+    with Louvain() as lv:
+        lv.load_edges([], [], [], 5)
+        res = lv.run()
+        assert res.n_levels == 1
+        assert lv.partition().tolist() == [0, 1, 2, 3, 4]
+
+
+def test_pass_cap_reports_not_converged(Louvain, gen):
+    from louvaingpu_b200 import LvgError
+    n, s, d, w = gen.sbm(2000, 20, 0.05, 0.002, 1, 1, seed=1)
+    with Louvain(max_passes=1) as lv:
+        lv.load_edges(s, d, w, n)
+        with pytest.raises(LvgError) as e:
+            lv.run()
+        assert e.value.status == 4
