@@ -51,7 +51,7 @@ typedef struct {
   int32_t max_passes;      /* <0: unbounded like __PASS_MAX=-1 (OneLevelKernel.cu:424) */
   int32_t max_levels;      /* <0: unbounded */
   int64_t arena_bytes;     /* 0: sized from the level-0 graph at load */
-  int32_t warp_max_degree; /* vertices up to this degree use a warp-per-vertex table (0: default) */
+  int32_t tile_max_degree; /* vertices up to this degree are packed into shared-memory tiles (<= 512) */
   int32_t block_max_degree;/* up to this degree a block-per-vertex shared table; above, global tables */
   int32_t passes_per_sync; /* passes launched between host checks of convergence (0: default) */
   int32_t use_graphs;      /* capture the pass sequence of a level in a CUDA graph (1: default on) */

@@ -31,7 +31,7 @@ class LvgConfig(ctypes.Structure):
         ("max_passes", ctypes.c_int32),
         ("max_levels", ctypes.c_int32),
         ("arena_bytes", ctypes.c_int64),
-        ("warp_max_degree", ctypes.c_int32),
+        ("tile_max_degree", ctypes.c_int32),
         ("block_max_degree", ctypes.c_int32),
         ("passes_per_sync", ctypes.c_int32),
         ("use_graphs", ctypes.c_int32),

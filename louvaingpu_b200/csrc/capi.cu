@@ -62,6 +62,8 @@ struct lvg_ctx {
   std::vector<LevelRec> levels;
   std::vector<float> pass_ms;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  SideStreams side{};
+  bool have_side = false;
   std::vector<cudaEvent_t> mev;   // move-phase events, two per pass
   double move_ms = 0.0;
   int64_t move_passes = 0;
@@ -200,7 +202,7 @@ void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int
         c->mev.push_back(ev);
       }
       LVG_CUDA(cudaEventRecord(c->mev[e], s));
-      launch_moves(c->g, c->st, s);
+      launch_moves(c->g, c->st, s, &c->side);
       LVG_CUDA(cudaEventRecord(c->mev[e + 1], s));
       launch_commit(c->g, c->st, s);
       ++launched;
@@ -317,7 +319,7 @@ lvg_status lvg_config_default(lvg_config* cfg) {
   cfg->max_passes = -1;        // __PASS_MAX (OneLevelKernel.cu:424)
   cfg->max_levels = -1;
   cfg->arena_bytes = 0;
-  cfg->warp_max_degree = 128;
+  cfg->tile_max_degree = 512;
   cfg->block_max_degree = 4096;
   cfg->passes_per_sync = 4;
   cfg->use_graphs = 1;
@@ -332,9 +334,9 @@ lvg_status lvg_create(const lvg_config* cfg, lvg_ctx** out) {
   lvg_status s = guarded(c, [&] {
     if (cfg) c->cfg = *cfg;
     else lvg_config_default(&c->cfg);
-    require(c->cfg.warp_max_degree >= 0 && c->cfg.block_max_degree >= 0, LVG_ERR_INVALID_ARG,
+    require(c->cfg.tile_max_degree >= 0 && c->cfg.block_max_degree >= 0, LVG_ERR_INVALID_ARG,
             "bucket thresholds must be >= 0");
-    c->tune.warp_max = c->cfg.warp_max_degree > 0 ? std::min(c->cfg.warp_max_degree, 128) : 128;
+    c->tune.warp_max = c->cfg.tile_max_degree > 0 ? std::min(c->cfg.tile_max_degree, 512) : 512;
     c->tune.block_max = c->cfg.block_max_degree > 0 ? std::min(c->cfg.block_max_degree, 8192) : 4096;
     if (c->tune.block_max < c->tune.warp_max) c->tune.block_max = c->tune.warp_max;
     c->device = c->cfg.device;
@@ -346,6 +348,12 @@ lvg_status lvg_create(const lvg_config* cfg, lvg_ctx** out) {
     c->stream = c->own_stream;
     LVG_CUDA(cudaEventCreate(&c->ev0));
     LVG_CUDA(cudaEventCreate(&c->ev1));
+    for (int k = 0; k < 3; ++k) {
+      LVG_CUDA(cudaStreamCreateWithFlags(&c->side.side[k], cudaStreamNonBlocking));
+      LVG_CUDA(cudaEventCreateWithFlags(&c->side.join[k], cudaEventDisableTiming));
+    }
+    LVG_CUDA(cudaEventCreateWithFlags(&c->side.fork, cudaEventDisableTiming));
+    c->have_side = true;
   });
   if (s != LVG_OK) {
     lvg_destroy(c);
@@ -363,6 +371,13 @@ lvg_status lvg_destroy(lvg_ctx* c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (cudaEvent_t e : c->mev) cudaEventDestroy(e);
+  if (c->have_side) {
+    for (int k = 0; k < 3; ++k) {
+      cudaStreamDestroy(c->side.side[k]);
+      cudaEventDestroy(c->side.join[k]);
+    }
+    cudaEventDestroy(c->side.fork);
+  }
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return LVG_OK;
@@ -642,7 +657,7 @@ lvg_status lvg_move_decide(lvg_ctx* c, int32_t* next, int32_t* cand) {
     cudaStream_t s = c->stream;
     reset_ctl(c->st, 0.0, c->cfg.pass_min_gain, -1, s);
     clear_deltas(c->g, c->st, s);
-    launch_moves(c->g, c->st, s);
+    launch_moves(c->g, c->st, s, &c->side);
     if (next && V) LVG_CUDA(cudaMemcpyAsync(next, c->st.next, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, s));
     if (cand && V) LVG_CUDA(cudaMemcpyAsync(cand, c->st.cand, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, s));
     PassCtl h;

@@ -18,11 +18,16 @@
 #include "prims.cuh"
 
 namespace lvg {
+
+struct HubPartial {
+  double g, w;
+  int32_t c, n;
+};
+
 namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHubChunk = 4096;
-constexpr int kHubThreads = 512;
 constexpr int kNone = INT_MAX;
 
 __device__ __forceinline__ uint32_t hash_c(int32_t c, int logT) {
@@ -121,32 +126,103 @@ __global__ void csr_emit_kernel(const uint64_t* keys, const float* vals, int64_t
   if (seg_warp_last<int64_t>(r, valid) && r >= 0) atomicAdd(&wsum[r], s);
 }
 
+// Sort-free build: a level list that is strictly sorted by (src, dst) and
+// symmetric with bitwise-equal weights doubles into each entry twice, so the
+// merged CSR row of u is its list row without the self loop, weights 2w.
+__global__ void row_count_kernel(const int32_t* src, int64_t E, int64_t* rowcnt) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd((unsigned long long*)&rowcnt[src[e]], 1ull);
+}
+
+enum : uint32_t { kNotSorted = 1u, kNotSymmetric = 2u };
+
+__global__ void list_check_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                  const int64_t* rowstart, uint32_t* flags) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    int32_t u = src[e], v = dst[e];
+    if (e + 1 < E) {
+      int32_t u2 = src[e + 1], v2 = dst[e + 1];
+      if (!(u2 > u || (u2 == u && v2 > v))) atomicOr(flags, kNotSorted);
+    }
+    if (u != v) {
+      int64_t lo = rowstart[v], hi = rowstart[v + 1] - 1;
+      bool found = false;
+      while (lo <= hi) {
+        int64_t mid = (lo + hi) >> 1;
+        int32_t x = dst[mid];
+        if (x == u) { found = __float_as_uint(w[mid]) == __float_as_uint(w[e]); break; }
+        if (x < u) lo = mid + 1; else hi = mid - 1;
+      }
+      if (!found) atomicOr(flags, kNotSymmetric);
+    }
+  }
+}
+
+__global__ void nonloop_flag_kernel(const int32_t* src, const int32_t* dst, int64_t E, uint32_t* flag) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
+    flag[e] = src[e] != dst[e] ? 1u : 0u;
+}
+
+__global__ void csr_fast_emit_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                     const uint32_t* pos, int32_t* col, float* cw, double* k, float* loopw,
+                                     uint8_t* has_loop) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool valid = e < E;
+  int64_t u = valid ? src[e] : -1;
+  int32_t v = valid ? dst[e] : -1;
+  float x = valid ? w[e] : 0.0f;
+  bool loop = valid && u == v;
+  if (valid && !loop) {
+    uint32_t p = pos[e];
+    col[p] = v;
+    cw[p] = __double2float_rn(__dadd_rn((double)x, (double)x));
+  }
+  if (loop) { loopw[u] = x; has_loop[u] = 1; }
+  float f = x == 0.0f ? 1.0f : x;             // InitKernel.cu:165-170, both copies of the entry
+  if (loop) f *= 2.0f;
+  double dv = valid ? __dadd_rn((double)f, (double)f) : 0.0;
+  double sum = seg_warp_sum<int64_t>(dv, u);
+  if (seg_warp_last<int64_t>(u, valid)) atomicAdd(&k[u], sum);
+}
+
+__global__ void row_off_kernel(const int64_t* rowstart, const uint32_t* pos, int32_t V, int64_t* off) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u <= V; u += (int64_t)gridDim.x * blockDim.x)
+    off[u] = pos[rowstart[u]];
+}
+
 __global__ void to_float_kernel(const double* x, float* y, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = __double2float_rn(x[i]);
 }
 
 // ------------------------------------------------------------------ buckets
-__device__ __forceinline__ int bucket_of(int32_t i, const int64_t* off, const double* k, int32_t wmax,
+// Degree classes: 1-4, 5-8, 9-16, 17-32 lanes per vertex (group kernels),
+// 33..tile_max (tiles), ..block_max (block per vertex), above (hubs).
+__device__ __forceinline__ int bucket_of(int32_t i, const int64_t* off, const double* k, int32_t tmax,
                                          int32_t bmax) {
-  if (!(k[i] > 0.0)) return 3;  // no entry in the doubled list: never moves
+  if (!(k[i] > 0.0)) return kNumBuckets;  // no entry in the doubled list: never moves
   int64_t d = off[i + 1] - off[i];
-  return d <= wmax ? 0 : (d <= bmax ? 1 : 2);
+  if (d <= 4) return kB4;
+  if (d <= 8) return kB8;
+  if (d <= 16) return kB16;
+  if (d <= 32) return kB32;
+  if (d <= tmax) return kBTile;
+  return d <= bmax ? kBBlock : kBHub;
 }
 
 __global__ void __launch_bounds__(kThreads) bucket_count_kernel(int32_t V, const int64_t* off, const double* k,
-                                                                int32_t wmax, int32_t bmax, uint32_t* cnt,
+                                                                int32_t tmax, int32_t bmax, uint32_t* cnt,
                                                                 int64_t nblk) {
-  uint32_t c[3] = {0, 0, 0};
+  uint32_t c[kNumBuckets] = {};
   int64_t base = (int64_t)blockIdx.x * 2048 + (int64_t)threadIdx.x * 8;
   for (int j = 0; j < 8; ++j) {
     int64_t i = base + j;
     if (i < V) {
-      int b = bucket_of((int32_t)i, off, k, wmax, bmax);
-      if (b < 3) c[b]++;
+      int b = bucket_of((int32_t)i, off, k, tmax, bmax);
+      if (b < kNumBuckets) c[b]++;
     }
   }
-  for (int b = 0; b < 3; ++b) {
+  for (int b = 0; b < kNumBuckets; ++b) {
     uint32_t tot;
     block_exclusive_scan256<uint32_t>(c[b], &tot);
     if (threadIdx.x == 0) cnt[b * nblk + blockIdx.x] = tot;
@@ -154,25 +230,25 @@ __global__ void __launch_bounds__(kThreads) bucket_count_kernel(int32_t V, const
 }
 
 __global__ void __launch_bounds__(kThreads) bucket_scatter_kernel(int32_t V, const int64_t* off, const double* k,
-                                                                  int32_t wmax, int32_t bmax,
+                                                                  int32_t tmax, int32_t bmax,
                                                                   const uint32_t* offs, int64_t nblk,
                                                                   int32_t* list) {
   int64_t base = (int64_t)blockIdx.x * 2048 + (int64_t)threadIdx.x * 8;
   int8_t bid[8];
-  uint32_t c[3] = {0, 0, 0};
+  uint32_t c[kNumBuckets] = {};
   for (int j = 0; j < 8; ++j) {
     int64_t i = base + j;
-    bid[j] = i < V ? (int8_t)bucket_of((int32_t)i, off, k, wmax, bmax) : (int8_t)3;
-    if (bid[j] < 3) c[bid[j]]++;
+    bid[j] = i < V ? (int8_t)bucket_of((int32_t)i, off, k, tmax, bmax) : (int8_t)kNumBuckets;
+    if (bid[j] < kNumBuckets) c[bid[j]]++;
   }
-  uint32_t pre[3];
-  for (int b = 0; b < 3; ++b) {
+  uint32_t pre[kNumBuckets];
+  for (int b = 0; b < kNumBuckets; ++b) {
     uint32_t tot;
     pre[b] = block_exclusive_scan256<uint32_t>(c[b], &tot) + offs[b * nblk + blockIdx.x];
   }
   for (int j = 0; j < 8; ++j) {
     int b = bid[j];
-    if (b < 3) list[pre[b]++] = (int32_t)(base + j);
+    if (b < kNumBuckets) list[pre[b]++] = (int32_t)(base + j);
   }
 }
 
@@ -284,58 +360,7 @@ __device__ __forceinline__ bool table_insert(int32_t* keys, double* vals, int lo
   return false;
 }
 
-// Warp per vertex, neighbour-community table in shared memory.
-constexpr int kWarpSlots = 256;
-__global__ void __launch_bounds__(kThreads) move_warp_kernel(MoveArgs P) {
-  __shared__ int32_t skeys[kThreads / 32][kWarpSlots];
-  __shared__ double svals[kThreads / 32][kWarpSlots];
-  if (P.ctl->done) return;
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int32_t* keys = skeys[w];
-  double* vals = svals[w];
-  for (int s = lane; s < kWarpSlots; s += 32) { keys[s] = -1; vals[s] = 0.0; }
-  __syncwarp();
-  bool overflow = false;
-  for (int64_t item = (int64_t)blockIdx.x * (kThreads / 32) + w; item < P.n;
-       item += (int64_t)gridDim.x * (kThreads / 32)) {
-    int32_t i = P.list[item];
-    int32_t own = P.comm[i];
-    int64_t beg = P.off[i], end = P.off[i + 1];
-    int logT = max(5, ceil_log2(2 * (end - beg)));
-    int T = 1 << logT;
-    bool sawown = false;
-    for (int64_t e = beg + lane; e < end; e += 32) {
-      int32_t c = P.comm[P.col[e]];
-      sawown |= (c == own);
-      if (!table_insert(keys, vals, logT, c, (double)P.cw[e])) overflow = true;
-    }
-    __syncwarp();
-    double kf = P.kfrac[i];
-    double bg = 0.0, bw = 0.0;
-    int32_t bc = kNone;
-    int nocc = 0;
-    for (int s = lane; s < T; s += 32) {
-      int32_t c = keys[s];
-      if (c >= 0) {
-        ++nocc;
-        consider(c, vals[s], kf, P.tot, bg, bc, bw);
-        keys[s] = -1;
-        vals[s] = 0.0;
-      }
-    }
-    warp_best(bg, bc, bw);
-    nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
-    sawown = __any_sync(0xffffffffu, sawown);
-    if (lane == 0) {
-      int32_t nseg = nocc + ((P.has_loop[i] && !sawown) ? 1 : 0);
-      apply_decision(P, i, own, bc, bw, nseg);
-    }
-    __syncwarp();
-  }
-  if (__any_sync(0xffffffffu, overflow) && lane == 0) atomicOr(&P.ctl->err, kErrProbe);
-}
-
-// Block per vertex, table of up to kBlockSlots slots in dynamic shared memory.
+// Block per vertex (degree up to block_max), table in dynamic shared memory.
 __global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int maxLog) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double rg[kThreads / 32], rw[kThreads / 32];
@@ -396,6 +421,269 @@ __global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int ma
   if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
 }
 
+// --------------------------------------------------------------- group kernels
+// Degree <= 32: G lanes per vertex (G = 4, 8, 16, 32), one CSR entry per lane,
+// 32/G vertices per warp.  __match_any_sync on (group, community) finds the
+// entries of equal communities; they add their weights into the slot of the
+// lowest such lane (shared memory), and a butterfly inside the group picks the
+// best community.  No table, no block barrier.
+template <int G>
+__device__ __forceinline__ void group_best(double& bg, int32_t& bc, double& bw) {
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = G / 2; o >= 1; o >>= 1) {
+    double g = __shfl_xor_sync(full, bg, o);
+    int32_t c = __shfl_xor_sync(full, bc, o);
+    double w = __shfl_xor_sync(full, bw, o);
+    if (better(g, c, bg, bc)) { bg = g; bc = c; bw = w; }
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kThreads) move_group_kernel(MoveArgs P) {
+  __shared__ double ssum[kThreads];
+  if (P.ctl->done) return;
+  constexpr int VPW = 32 / G;
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int gi = lane / G, gl = lane % G;
+  const unsigned gmask = G == 32 ? full : (((1u << G) - 1u) << (gi * G));
+  double* my = &ssum[threadIdx.x & ~31];
+  const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
+  for (int64_t base = warp * VPW; base < P.n; base += nwarps * VPW) {
+    const int64_t item = base + gi;
+    const bool act = item < P.n;
+    int32_t i = 0, own = -1, deg = 0;
+    int64_t beg = 0;
+    if (act) {
+      i = P.list[item];
+      beg = P.off[i];
+      deg = (int32_t)(P.off[i + 1] - beg);
+      own = P.comm[i];
+    }
+    const bool valid = gl < deg;
+    int32_t c = -1;
+    float w = 0.0f;
+    if (valid) { c = P.col[beg + gl]; w = P.cw[beg + gl]; }
+    if (valid) c = P.comm[c];
+    unsigned long long key = valid ? (((unsigned long long)gi << 32) | (uint32_t)c)
+                                   : (0xFFFFFFFF00000000ull | (unsigned)lane);
+    unsigned peers = __match_any_sync(full, key);
+    int leader = __ffs(peers) - 1;
+    my[lane] = 0.0;
+    __syncwarp();
+    if (valid) atomicAdd(&my[leader], (double)w);
+    __syncwarp();
+    const bool isl = valid && leader == lane;
+    unsigned bl = __ballot_sync(full, isl) & gmask;
+    unsigned bo = __ballot_sync(full, valid && c == own) & gmask;
+    double bg = 0.0, bw = 0.0;
+    int32_t bc = kNone;
+    if (isl) consider(c, my[lane], P.kfrac[i], P.tot, bg, bc, bw);
+    group_best<G>(bg, bc, bw);
+    if (act && gl == 0) {
+      int32_t nseg = __popc(bl) + ((P.has_loop[i] && bo == 0) ? 1 : 0);
+      apply_decision(P, i, own, bc, bw, nseg);
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- tile kernel
+// Degrees 33..kTileMaxDeg are packed, in index order, into tiles of about
+// kTileCost cost units (degree + 4 per vertex).  One block hashes every
+// (vertex, neighbour community) pair of its tile into a shared-memory table
+// -- all entry loads of the tile independent of each other -- and keeps the
+// claimed slots in a list, then resolves each vertex's best community: the
+// largest gain bits (positive doubles order like their bit patterns), then the
+// smallest community among equal gains.
+constexpr int kTileMaxDeg = 512;
+constexpr int kTileCost = 1536;
+constexpr int kTileVtx = 48;          // >= kTileCost / (33 + 4) + 1
+constexpr int kTileSlotsLog = 12;     // 4096 slots for <= kTileCost + kTileMaxDeg + 4 entries
+constexpr int kTileSlots = 1 << kTileSlotsLog;
+constexpr unsigned long long kEmptyKey = ~0ull;
+static_assert(kTileVtx >= kTileCost / 37 + 1, "tile vertex arrays too small");
+static_assert(kTileCost + kTileMaxDeg + 4 <= (1 << 11) + 8, "tile table load above one half");
+
+template <typename Acc>
+struct TileSmem {
+  unsigned long long key[kTileSlots];
+  Acc val[kTileSlots];
+  uint16_t claimed[kTileSlots];
+  int64_t beg[kTileVtx];
+  double kf[kTileVtx];
+  double bestw[kTileVtx];
+  unsigned long long bestg[kTileVtx];
+  int32_t vid[kTileVtx];
+  int32_t own[kTileVtx];
+  int32_t rowbeg[kTileVtx + 1];
+  int32_t bestc[kTileVtx];
+  int32_t nseg[kTileVtx];
+  int32_t flags[kTileVtx];   // bit0 saw own community, bit1 has self loop
+  int32_t nclaimed;
+};
+
+template <typename Acc>
+__device__ __forceinline__ void tile_insert(TileSmem<Acc>& S, unsigned long long k, Acc w, bool& overflow) {
+  uint32_t h = (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> (64 - kTileSlotsLog));
+  for (int p = 0; p < kTileSlots; ++p) {
+    unsigned long long prev = atomicCAS(&S.key[h], kEmptyKey, k);
+    if (prev == kEmptyKey) S.claimed[atomicAdd(&S.nclaimed, 1)] = (uint16_t)h;
+    if (prev == kEmptyKey || prev == k) { atomicAdd(&S.val[h], w); return; }
+    h = (h + 1) & (kTileSlots - 1);
+  }
+  overflow = true;
+}
+
+__device__ __forceinline__ int tile_find(const int32_t* rowbeg, int nv, int q) {
+  int lo = 0, hi = nv - 1;
+  while (lo < hi) {            // last j with rowbeg[j] <= q
+    int mid = (lo + hi + 1) >> 1;
+    if (rowbeg[mid] <= q) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename Acc>
+__global__ void __launch_bounds__(kThreads) move_tile_kernel(MoveArgs P, const int32_t* tile_start, int64_t ntiles) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  TileSmem<Acc>& S = *reinterpret_cast<TileSmem<Acc>*>(smem);
+  if (P.ctl->done) return;
+  for (int sl = threadIdx.x; sl < kTileSlots; sl += kThreads) { S.key[sl] = kEmptyKey; S.val[sl] = Acc(0); }
+  if (threadIdx.x == 0) S.nclaimed = 0;
+  bool overflow = false;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int vb = tile_start[t];
+    const int nv = tile_start[t + 1] - vb;
+    int deg = 0;
+    if (threadIdx.x < nv) {
+      int32_t i = P.list[vb + threadIdx.x];
+      int64_t b = P.off[i];
+      deg = (int)(P.off[i + 1] - b);
+      S.vid[threadIdx.x] = i;
+      S.beg[threadIdx.x] = b;
+      S.own[threadIdx.x] = P.comm[i];
+      S.kf[threadIdx.x] = P.kfrac[i];
+      S.flags[threadIdx.x] = P.has_loop[i] ? 2 : 0;
+      S.bestg[threadIdx.x] = 0ull;
+      S.bestc[threadIdx.x] = kNone;
+      S.nseg[threadIdx.x] = 0;
+    }
+    int ne;
+    int pre = block_exclusive_scan256<int>(deg, &ne);
+    if (threadIdx.x < nv) S.rowbeg[threadIdx.x] = pre;
+    if (threadIdx.x == 0) S.rowbeg[nv] = ne;
+    __syncthreads();
+    for (int q0 = threadIdx.x; q0 < ne; q0 += 4 * kThreads) {
+      int jj[4];
+      int32_t cc[4];
+      float ww[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        int q = q0 + u * kThreads;
+        jj[u] = -1;
+        if (q < ne) {
+          int j = tile_find(S.rowbeg, nv, q);
+          int64_t e = S.beg[j] + (q - S.rowbeg[j]);
+          jj[u] = j;
+          cc[u] = P.col[e];
+          ww[u] = P.cw[e];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (jj[u] >= 0) cc[u] = P.comm[cc[u]];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (jj[u] >= 0) {
+          int j = jj[u];
+          if (cc[u] == S.own[j]) atomicOr(&S.flags[j], 1);
+          unsigned long long k = ((unsigned long long)(uint32_t)j << 32) | (uint32_t)cc[u];
+          tile_insert(S, k, (Acc)ww[u], overflow);
+        }
+      }
+    }
+    __syncthreads();
+    const int nc = S.nclaimed;
+    for (int x = threadIdx.x; x < nc; x += kThreads) {       // count, best gain bits
+      int sl = S.claimed[x];
+      unsigned long long k = S.key[sl];
+      int j = (int)(k >> 32);
+      int32_t c = (int32_t)(uint32_t)k;
+      atomicAdd(&S.nseg[j], 1);
+      double W = (double)S.val[sl];
+      if (W != 0.0) {
+        double g = __dsub_rn(W, __dmul_rn(P.tot[c], S.kf[j]));
+        if (g > 0.0) atomicMax(&S.bestg[j], (unsigned long long)__double_as_longlong(g));
+      }
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < nc; x += kThreads) {       // smallest community among the best gains
+      int sl = S.claimed[x];
+      unsigned long long k = S.key[sl];
+      int j = (int)(k >> 32);
+      int32_t c = (int32_t)(uint32_t)k;
+      double W = (double)S.val[sl];
+      if (W != 0.0 && S.bestg[j] != 0ull) {
+        double g = __dsub_rn(W, __dmul_rn(P.tot[c], S.kf[j]));
+        if ((unsigned long long)__double_as_longlong(g) == S.bestg[j]) atomicMin(&S.bestc[j], c);
+      }
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < nc; x += kThreads) {       // weight to the winner; clear the table
+      int sl = S.claimed[x];
+      unsigned long long k = S.key[sl];
+      int j = (int)(k >> 32);
+      int32_t c = (int32_t)(uint32_t)k;
+      if (c == S.bestc[j]) S.bestw[j] = (double)S.val[sl];
+      S.key[sl] = kEmptyKey;
+      S.val[sl] = Acc(0);
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+      int j = threadIdx.x;
+      int f = S.flags[j];
+      int32_t nseg = S.nseg[j] + (((f & 2) && !(f & 1)) ? 1 : 0);
+      int32_t bc = S.bestc[j];
+      apply_decision(P, S.vid[j], S.own[j], bc, bc == kNone ? 0.0 : S.bestw[j], nseg);
+    }
+    if (threadIdx.x == 0) S.nclaimed = 0;
+    __syncthreads();
+  }
+  if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
+}
+
+// Tile boundaries: vertex j of the tile bucket belongs to tile
+// floor(cumcost_j / kTileCost), cost = degree + 4, so a tile holds at most
+// kTileCost / 37 + 1 vertices and kTileCost + kTileMaxDeg + 4 entries.
+__global__ void tile_cost_kernel(const int32_t* list, int64_t n, const int64_t* off, int64_t* cost) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    int32_t i = list[j];
+    cost[j] = off[i + 1] - off[i] + 4;
+  }
+}
+
+__global__ void tile_start_kernel(const int64_t* cum, int64_t n, int32_t* tile_start) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    int64_t t = cum[j] / kTileCost;
+    if (j == 0 || cum[j - 1] / kTileCost != t) tile_start[t] = (int32_t)j;
+    if (j == n - 1) tile_start[t + 1] = (int32_t)n;
+  }
+}
+
+// Integral weights with small degrees allow an exact int32 accumulator.
+__global__ void int_weights_kernel(const float* cw, int64_t nnz, const double* k, int32_t V, uint32_t* notint) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += stride) {
+    float x = cw[e];
+    if (x != truncf(x)) atomicOr(notint, 1u);
+  }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += stride)
+    if (!(k[i] < 1073741824.0)) atomicOr(notint, 1u);
+}
+
 // Hubs: chunks of a hub's row insert into the hub's global table ...
 struct HubArgs {
   const int32_t* hubs;
@@ -428,28 +716,34 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(MoveArgs P, HubArg
   if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
 }
 
-// ... then one block per hub scans its table, decides and clears it.
-__global__ void __launch_bounds__(kHubThreads) hub_decide_kernel(MoveArgs P, HubArgs H) {
-  __shared__ double rg[kHubThreads / 32], rw[kHubThreads / 32];
-  __shared__ int32_t rc[kHubThreads / 32], rn[kHubThreads / 32];
+// ... then blocks scan 8192-slot segments of the hub tables (best candidate,
+// occupancy, clearing the slots) and one thread per hub combines its segments
+// in order and decides.
+constexpr int kHubSeg = 8192;
+
+__global__ void __launch_bounds__(kThreads) hub_scan_kernel(MoveArgs P, HubArgs H, const int32_t* seg_hub,
+                                                            const int64_t* seg_beg, HubPartial* part) {
+  __shared__ double rg[kThreads / 32], rw[kThreads / 32];
+  __shared__ int32_t rc[kThreads / 32], rn[kThreads / 32];
   if (P.ctl->done) return;
-  int32_t h = blockIdx.x;
+  int32_t h = seg_hub[blockIdx.x];
   int32_t i = H.hubs[h];
-  int32_t own = P.comm[i];
+  int64_t T = (int64_t)1 << H.tlog[h];
+  int64_t b0 = seg_beg[blockIdx.x];
+  int64_t b1 = min(b0 + (int64_t)kHubSeg, T);
   int32_t* keys = H.keys + H.toff[h];
   double* vals = H.vals + H.toff[h];
-  int64_t T = (int64_t)1 << H.tlog[h];
   double kf = P.kfrac[i];
   double bg = 0.0, bw = 0.0;
   int32_t bc = kNone;
   int nocc = 0;
-  for (int64_t s = threadIdx.x; s < T; s += kHubThreads) {
-    int32_t c = keys[s];
+  for (int64_t sl = b0 + threadIdx.x; sl < b1; sl += kThreads) {
+    int32_t c = keys[sl];
     if (c >= 0) {
       ++nocc;
-      consider(c, vals[s], kf, P.tot, bg, bc, bw);
-      keys[s] = -1;
-      vals[s] = 0.0;
+      consider(c, vals[sl], kf, P.tot, bg, bc, bw);
+      keys[sl] = -1;
+      vals[sl] = 0.0;
     }
   }
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -461,15 +755,33 @@ __global__ void __launch_bounds__(kHubThreads) hub_decide_kernel(MoveArgs P, Hub
     double g = rg[0], ww = rw[0];
     int32_t c = rc[0];
     int n = rn[0];
-    for (int k2 = 1; k2 < kHubThreads / 32; ++k2) {
+    for (int k2 = 1; k2 < kThreads / 32; ++k2) {
       if (better(rg[k2], rc[k2], g, c)) { g = rg[k2]; c = rc[k2]; ww = rw[k2]; }
       n += rn[k2];
     }
-    bool sw = H.sawown[h] != 0;
-    H.sawown[h] = 0;
-    int32_t nseg = n + ((P.has_loop[i] && !sw) ? 1 : 0);
-    apply_decision(P, i, own, c, ww, nseg);
+    part[blockIdx.x] = HubPartial{g, ww, c, n};
   }
+}
+
+__global__ void hub_decide_kernel(MoveArgs P, HubArgs H, const int32_t* hub_seg0, const HubPartial* part,
+                                  int64_t nhub) {
+  if (P.ctl->done) return;
+  int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (h >= nhub) return;
+  int32_t i = H.hubs[h];
+  int32_t own = P.comm[i];
+  double g = 0.0, ww = 0.0;
+  int32_t c = kNone;
+  int n = 0;
+  for (int32_t sg = hub_seg0[h]; sg < hub_seg0[h + 1]; ++sg) {
+    HubPartial q = part[sg];
+    if (better(q.g, q.c, g, c)) { g = q.g; c = q.c; ww = q.w; }
+    n += q.n;
+  }
+  bool sw = H.sawown[h] != 0;
+  H.sawown[h] = 0;
+  int32_t nseg = n + ((P.has_loop[i] && !sw) ? 1 : 0);
+  apply_decision(P, i, own, c, ww, nseg);
 }
 
 // ------------------------------------------------------------------ commit + Q
@@ -685,6 +997,32 @@ __global__ void run_sum_kernel(const uint64_t* keys, const float* vals, int64_t 
 }
 
 // ------------------------------------------------------------------ modularity
+// Community strength Kc (both endpoints of every entry) and internal weight
+// Ain (2w for entries inside one community).  Few communities: block-private
+// shared-memory sums flushed once per block; many: global atomics.
+constexpr int kNmSmemMax = 4096;
+__global__ void __launch_bounds__(kThreads) nm_accum_smem_kernel(const int32_t* src, const int32_t* dst,
+                                                                 const float* w, int64_t E, const int32_t* part,
+                                                                 int32_t C, double* Kc, double* Ain) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* sK = reinterpret_cast<double*>(smem);
+  double* sA = sK + C;
+  for (int c = threadIdx.x; c < 2 * C; c += kThreads) sK[c] = 0.0;
+  __syncthreads();
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    double x = (double)w[e];
+    int32_t a = part[src[e]], b = part[dst[e]];
+    atomicAdd(&sK[a], x);
+    atomicAdd(&sK[b], x);
+    if (a == b) atomicAdd(&sA[a], 2.0 * x);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += kThreads) {
+    if (sK[c] != 0.0) atomicAdd(&Kc[c], sK[c]);
+    if (sA[c] != 0.0) atomicAdd(&Ain[c], sA[c]);
+  }
+}
+
 __global__ void nm_accum_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
                                 const int32_t* part, double* Kc, double* Ain) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
@@ -709,7 +1047,7 @@ __global__ void compose_kernel(int32_t* composed, const int32_t* part_level, int
     composed[i] = part_level[composed[i]];
 }
 
-unsigned sm_grid(int64_t n, int threads) {
+int sm_count() {
   static int sms = 0;
   if (!sms) {
     int dev = 0;
@@ -717,6 +1055,11 @@ unsigned sm_grid(int64_t n, int threads) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (sms <= 0) sms = 148;
   }
+  return sms;
+}
+
+unsigned sm_grid(int64_t n, int threads) {
+  int sms = sm_count();
   int64_t g = (n + threads - 1) / threads;
   int64_t cap = (int64_t)sms * 16;
   if (g > cap) g = cap;
@@ -759,6 +1102,44 @@ bool validate_edges(const int32_t* src, const int32_t* dst, const float* w, int6
   return h == 0;
 }
 
+// Sort-free CSR build; returns false (and builds nothing) unless the level
+// list is strictly sorted and symmetric.
+static bool build_csr_fast(LevelGraph& g, Arena& a, cudaStream_t s) {
+  const int32_t V = g.V;
+  const int64_t E = g.E;
+  if (E >= ((int64_t)1 << 32) - 1) return false;
+  HiScope hs(a);
+  int64_t* rowstart = a.hi_n<int64_t>(V + 1);
+  uint32_t* flags = a.hi_n<uint32_t>(1);
+  LVG_CUDA(cudaMemsetAsync(rowstart, 0, sizeof(int64_t) * (V + 1), s));
+  LVG_CUDA(cudaMemsetAsync(flags, 0, sizeof(uint32_t), s));
+  row_count_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, E, rowstart);
+  LVG_LAUNCH();
+  scan_i64(rowstart, rowstart, V, a, s);
+  list_check_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, g.w, E, rowstart, flags);
+  LVG_LAUNCH();
+  uint32_t h = 0;
+  LVG_CUDA(cudaMemcpyAsync(&h, flags, sizeof h, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  if (h != 0) return false;
+  uint32_t* pos = a.hi_n<uint32_t>(E + 1);
+  nonloop_flag_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, E, pos);
+  LVG_LAUNCH();
+  scan_u32(pos, pos, E, a, s);
+  uint32_t nnz = 0;
+  LVG_CUDA(cudaMemcpyAsync(&nnz, pos + E, sizeof nnz, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  g.nnz = nnz;
+  g.col = a.lo_n<int32_t>(nnz);
+  g.cw = a.lo_n<float>(nnz);
+  csr_fast_emit_kernel<<<grid_for(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, g.w, E, pos, g.col, g.cw, g.k,
+                                                                    g.loopw, g.has_loop);
+  LVG_LAUNCH();
+  row_off_kernel<<<sm_grid(V + 1, kThreads), kThreads, 0, s>>>(rowstart, pos, V, g.off);
+  LVG_LAUNCH();
+  return true;
+}
+
 void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
   const int32_t V = g.V;
   const int64_t E = g.E;
@@ -775,7 +1156,8 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
   LVG_CUDA(cudaMemsetAsync(g.loopw, 0, sizeof(float) * std::max<int32_t>(V, 1), s));
   LVG_CUDA(cudaMemsetAsync(g.has_loop, 0, std::max<int32_t>(V, 1), s));
   tree_sum_f32(g.w, E, d_m, a, s);                                  // NeighbourCompute.cu:46
-  {
+  g.sorted_symmetric = E > 0 && build_csr_fast(g, a, s);
+  if (!g.sorted_symmetric) {
     HiScope hs(a);
     const int B = std::max(1, bits_for(V));
     uint64_t* k0 = a.hi_n<uint64_t>(n);
@@ -802,7 +1184,6 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
     scan_i64(rowcnt, g.off, V, a, s);
     int64_t nnz = 0;
     LVG_CUDA(cudaMemcpyAsync(&nnz, g.off + V, sizeof nnz, cudaMemcpyDeviceToHost, s));
-    LVG_CUDA(cudaMemcpyAsync(&g.m, d_m, sizeof(double), cudaMemcpyDeviceToHost, s));
     LVG_CUDA(cudaStreamSynchronize(s));
     g.nnz = nnz;
     // exact CSR on the low end
@@ -819,34 +1200,70 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
       LVG_LAUNCH();
     }
   }
+  LVG_CUDA(cudaMemcpyAsync(&g.m, d_m, sizeof(double), cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
   // degree buckets (stable by vertex index)
   g.blist = a.lo_n<int32_t>(V);
   {
     HiScope hs(a);
     int64_t nblk = (V + 2047) / 2048;
     if (nblk == 0) nblk = 1;
-    uint32_t* cnt = a.hi_n<uint32_t>(3 * nblk + 1);
+    uint32_t* cnt = a.hi_n<uint32_t>(kNumBuckets * nblk + 1);
     bucket_count_kernel<<<(unsigned)nblk, kThreads, 0, s>>>(V, g.off, g.k, t.warp_max, t.block_max, cnt, nblk);
     LVG_LAUNCH();
-    std::vector<uint32_t> host_cnt(3 * nblk);
-    LVG_CUDA(cudaMemcpyAsync(host_cnt.data(), cnt, sizeof(uint32_t) * 3 * nblk, cudaMemcpyDeviceToHost, s));
-    scan_u32(cnt, cnt, 3 * nblk, a, s);
+    std::vector<uint32_t> host_cnt(kNumBuckets * nblk);
+    LVG_CUDA(cudaMemcpyAsync(host_cnt.data(), cnt, sizeof(uint32_t) * kNumBuckets * nblk, cudaMemcpyDeviceToHost,
+                             s));
+    scan_u32(cnt, cnt, kNumBuckets * nblk, a, s);
     bucket_scatter_kernel<<<(unsigned)nblk, kThreads, 0, s>>>(V, g.off, g.k, t.warp_max, t.block_max, cnt, nblk,
                                                               g.blist);
     LVG_LAUNCH();
     LVG_CUDA(cudaStreamSynchronize(s));
-    for (int b = 0; b < 3; ++b) {
+    int64_t acc = 0;
+    for (int b = 0; b < kNumBuckets; ++b) {
       int64_t c = 0;
       for (int64_t j = 0; j < nblk; ++j) c += host_cnt[b * nblk + j];
       g.nbucket[b] = c;
+      g.bstart[b] = acc;
+      acc += c;
     }
+  }
+  // tiles of the small-degree bucket
+  g.ntiles = 0;
+  const int64_t n0 = g.nbucket[kBTile];
+  const int32_t* tlist = g.blist + g.bstart[kBTile];
+  g.tile_start = a.lo_n<int32_t>(n0 + 2);
+  if (n0 > 0) {
+    HiScope hs(a);
+    int64_t* cum = a.hi_n<int64_t>(n0 + 1);
+    tile_cost_kernel<<<sm_grid(n0, kThreads), kThreads, 0, s>>>(tlist, n0, g.off, cum);
+    LVG_LAUNCH();
+    scan_i64(cum, cum, n0, a, s);
+    tile_start_kernel<<<sm_grid(n0, kThreads), kThreads, 0, s>>>(cum, n0, g.tile_start);
+    LVG_LAUNCH();
+    int64_t last = 0;
+    LVG_CUDA(cudaMemcpyAsync(&last, cum + n0 - 1, sizeof last, cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaStreamSynchronize(s));
+    g.ntiles = last / kTileCost + 1;
+  }
+  {
+    HiScope hs(a);
+    uint32_t* notint = a.hi_n<uint32_t>(1);
+    LVG_CUDA(cudaMemsetAsync(notint, 0, sizeof(uint32_t), s));
+    int_weights_kernel<<<sm_grid(std::max<int64_t>(g.nnz, V), kThreads), kThreads, 0, s>>>(g.cw, g.nnz, g.k, V,
+                                                                                          notint);
+    LVG_LAUNCH();
+    uint32_t h = 0;
+    LVG_CUDA(cudaMemcpyAsync(&h, notint, sizeof h, cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaStreamSynchronize(s));
+    g.int_acc = h == 0;
   }
   // hub tables
   g.nchunk = 0;
   g.hub_slots = 0;
-  const int64_t nhub = g.nbucket[2];
+  const int64_t nhub = g.nbucket[kBHub];
   if (nhub > 0) {
-    const int32_t* hubs = g.blist + g.nbucket[0] + g.nbucket[1];
+    const int32_t* hubs = g.blist + g.bstart[kBHub];
     std::vector<int64_t> be(2 * nhub);
     {
       HiScope hs(a);
@@ -857,8 +1274,8 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
       LVG_CUDA(cudaStreamSynchronize(s));
     }
     std::vector<int64_t> toff(nhub);
-    std::vector<int32_t> tlog(nhub), chub;
-    std::vector<int64_t> cbeg;
+    std::vector<int32_t> tlog(nhub), chub, shub, seg0(nhub + 1);
+    std::vector<int64_t> cbeg, sbeg;
     int64_t slots = 0;
     for (int64_t h = 0; h < nhub; ++h) {
       int64_t d = be[2 * h + 1] - be[2 * h];
@@ -871,7 +1288,21 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
         chub.push_back((int32_t)h);
         cbeg.push_back(b);
       }
+      seg0[h] = (int32_t)shub.size();
+      for (int64_t b = 0; b < ((int64_t)1 << l); b += kHubSeg) {
+        shub.push_back((int32_t)h);
+        sbeg.push_back(b);
+      }
     }
+    seg0[nhub] = (int32_t)shub.size();
+    g.nseg = (int64_t)shub.size();
+    g.seg_hub = a.lo_n<int32_t>(g.nseg);
+    g.seg_beg = a.lo_n<int64_t>(g.nseg);
+    g.hub_seg0 = a.lo_n<int32_t>(nhub + 1);
+    g.hub_part = a.lo_n<HubPartial>(g.nseg);
+    LVG_CUDA(cudaMemcpyAsync(g.seg_hub, shub.data(), sizeof(int32_t) * g.nseg, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.seg_beg, sbeg.data(), sizeof(int64_t) * g.nseg, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.hub_seg0, seg0.data(), sizeof(int32_t) * (nhub + 1), cudaMemcpyHostToDevice, s));
     g.hub_slots = slots;
     g.nchunk = (int64_t)chub.size();
     g.hub_toff = a.lo_n<int64_t>(nhub);
@@ -952,23 +1383,61 @@ void launch_q(const LevelGraph& g, CommState& st, double* dst, cudaStream_t s) {
   q_tail(st, dst, s, false);
 }
 
-void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s) {
+template <typename Acc>
+static void launch_tiles(const LevelGraph& g, MoveArgs P, cudaStream_t s) {
+  size_t smem = sizeof(TileSmem<Acc>);
+  static size_t attr = 0;
+  if (smem > attr) {
+    LVG_CUDA(cudaFuncSetAttribute(move_tile_kernel<Acc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = smem;
+  }
+  int per_sm = (int)((227u * 1024u) / (smem + 1024));
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = std::min<int64_t>(g.ntiles, (int64_t)sm_count() * per_sm);
+  move_tile_kernel<Acc><<<(unsigned)std::max<int64_t>(grid, 1), kThreads, smem, s>>>(P, g.tile_start, g.ntiles);
+  LVG_LAUNCH();
+}
+
+template <int G>
+static void launch_group(const LevelGraph& g, MoveArgs P, int bucket, cudaStream_t s) {
+  P.list = g.blist + g.bstart[bucket];
+  P.n = g.nbucket[bucket];
+  if (P.n == 0) return;
+  int64_t warps = (P.n + 32 / G - 1) / (32 / G);
+  int64_t blocks = std::min<int64_t>((warps + 7) / 8, (int64_t)sm_count() * 8);
+  move_group_kernel<G><<<(unsigned)blocks, kThreads, 0, s>>>(P);
+  LVG_LAUNCH();
+}
+
+// The degree classes are independent within a pass (each writes only its own
+// vertices' decisions and atomically adds into the deltas), so the small-grid
+// classes run on side streams, forked from and joined back into `s`.
+void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const SideStreams* ss) {
   MoveArgs P = move_args(g, st);
-  const int64_t nhub = g.nbucket[2];
+  cudaStream_t sh = s, sb = s, st2 = s;
+  if (ss) {
+    LVG_CUDA(cudaEventRecord(ss->fork, s));
+    for (int k = 0; k < 3; ++k) LVG_CUDA(cudaStreamWaitEvent(ss->side[k], ss->fork, 0));
+    sh = ss->side[0]; sb = ss->side[1]; st2 = ss->side[2];
+  }
+  const int64_t nhub = g.nbucket[kBHub];
   if (nhub > 0) {
     HubArgs H;
-    H.hubs = g.blist + g.nbucket[0] + g.nbucket[1];
+    H.hubs = g.blist + g.bstart[kBHub];
     H.chunk_hub = g.chunk_hub; H.chunk_beg = g.chunk_beg;
     H.toff = g.hub_toff; H.tlog = g.hub_tlog;
     H.keys = g.hub_keys; H.vals = g.hub_vals; H.sawown = g.hub_sawown;
-    hub_insert_kernel<<<(unsigned)g.nchunk, kThreads, 0, s>>>(P, H);
+    hub_insert_kernel<<<(unsigned)g.nchunk, kThreads, 0, sh>>>(P, H);
     LVG_LAUNCH();
-    hub_decide_kernel<<<(unsigned)nhub, kHubThreads, 0, s>>>(P, H);
+    hub_scan_kernel<<<(unsigned)g.nseg, kThreads, 0, sh>>>(P, H, g.seg_hub, g.seg_beg, g.hub_part);
+    LVG_LAUNCH();
+    hub_decide_kernel<<<grid_for(nhub, 128), 128, 0, sh>>>(P, H, g.hub_seg0, g.hub_part, nhub);
     LVG_LAUNCH();
   }
-  if (g.nbucket[1] > 0) {
-    P.list = g.blist + g.nbucket[0];
-    P.n = g.nbucket[1];
+  if (g.nbucket[kBBlock] > 0) {
+    MoveArgs Q = P;
+    Q.list = g.blist + g.bstart[kBBlock];
+    Q.n = g.nbucket[kBBlock];
     int lg = g.block_log;
     size_t smem = ((size_t)1 << lg) * (sizeof(double) + sizeof(int32_t));
     static size_t attr = 0;
@@ -976,19 +1445,30 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s) {
       LVG_CUDA(cudaFuncSetAttribute(move_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       attr = smem;
     }
-    move_block_kernel<<<sm_grid(P.n, 1), kThreads, smem, s>>>(P, lg);
+    move_block_kernel<<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg);
     LVG_LAUNCH();
   }
-  if (g.nbucket[0] > 0) {
-    P.list = g.blist;
-    P.n = g.nbucket[0];
-    move_warp_kernel<<<grid_for(P.n, kThreads / 32), kThreads, 0, s>>>(P);
-    LVG_LAUNCH();
+  if (g.ntiles > 0) {
+    MoveArgs Q = P;
+    Q.list = g.blist + g.bstart[kBTile];
+    Q.n = g.nbucket[kBTile];
+    if (g.int_acc) launch_tiles<int>(g, Q, st2);
+    else launch_tiles<double>(g, Q, st2);
+  }
+  launch_group<32>(g, P, kB32, s);
+  launch_group<16>(g, P, kB16, s);
+  launch_group<8>(g, P, kB8, s);
+  launch_group<4>(g, P, kB4, s);
+  if (ss) {
+    for (int k = 0; k < 3; ++k) {
+      LVG_CUDA(cudaEventRecord(ss->join[k], ss->side[k]));
+      LVG_CUDA(cudaStreamWaitEvent(s, ss->join[k], 0));
+    }
   }
 }
 
-void launch_pass(const LevelGraph& g, CommState& st, cudaStream_t s) {
-  launch_moves(g, st, s);
+void launch_pass(const LevelGraph& g, CommState& st, cudaStream_t s, const SideStreams* ss) {
+  launch_moves(g, st, s, ss);
   launch_commit(g, st, s);
 }
 
@@ -1119,7 +1599,16 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
   double* twoW = a.hi_n<double>(2);
   LVG_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * std::max(C, 1), s));
   LVG_CUDA(cudaMemsetAsync(Ain, 0, sizeof(double) * std::max(C, 1), s));
-  if (E > 0) {
+  if (E > 0 && C <= kNmSmemMax) {
+    size_t smem = sizeof(double) * 2 * (size_t)C;
+    static size_t attr = 0;
+    if (smem > 48 * 1024 && smem > attr) {
+      LVG_CUDA(cudaFuncSetAttribute(nm_accum_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr = smem;
+    }
+    nm_accum_smem_kernel<<<sm_grid(E, kThreads), kThreads, smem, s>>>(src, dst, w, E, part, C, Kc, Ain);
+    LVG_LAUNCH();
+  } else if (E > 0) {
     nm_accum_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
     LVG_LAUNCH();
   }

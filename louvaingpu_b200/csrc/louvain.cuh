@@ -27,6 +27,9 @@ struct PassCtl {
 
 enum : uint32_t { kErrProbe = 1u };
 
+// Degree classes of the move kernels (see bucket_of).
+enum { kB4 = 0, kB8, kB16, kB32, kBTile, kBBlock, kBHub, kNumBuckets };
+
 // One level of the graph on the device.
 struct LevelGraph {
   int32_t V = 0;
@@ -43,10 +46,16 @@ struct LevelGraph {
   float* loopw = nullptr;         // last self-loop weight (InitKernel.cu:181-194,239-242)
   uint8_t* has_loop = nullptr;
   double m = 0.0;                 // sum of input weights (NeighbourCompute.cu:46)
-  int32_t* blist = nullptr;       // vertices grouped by bucket: warp | block | hub
-  int64_t nbucket[3] = {0, 0, 0};
+  bool sorted_symmetric = false;  // CSR built without sorting (list sorted and symmetric)
+  int32_t* blist = nullptr;       // vertices grouped by degree class, in index order inside a class
+  int64_t nbucket[kNumBuckets] = {};
+  int64_t bstart[kNumBuckets] = {};
   int32_t max_deg = 0;
   int block_log = 13;             // log2 slots of the block-per-vertex table
+  // tiles of the small-degree bucket
+  int32_t* tile_start = nullptr;  // [ntiles+1] first bucket index of each tile
+  int64_t ntiles = 0;
+  bool int_acc = false;           // integral weights, degrees < 2^30: exact int32 sums
   // hub tables
   int64_t hub_slots = 0;
   int64_t* hub_toff = nullptr;    // [nhub] table offset
@@ -57,6 +66,11 @@ struct LevelGraph {
   int32_t* hub_keys = nullptr;
   double* hub_vals = nullptr;
   uint32_t* hub_sawown = nullptr;
+  int64_t nseg = 0;               // 8192-slot segments of the hub tables
+  int32_t* seg_hub = nullptr;
+  int64_t* seg_beg = nullptr;
+  int32_t* hub_seg0 = nullptr;    // [nhub+1] first segment of each hub
+  struct HubPartial* hub_part = nullptr;
 };
 
 struct CommState {
@@ -76,8 +90,8 @@ struct CommState {
 };
 
 struct Tuning {
-  int32_t warp_max = 128;
-  int32_t block_max = 4096;
+  int32_t warp_max = 512;         // largest degree packed into tiles
+  int32_t block_max = 4096;       // largest degree with a block-private table
 };
 
 // Validate an input list on the device: ids in range, weights finite >= 0.
@@ -94,12 +108,19 @@ void alloc_state(const LevelGraph& g, CommState& st, Arena& a);
 void init_state(const LevelGraph& g, CommState& st, double lower, double pass_min, int32_t max_passes,
                 Arena& a, cudaStream_t s);
 
+// Side streams on which the smaller degree classes of a pass run.
+struct SideStreams {
+  cudaStream_t side[3];
+  cudaEvent_t fork;
+  cudaEvent_t join[3];
+};
+
 // Launch one pass: move kernels + conditional commit + control.
-void launch_pass(const LevelGraph& g, CommState& st, cudaStream_t s);
+void launch_pass(const LevelGraph& g, CommState& st, cudaStream_t s, const SideStreams* ss);
 // The ΔQ test, conditional commit and pass control of one pass.
 void launch_commit(const LevelGraph& g, CommState& st, cudaStream_t s);
 // Launch only the move kernels (decisions, accumulations into d*).
-void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s);
+void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const SideStreams* ss);
 // After the loop is done: isolated-vertex merge, final commit, ctl->q_ret.
 void launch_merge(const LevelGraph& g, CommState& st, cudaStream_t s);
 // Q of the committed state into *dst (device).

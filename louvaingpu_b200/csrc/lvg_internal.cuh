@@ -41,6 +41,7 @@ struct Arena {
   size_t cap = 0, lo = 0, hi = 0, peak = 0;
   static constexpr size_t kAlign = 256;
   void reserve(size_t bytes) {
+    bytes = (bytes + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);  // both ends stay 256-aligned
     if (bytes <= cap) { lo = 0; hi = cap; return; }
     release();
     LVG_CUDA(cudaMalloc(&base, bytes));

@@ -44,7 +44,7 @@ class RunResult:
 
 class Louvain:
     def __init__(self, device=0, pass_min_gain=1e-7, level_min_gain=1e-7, max_passes=-1, max_levels=-1,
-                 arena_bytes=0, warp_max_degree=0, block_max_degree=0, passes_per_sync=0):
+                 arena_bytes=0, tile_max_degree=0, block_max_degree=0, passes_per_sync=0):
         L = _lib.load()
         cfg = _lib.LvgConfig()
         L.lvg_config_default(ctypes.byref(cfg))
@@ -54,8 +54,8 @@ class Louvain:
         cfg.max_passes = max_passes
         cfg.max_levels = max_levels
         cfg.arena_bytes = arena_bytes
-        if warp_max_degree:
-            cfg.warp_max_degree = warp_max_degree
+        if tile_max_degree:
+            cfg.tile_max_degree = tile_max_degree
         if block_max_degree:
             cfg.block_max_degree = block_max_degree
         if passes_per_sync:

@@ -47,7 +47,7 @@ def test_status_strings_and_config_defaults(lib):
     cfg = _lib.LvgConfig()
     assert lib.lvg_config_default(ctypes.byref(cfg)) == 0
     assert cfg.pass_min_gain == 1e-7 and cfg.level_min_gain == 1e-7
-    assert cfg.max_passes == -1 and cfg.warp_max_degree == 128 and cfg.block_max_degree == 4096
+    assert cfg.max_passes == -1 and cfg.tile_max_degree == 512 and cfg.block_max_degree == 4096
 
 
 def test_null_arguments_rejected_without_device(lib):

@@ -72,7 +72,7 @@ def test_two_triangles_known_answer(Louvain, oracle):
         assert res.q_final == pytest.approx(g["final_modularity_fp64"], abs=1e-12)
 
 
-@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "hub"])
+@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "odd_sizes", "hub"])
 def test_csr_build_bit_exact(Louvain, oracle, gen, case):
     n, s, d, w = make_case(gen, case)
     oc = oracle.Csr(n, s, d, w)
@@ -94,6 +94,13 @@ def make_case(gen, case):
         d = rng.integers(0, n - 50, m).astype(np.int32)
         w = rng.integers(0, 4, m).astype(np.float32)       # zero weights and self loops included
         return n, s, d, w
+    if case == "odd_sizes":
+        n = 1001
+        m = 2999
+        s = rng.integers(0, n, m).astype(np.int32)
+        d = rng.integers(0, n, m).astype(np.int32)
+        w = rng.integers(1, 6, m).astype(np.float32)
+        return n, s, d, w
     if case == "hub":
         # a star hub of degree 12000 (global-table path) plus a block-bucket hub and SBM background
         n, s, d, w = gen.sbm(20000, 40, 0.01, 0.0002, 1, 3, seed=3)
@@ -106,7 +113,7 @@ def make_case(gen, case):
     raise ValueError(case)
 
 
-@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "hub"])
+@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "odd_sizes", "hub"])
 def test_move_decisions_bit_exact(Louvain, oracle, gen, case):
     n, s, d, w = make_case(gen, case)
     oc = oracle.Csr(n, s, d, w)
@@ -126,7 +133,7 @@ def test_move_decisions_bit_exact(Louvain, oracle, gen, case):
             np.testing.assert_array_equal(cand, exp_cand)
 
 
-@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "hub"])
+@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "odd_sizes", "hub"])
 def test_full_run_bit_exact(Louvain, oracle, gen, case):
     n, s, d, w = make_case(gen, case)
     orun = oracle.Run(n, s, d, w)
