@@ -54,7 +54,8 @@ typedef struct {
   int32_t tile_max_degree; /* vertices up to this degree are packed into shared-memory tiles (<= 512) */
   int32_t block_max_degree;/* up to this degree a block-per-vertex shared table; above, global tables */
   int32_t passes_per_sync; /* passes launched between host checks of convergence (0: default) */
-  int32_t use_graphs;      /* capture the pass sequence of a level in a CUDA graph (1: default on) */
+  int32_t use_graphs;      /* replay each pass from CUDA graphs captured once per level (1: on) */
+  int32_t l2_persist;      /* keep the gathered community arrays in an L2 persisting window (1: on) */
 } lvg_config;
 
 /* Per-level record of a run (the reference keeps one Partition per level,

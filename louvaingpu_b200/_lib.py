@@ -35,6 +35,7 @@ class LvgConfig(ctypes.Structure):
         ("block_max_degree", ctypes.c_int32),
         ("passes_per_sync", ctypes.c_int32),
         ("use_graphs", ctypes.c_int32),
+        ("l2_persist", ctypes.c_int32),
     ]
 
 

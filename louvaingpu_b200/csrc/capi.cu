@@ -65,6 +65,10 @@ struct lvg_ctx {
   SideStreams side{};
   bool have_side = false;
   std::vector<cudaEvent_t> mev;   // move-phase events, two per pass
+  cudaGraphExec_t g_moves = nullptr;   // captured move kernels of one pass (current level)
+  cudaGraphExec_t g_commit = nullptr;  // captured commit + pass control
+  size_t persist_max = 0;         // device limits for L2 persistence
+  size_t window_max = 0;
   double move_ms = 0.0;
   int64_t move_passes = 0;
 };
@@ -118,7 +122,32 @@ size_t arena_estimate(int64_t V, int64_t E, bool copy_list) {
 void sync(lvg_ctx* c) { LVG_CUDA(cudaStreamSynchronize(c->stream)); }
 
 // Prepare the current level (c->g holds the level input list): build, state.
+void drop_graphs(lvg_ctx* c) {
+  if (c->g_moves) cudaGraphExecDestroy(c->g_moves);
+  if (c->g_commit) cudaGraphExecDestroy(c->g_commit);
+  c->g_moves = c->g_commit = nullptr;
+}
+
+// Capture the two halves of a pass once per level; replaying them replaces
+// about a dozen launches and the side-stream fork/join per pass.
+void ensure_graphs(lvg_ctx* c) {
+  if (c->g_moves && c->g_commit) return;
+  cudaStream_t s = c->stream;
+  cudaGraph_t gr = nullptr;
+  LVG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  launch_moves(c->g, c->st, s, &c->side);
+  LVG_CUDA(cudaStreamEndCapture(s, &gr));
+  LVG_CUDA(cudaGraphInstantiate(&c->g_moves, gr, 0));
+  cudaGraphDestroy(gr);
+  LVG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  launch_commit(c->g, c->st, s);
+  LVG_CUDA(cudaStreamEndCapture(s, &gr));
+  LVG_CUDA(cudaGraphInstantiate(&c->g_commit, gr, 0));
+  cudaGraphDestroy(gr);
+}
+
 void prepare_level(lvg_ctx* c) {
+  drop_graphs(c);
   build_level(c->g, c->tune, c->arena, c->stream);
   alloc_state(c->g, c->st, c->arena);
   init_state(c->g, c->st, 0.0, c->cfg.pass_min_gain, c->cfg.max_passes, c->arena, c->stream);
@@ -183,11 +212,45 @@ double read_q(lvg_ctx* c) {
 
 constexpr int kHardPassCap = 1 << 20;
 
+// Keeps the gathered community arrays (tot, comm, size) in L2 while the move
+// passes stream the CSR through it; the streams' previous windows come back
+// when the scope ends.
+struct L2Window {
+  lvg_ctx* c;
+  cudaStream_t streams[4];
+  cudaStreamAttrValue saved[4];
+  int n = 0;
+  L2Window(lvg_ctx* ctx, const CommState& st) : c(ctx) {
+    if (!c->cfg.l2_persist || c->persist_max == 0 || c->window_max == 0 || st.hot_bytes == 0) return;
+    cudaStreamAttrValue v = {};
+    size_t bytes = std::min(st.hot_bytes, c->window_max);
+    v.accessPolicyWindow.base_ptr = (void*)st.tot;
+    v.accessPolicyWindow.num_bytes = bytes;
+    v.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)c->persist_max / (double)bytes);
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    streams[0] = c->stream;
+    for (int k = 0; k < 3; ++k) streams[k + 1] = c->side.side[k];
+    for (int k = 0; k < 4; ++k) {
+      if (cudaStreamGetAttribute(streams[k], cudaStreamAttributeAccessPolicyWindow, &saved[k]) != cudaSuccess) break;
+      if (cudaStreamSetAttribute(streams[k], cudaStreamAttributeAccessPolicyWindow, &v) != cudaSuccess) break;
+      n = k + 1;
+    }
+  }
+  ~L2Window() {
+    for (int k = 0; k < n; ++k) cudaStreamSetAttribute(streams[k], cudaStreamAttributeAccessPolicyWindow, &saved[k]);
+    if (n) cudaCtxResetPersistingL2Cache();
+  }
+};
+
 // One-level phase (oneLevelCUDA, OneLevelKernel.cu:518-954).
 void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int32_t* status_out,
                double* q_start_out) {
   cudaStream_t s = c->stream;
   init_state(c->g, c->st, lower, c->cfg.pass_min_gain, c->cfg.max_passes, c->arena, s);
+  L2Window l2(c, c->st);
+  const bool use_graphs = c->cfg.use_graphs != 0;
+  if (use_graphs) ensure_graphs(c);
   PassCtl h;
   const int chunk = c->cfg.passes_per_sync > 0 ? c->cfg.passes_per_sync : 4;
   c->pass_ms.clear();
@@ -202,9 +265,11 @@ void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int
         c->mev.push_back(ev);
       }
       LVG_CUDA(cudaEventRecord(c->mev[e], s));
-      launch_moves(c->g, c->st, s, &c->side);
+      if (use_graphs) LVG_CUDA(cudaGraphLaunch(c->g_moves, s));
+      else launch_moves(c->g, c->st, s, &c->side);
       LVG_CUDA(cudaEventRecord(c->mev[e + 1], s));
-      launch_commit(c->g, c->st, s);
+      if (use_graphs) LVG_CUDA(cudaGraphLaunch(c->g_commit, s));
+      else launch_commit(c->g, c->st, s);
       ++launched;
     }
     LVG_CUDA(cudaMemcpyAsync(&h, c->st.ctl, sizeof h, cudaMemcpyDeviceToHost, s));
@@ -323,6 +388,7 @@ lvg_status lvg_config_default(lvg_config* cfg) {
   cfg->block_max_degree = 4096;
   cfg->passes_per_sync = 4;
   cfg->use_graphs = 1;
+  cfg->l2_persist = 1;
   return LVG_OK;
 }
 
@@ -354,6 +420,12 @@ lvg_status lvg_create(const lvg_config* cfg, lvg_ctx** out) {
     }
     LVG_CUDA(cudaEventCreateWithFlags(&c->side.fork, cudaEventDisableTiming));
     c->have_side = true;
+    cudaDeviceProp prop;
+    LVG_CUDA(cudaGetDeviceProperties(&prop, c->device));
+    c->persist_max = (size_t)prop.persistingL2CacheMaxSize;
+    c->window_max = (size_t)prop.accessPolicyMaxWindowSize;
+    if (c->persist_max > 0)   // per-context limit, released with the context
+      LVG_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, c->persist_max));
   });
   if (s != LVG_OK) {
     lvg_destroy(c);
@@ -367,6 +439,7 @@ lvg_status lvg_destroy(lvg_ctx* c) {
   if (!c) return LVG_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
   c->arena.release();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);

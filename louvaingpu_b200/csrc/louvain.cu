@@ -27,7 +27,7 @@ struct HubPartial {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kHubChunk = 4096;
+constexpr int kHubChunk = 512;
 constexpr int kNone = INT_MAX;
 
 __device__ __forceinline__ uint32_t hash_c(int32_t c, int logT) {
@@ -381,9 +381,9 @@ __global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int ma
     int T = 1 << logT;
     bool sawown = false;
     for (int64_t e = beg + threadIdx.x; e < end; e += kThreads) {
-      int32_t c = P.comm[P.col[e]];
+      int32_t c = P.comm[__ldcs(P.col + e)];
       sawown |= (c == own);
-      if (!table_insert(keys, vals, logT, c, (double)P.cw[e])) overflow = true;
+      if (!table_insert(keys, vals, logT, c, (double)__ldcs(P.cw + e))) overflow = true;
     }
     __syncthreads();
     double kf = P.kfrac[i];
@@ -421,72 +421,104 @@ __global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int ma
   if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
 }
 
-// --------------------------------------------------------------- group kernels
-// Degree <= 32: G lanes per vertex (G = 4, 8, 16, 32), one CSR entry per lane,
-// 32/G vertices per warp.  __match_any_sync on (group, community) finds the
-// entries of equal communities; they add their weights into the slot of the
-// lowest such lane (shared memory), and a butterfly inside the group picks the
-// best community.  No table, no block barrier.
-template <int G>
-__device__ __forceinline__ void group_best(double& bg, int32_t& bc, double& bw) {
-  const unsigned full = 0xffffffffu;
+// ----------------------------------------------------------------- ELL kernels
+// Degree <= 32: vertices of class D (4, 8, 16, 32) keep their entries in a
+// sliced-ELL copy of the CSR built once per level: vertex j of the class owns
+// slots [j*D, j*D+D), padding holds column -1.
+struct EllArgs {
+  const int32_t* col;   // [n * G] neighbour of each slot, -1 for padding
+  const float* w;       // [n * G]
+  const int32_t* list;  // [n] vertex of each item
+  int64_t n;
+};
+
+// One thread per vertex.  The thread loads its ELL row with
+// 16-byte loads, gathers the neighbour communities, sorts the (community,
+// weight) pairs in registers with a bitonic network and walks them once in
+// ascending order: equal communities are adjacent, so each run gives one
+// candidate's summed weight, and keeping only strictly larger gains leaves
+// the lowest community among equal gains (OneLevelKernel.cu:330,358).
+template <int D>
+__device__ __forceinline__ void cas_pair(int32_t (&c)[D], float (&w)[D], int a, int b) {
+  int32_t ca = c[a], cb = c[b];
+  bool sw = ca > cb;
+  float wa = w[a], wb = w[b];
+  c[a] = sw ? cb : ca; c[b] = sw ? ca : cb;
+  w[a] = sw ? wb : wa; w[b] = sw ? wa : wb;
+}
+
+template <int D>
+__device__ __forceinline__ void bitonic_sort(int32_t (&c)[D], float (&w)[D]) {
 #pragma unroll
-  for (int o = G / 2; o >= 1; o >>= 1) {
-    double g = __shfl_xor_sync(full, bg, o);
-    int32_t c = __shfl_xor_sync(full, bc, o);
-    double w = __shfl_xor_sync(full, bw, o);
-    if (better(g, c, bg, bc)) { bg = g; bc = c; bw = w; }
+  for (int k = 2; k <= D; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int x = 0; x < D; ++x) {
+        int y = x ^ j;
+        if (y > x) {
+          if ((x & k) == 0) cas_pair<D>(c, w, x, y);
+          else cas_pair<D>(c, w, y, x);
+        }
+      }
+    }
   }
 }
 
-template <int G>
-__global__ void __launch_bounds__(kThreads) move_group_kernel(MoveArgs P) {
-  __shared__ double ssum[kThreads];
+template <int D>
+__global__ void __launch_bounds__(kThreads) move_thread_kernel(MoveArgs P, EllArgs L) {
   if (P.ctl->done) return;
-  constexpr int VPW = 32 / G;
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int gi = lane / G, gl = lane % G;
-  const unsigned gmask = G == 32 ? full : (((1u << G) - 1u) << (gi * G));
-  double* my = &ssum[threadIdx.x & ~31];
-  const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
-  for (int64_t base = warp * VPW; base < P.n; base += nwarps * VPW) {
-    const int64_t item = base + gi;
-    const bool act = item < P.n;
-    int32_t i = 0, own = -1, deg = 0;
-    int64_t beg = 0;
-    if (act) {
-      i = P.list[item];
-      beg = P.off[i];
-      deg = (int32_t)(P.off[i + 1] - beg);
-      own = P.comm[i];
+  for (int64_t j = blockIdx.x * (int64_t)kThreads + threadIdx.x; j < L.n; j += (int64_t)gridDim.x * kThreads) {
+    int32_t c[D];
+    float w[D];
+    const int4* cp = reinterpret_cast<const int4*>(L.col + j * D);
+    const float4* wp = reinterpret_cast<const float4*>(L.w + j * D);
+#pragma unroll
+    for (int q = 0; q < D / 4; ++q) {
+      int4 a = __ldcs(cp + q);          // streamed once per pass: evict first
+      float4 b = __ldcs(wp + q);
+      c[4 * q] = a.x; c[4 * q + 1] = a.y; c[4 * q + 2] = a.z; c[4 * q + 3] = a.w;
+      w[4 * q] = b.x; w[4 * q + 1] = b.y; w[4 * q + 2] = b.z; w[4 * q + 3] = b.w;
     }
-    const bool valid = gl < deg;
-    int32_t c = -1;
-    float w = 0.0f;
-    if (valid) { c = P.col[beg + gl]; w = P.cw[beg + gl]; }
-    if (valid) c = P.comm[c];
-    unsigned long long key = valid ? (((unsigned long long)gi << 32) | (uint32_t)c)
-                                   : (0xFFFFFFFF00000000ull | (unsigned)lane);
-    unsigned peers = __match_any_sync(full, key);
-    int leader = __ffs(peers) - 1;
-    my[lane] = 0.0;
-    __syncwarp();
-    if (valid) atomicAdd(&my[leader], (double)w);
-    __syncwarp();
-    const bool isl = valid && leader == lane;
-    unsigned bl = __ballot_sync(full, isl) & gmask;
-    unsigned bo = __ballot_sync(full, valid && c == own) & gmask;
-    double bg = 0.0, bw = 0.0;
+    const int32_t i = L.list[j];
+#pragma unroll
+    for (int q = 0; q < D; ++q) c[q] = c[q] >= 0 ? P.comm[c[q]] : kNone;
+    const int32_t own = P.comm[i];
+    const double kf = P.kfrac[i];
+    bitonic_sort<D>(c, w);
+    double bg = 0.0, bw = 0.0, run = 0.0;
     int32_t bc = kNone;
-    if (isl) consider(c, my[lane], P.kfrac[i], P.tot, bg, bc, bw);
-    group_best<G>(bg, bc, bw);
-    if (act && gl == 0) {
-      int32_t nseg = __popc(bl) + ((P.has_loop[i] && bo == 0) ? 1 : 0);
-      apply_decision(P, i, own, bc, bw, nseg);
+    int nseg = 0;
+    bool sawown = false;
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+      const bool ok = c[q] != kNone;
+      const bool head = ok && (q == 0 || c[q] != c[q - 1]);
+      const bool tail = ok && (q == D - 1 || c[q + 1] != c[q]);
+      run = head ? (double)w[q] : __dadd_rn(run, (double)w[q]);
+      nseg += head ? 1 : 0;
+      sawown |= ok && c[q] == own;
+      if (tail && run != 0.0) {                                  // OneLevelKernel.cu:303
+        double g = __dsub_rn(run, __dmul_rn(P.tot[c[q]], kf));   // OneLevelKernel.cu:307-313
+        if (g > 0.0 && g > bg) { bg = g; bc = c[q]; bw = run; }
+      }
     }
-    __syncwarp();
+    nseg += (P.has_loop[i] && !sawown) ? 1 : 0;
+    apply_decision(P, i, own, bc, bw, nseg);
+  }
+}
+
+// Sliced-ELL copy of the degree-class rows: slot (class b, item j, lane s).
+__global__ void ell_fill_kernel(const int32_t* list, const int64_t* off, const int32_t* col, const float* cw,
+                                int64_t n, int G, int32_t* ecol, float* ew) {
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n * G; x += (int64_t)gridDim.x * blockDim.x) {
+    int64_t j = x / G;
+    int sl = (int)(x - j * G);
+    int32_t i = list[j];
+    int64_t b = off[i];
+    int64_t d = off[i + 1] - b;
+    ecol[x] = sl < d ? col[b + sl] : -1;
+    ew[x] = sl < d ? cw[b + sl] : 0.0f;
   }
 }
 
@@ -588,8 +620,8 @@ __global__ void __launch_bounds__(kThreads) move_tile_kernel(MoveArgs P, const i
           int j = tile_find(S.rowbeg, nv, q);
           int64_t e = S.beg[j] + (q - S.rowbeg[j]);
           jj[u] = j;
-          cc[u] = P.col[e];
-          ww[u] = P.cw[e];
+          cc[u] = __ldcs(P.col + e);
+          ww[u] = __ldcs(P.cw + e);
         }
       }
 #pragma unroll
@@ -708,18 +740,18 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(MoveArgs P, HubArg
   int logT = H.tlog[h];
   bool sawown = false, overflow = false;
   for (int64_t e = beg + threadIdx.x; e < end; e += kThreads) {
-    int32_t c = P.comm[P.col[e]];
+    int32_t c = P.comm[__ldcs(P.col + e)];
     sawown |= (c == own);
-    if (!table_insert(keys, vals, logT, c, (double)P.cw[e])) overflow = true;
+    if (!table_insert(keys, vals, logT, c, (double)__ldcs(P.cw + e))) overflow = true;
   }
   if (__syncthreads_or(sawown) && threadIdx.x == 0) atomicOr(&H.sawown[h], 1u);
   if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
 }
 
-// ... then blocks scan 8192-slot segments of the hub tables (best candidate,
+// ... then blocks scan 1024-slot segments of the hub tables (best candidate,
 // occupancy, clearing the slots) and one thread per hub combines its segments
 // in order and decides.
-constexpr int kHubSeg = 8192;
+constexpr int kHubSeg = 1024;
 
 __global__ void __launch_bounds__(kThreads) hub_scan_kernel(MoveArgs P, HubArgs H, const int32_t* seg_hub,
                                                             const int64_t* seg_beg, HubPartial* part) {
@@ -1104,6 +1136,8 @@ bool validate_edges(const int32_t* src, const int32_t* dst, const float* w, int6
 
 // Sort-free CSR build; returns false (and builds nothing) unless the level
 // list is strictly sorted and symmetric.
+static void set_move_attributes(int block_log);
+
 static bool build_csr_fast(LevelGraph& g, Arena& a, cudaStream_t s) {
   const int32_t V = g.V;
   const int64_t E = g.E;
@@ -1228,6 +1262,26 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
       acc += c;
     }
   }
+  // sliced-ELL copies of the degree classes up to 32
+  {
+    static const int kG[4] = {4, 8, 16, 32};
+    int64_t slots = 0;
+    for (int b = kB4; b <= kB32; ++b) {
+      g.ell_base[b] = slots;
+      slots += g.nbucket[b] * kG[b - kB4];
+    }
+    g.ell_col = a.lo_n<int32_t>(slots);
+    g.ell_w = a.lo_n<float>(slots);
+    for (int b = kB4; b <= kB32; ++b) {
+      int64_t nb = g.nbucket[b];
+      if (nb == 0) continue;
+      int G = kG[b - kB4];
+      ell_fill_kernel<<<sm_grid(nb * G, kThreads), kThreads, 0, s>>>(g.blist + g.bstart[b], g.off, g.col, g.cw, nb,
+                                                                      G, g.ell_col + g.ell_base[b],
+                                                                      g.ell_w + g.ell_base[b]);
+      LVG_LAUNCH();
+    }
+  }
   // tiles of the small-degree bucket
   g.ntiles = 0;
   const int64_t n0 = g.nbucket[kBTile];
@@ -1322,15 +1376,19 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
     LVG_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
   }
   g.block_log = block_table_log(t);
+  set_move_attributes(g.block_log);
 }
 
 void alloc_state(const LevelGraph& g, CommState& st, Arena& a) {
   const int32_t V = g.V;
-  st.comm = a.lo_n<int32_t>(V);
-  st.next = a.lo_n<int32_t>(V);
+  // comm, tot and size are gathered per entry / per candidate: keep them
+  // adjacent so that one L2 persistence window covers them
   st.tot = a.lo_n<double>(V);
-  st.in = a.lo_n<double>(V);
+  st.comm = a.lo_n<int32_t>(V);
   st.size = a.lo_n<int32_t>(V);
+  st.hot_bytes = (size_t)((char*)(st.size + std::max<int32_t>(V, 1)) - (char*)st.tot);
+  st.next = a.lo_n<int32_t>(V);
+  st.in = a.lo_n<double>(V);
   st.dtot = a.lo_n<double>(V);
   st.din = a.lo_n<double>(V);
   st.dsize = a.lo_n<int32_t>(V);
@@ -1383,14 +1441,22 @@ void launch_q(const LevelGraph& g, CommState& st, double* dst, cudaStream_t s) {
   q_tail(st, dst, s, false);
 }
 
+// Dynamic shared memory limits of the move kernels, set before any capture.
+static void set_move_attributes(int block_log) {
+  static int done_log = -1;
+  if (done_log >= block_log) return;
+  LVG_CUDA(cudaFuncSetAttribute(move_tile_kernel<int>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TileSmem<int>)));
+  LVG_CUDA(cudaFuncSetAttribute(move_tile_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TileSmem<double>)));
+  size_t smem = ((size_t)1 << block_log) * (sizeof(double) + sizeof(int32_t));
+  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  done_log = block_log;
+}
+
 template <typename Acc>
 static void launch_tiles(const LevelGraph& g, MoveArgs P, cudaStream_t s) {
   size_t smem = sizeof(TileSmem<Acc>);
-  static size_t attr = 0;
-  if (smem > attr) {
-    LVG_CUDA(cudaFuncSetAttribute(move_tile_kernel<Acc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = smem;
-  }
   int per_sm = (int)((227u * 1024u) / (smem + 1024));
   if (per_sm < 1) per_sm = 1;
   int64_t grid = std::min<int64_t>(g.ntiles, (int64_t)sm_count() * per_sm);
@@ -1398,14 +1464,16 @@ static void launch_tiles(const LevelGraph& g, MoveArgs P, cudaStream_t s) {
   LVG_LAUNCH();
 }
 
-template <int G>
-static void launch_group(const LevelGraph& g, MoveArgs P, int bucket, cudaStream_t s) {
-  P.list = g.blist + g.bstart[bucket];
-  P.n = g.nbucket[bucket];
-  if (P.n == 0) return;
-  int64_t warps = (P.n + 32 / G - 1) / (32 / G);
-  int64_t blocks = std::min<int64_t>((warps + 7) / 8, (int64_t)sm_count() * 8);
-  move_group_kernel<G><<<(unsigned)blocks, kThreads, 0, s>>>(P);
+template <int D>
+static void launch_thread(const LevelGraph& g, MoveArgs P, int bucket, cudaStream_t s) {
+  EllArgs L;
+  L.n = g.nbucket[bucket];
+  if (L.n == 0) return;
+  L.col = g.ell_col + g.ell_base[bucket];
+  L.w = g.ell_w + g.ell_base[bucket];
+  L.list = g.blist + g.bstart[bucket];
+  int64_t blocks = std::min<int64_t>((L.n + kThreads - 1) / kThreads, (int64_t)sm_count() * 8);
+  move_thread_kernel<D><<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, 0, s>>>(P, L);
   LVG_LAUNCH();
 }
 
@@ -1440,11 +1508,6 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     Q.n = g.nbucket[kBBlock];
     int lg = g.block_log;
     size_t smem = ((size_t)1 << lg) * (sizeof(double) + sizeof(int32_t));
-    static size_t attr = 0;
-    if (smem > attr) {
-      LVG_CUDA(cudaFuncSetAttribute(move_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr = smem;
-    }
     move_block_kernel<<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg);
     LVG_LAUNCH();
   }
@@ -1455,10 +1518,10 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     if (g.int_acc) launch_tiles<int>(g, Q, st2);
     else launch_tiles<double>(g, Q, st2);
   }
-  launch_group<32>(g, P, kB32, s);
-  launch_group<16>(g, P, kB16, s);
-  launch_group<8>(g, P, kB8, s);
-  launch_group<4>(g, P, kB4, s);
+  launch_thread<32>(g, P, kB32, s);
+  launch_thread<16>(g, P, kB16, s);
+  launch_thread<8>(g, P, kB8, s);
+  launch_thread<4>(g, P, kB4, s);
   if (ss) {
     for (int k = 0; k < 3; ++k) {
       LVG_CUDA(cudaEventRecord(ss->join[k], ss->side[k]));

@@ -52,6 +52,10 @@ struct LevelGraph {
   int64_t bstart[kNumBuckets] = {};
   int32_t max_deg = 0;
   int block_log = 13;             // log2 slots of the block-per-vertex table
+  // sliced-ELL copies of the degree classes up to 32 (slots of class b from ell_base[b])
+  int32_t* ell_col = nullptr;
+  float* ell_w = nullptr;
+  int64_t ell_base[kNumBuckets] = {};
   // tiles of the small-degree bucket
   int32_t* tile_start = nullptr;  // [ntiles+1] first bucket index of each tile
   int64_t ntiles = 0;
@@ -87,6 +91,7 @@ struct CommState {
   double* partials2 = nullptr;
   PassCtl* ctl = nullptr;
   int64_t ngroups = 0;
+  size_t hot_bytes = 0;           // tot | comm | size, contiguous from tot
 };
 
 struct Tuning {

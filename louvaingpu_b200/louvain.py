@@ -44,7 +44,7 @@ class RunResult:
 
 class Louvain:
     def __init__(self, device=0, pass_min_gain=1e-7, level_min_gain=1e-7, max_passes=-1, max_levels=-1,
-                 arena_bytes=0, tile_max_degree=0, block_max_degree=0, passes_per_sync=0):
+                 arena_bytes=0, tile_max_degree=0, block_max_degree=0, passes_per_sync=0, use_graphs=True, l2_persist=True):
         L = _lib.load()
         cfg = _lib.LvgConfig()
         L.lvg_config_default(ctypes.byref(cfg))
@@ -60,6 +60,8 @@ class Louvain:
             cfg.block_max_degree = block_max_degree
         if passes_per_sync:
             cfg.passes_per_sync = passes_per_sync
+        cfg.use_graphs = 1 if use_graphs else 0
+        cfg.l2_persist = 1 if l2_persist else 0
         self._L = L
         h = ctypes.c_void_p()
         _lib.check(None, L.lvg_create(ctypes.byref(cfg), ctypes.byref(h)))

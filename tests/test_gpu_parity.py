@@ -186,6 +186,32 @@ def test_lfr_full_size(Louvain, oracle, gen):
         run_equal(lv, res, orun, n, s, d, w, oracle)
 
 
+@pytest.mark.parametrize("use_graphs,passes_per_sync", [(False, 1), (True, 1), (True, 7)])
+def test_graph_replay_and_sync_interval_do_not_change_results(Louvain, oracle, gen, use_graphs, passes_per_sync):
+    n, s, d, w = gen.sbm(4000, 40, 0.05, 0.002, 1, 2, seed=6)
+    orun = oracle.Run(n, s, d, w)
+    with Louvain(use_graphs=use_graphs, passes_per_sync=passes_per_sync) as lv:
+        lv.load_edges(s, d, w, n)
+        res = lv.run()
+        run_equal(lv, res, orun, n, s, d, w, oracle)
+
+
+def test_unsorted_input_matches_sorted(Louvain, gen):
+    """The sort-free CSR build (sorted symmetric list) and the sorting build
+    (the same list shuffled) give the same CSR and dendrogram."""
+    n, s, d, w = gen.sbm(3000, 30, 0.05, 0.002, 1, 3, seed=8)
+    perm = np.random.default_rng(1).permutation(len(s))
+    with Louvain() as a, Louvain() as b:
+        a.load_edges(s, d, w, n)
+        b.load_edges(s[perm], d[perm], w[perm], n)
+        ca, cb = a.csr(), b.csr()
+        for key in ("off", "col", "w", "k", "loopw", "has_loop"):
+            np.testing.assert_array_equal(ca[key], cb[key])
+        ra, rb = a.run(), b.run()
+        assert ra.n_levels == rb.n_levels
+        np.testing.assert_array_equal(a.partition(), b.partition())
+
+
 def test_invalid_input_is_an_error(Louvain):
     from louvaingpu_b200 import LvgError
     with Louvain() as lv:
