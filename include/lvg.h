@@ -172,6 +172,30 @@ lvg_status lvg_move_stats(const lvg_ctx* ctx, double* ms_total, int64_t* n_passe
 /* Number of CUDA kernels this library has launched in this process. */
 lvg_status lvg_kernel_launches(int64_t* n);
 
+/* Largest community count lvg_modularity_fp64_noalloc accepts. */
+#define LVG_NOALLOC_MAX_COMMS (1 << 18)
+
+/* FP64 Newman modularity of a partition, like lvg_modularity_fp64, for
+ * callers that cannot allocate device memory at call time: code running while
+ * a stream is captured into a CUDA graph (cudaMalloc/cudaFree are not allowed
+ * there), serving loops whose HBM is all held by their own pool, and paths
+ * that cannot take the device-wide synchronisation of cudaMalloc/cudaFree.
+ * No counterpart in the reference.
+ * Inputs are device pointers: the edge list (n_entries entries) and the
+ * community of each vertex, values in [0, n_comms); the result goes to the
+ * host double *q.  The call allocates nothing: its scratch is a fixed device
+ * array of 3 * LVG_NOALLOC_MAX_COMMS doubles (6 MiB) that every GPU which
+ * loads the library holds until the process exits.  n_comms above
+ * LVG_NOALLOC_MAX_COMMS returns LVG_ERR_CAPACITY.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make it
+ * before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU (other streams, other host threads) race and must be serialised by
+ * the caller.  The call synchronises `stream` (a cudaStream_t, NULL for the
+ * legacy default stream) to return the value. */
+lvg_status lvg_modularity_fp64_noalloc(const int32_t* d_src, const int32_t* d_dst, const float* d_w,
+                                       int64_t n_entries, const int32_t* d_part, int32_t n_comms,
+                                       void* stream, double* q);
+
 /* Bytes of device memory the context holds (arena capacity) and its peak use. */
 lvg_status lvg_memory(const lvg_ctx* ctx, int64_t* capacity, int64_t* peak);
 

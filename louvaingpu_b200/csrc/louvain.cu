@@ -1685,6 +1685,39 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
   return q;
 }
 
+// The modularity kernels of modularity_fp64 with every scratch array given by
+// the caller (used by the allocation-free entry point).  C <= 2048 * 2048.
+void modularity_fp64_scratch(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
+                             const int32_t* part, double* Kc, double* Ain, double* t, double* partials,
+                             double* twoW_q, cudaStream_t s) {
+  LVG_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * C, s));
+  LVG_CUDA(cudaMemsetAsync(Ain, 0, sizeof(double) * C, s));
+  if (E > 0 && C <= kNmSmemMax) {
+    size_t smem = sizeof(double) * 2 * (size_t)C;
+    if (smem > 48 * 1024)
+      LVG_CUDA(cudaFuncSetAttribute(nm_accum_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    nm_accum_smem_kernel<<<sm_grid(E, kThreads), kThreads, smem, s>>>(src, dst, w, E, part, C, Kc, Ain);
+    LVG_LAUNCH();
+  } else if (E > 0) {
+    nm_accum_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
+    LVG_LAUNCH();
+  }
+  // the fixed tree of tree_sum_f64, partials from the caller
+  auto tree = [&](const double* x, double* out) {
+    int64_t nb = ((int64_t)C + kGroup - 1) / kGroup;
+    tree_level_ctl_kernel<<<(unsigned)nb, kRedThreads, 0, s>>>(x, C, nb == 1 ? out : partials, nullptr, 0);
+    LVG_LAUNCH();
+    if (nb > 1) {
+      ctl_q_kernel<<<1, kRedThreads, 0, s>>>(partials, nb, out);
+      LVG_LAUNCH();
+    }
+  };
+  tree(Kc, twoW_q);
+  nm_term_kernel<<<sm_grid(C, kThreads), kThreads, 0, s>>>(Kc, Ain, C, twoW_q, t);
+  LVG_LAUNCH();
+  tree(t, twoW_q + 1);
+}
+
 void compose(int32_t* composed, const int32_t* part_level, int64_t n, cudaStream_t s) {
   if (n <= 0) return;
   compose_kernel<<<sm_grid(n, kThreads), kThreads, 0, s>>>(composed, part_level, n);

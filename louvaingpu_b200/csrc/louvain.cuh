@@ -148,6 +148,12 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
 double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
                        const int32_t* part, Arena& a, cudaStream_t s);
 
+// The same modularity with caller-provided scratch: Kc, Ain, t of C doubles,
+// partials of ceil(C/2048) doubles; twoW_q[0] = 2W, twoW_q[1] = Q (device).
+void modularity_fp64_scratch(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
+                             const int32_t* part, double* Kc, double* Ain, double* t, double* partials,
+                             double* twoW_q, cudaStream_t s);
+
 // part_out[i] = part_level[composed[i]] for i < n.
 void compose(int32_t* composed, const int32_t* part_level, int64_t n, cudaStream_t s);
 
