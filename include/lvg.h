@@ -172,6 +172,23 @@ lvg_status lvg_move_stats(const lvg_ctx* ctx, double* ms_total, int64_t* n_passe
 /* Number of CUDA kernels this library has launched in this process. */
 lvg_status lvg_kernel_launches(int64_t* n);
 
+/* Batched form: run the whole dendrogram of n_graphs independent graphs at
+ * once.  Graph g owns entries entry_off[g]..entry_off[g+1] of the HOST arrays
+ * src/dst/w, whose vertex ids are local to the graph (0..n_g-1), and
+ * n_g = vertex_off[g+1] - vertex_off[g] vertices.  Every graph gets exactly
+ * the result of its own lvg_run (same passes, levels, partitions): the graphs
+ * share launches, while m, the pass control, Q and the level break stay per
+ * graph.  Outputs (host, each nullable): part_out[vertex_off[n_graphs]] final
+ * community of every vertex (local to its graph), q_out[g] FP64 Newman
+ * modularity, levels_out[g], comms_out[g], status_out[g] (LVG_OK or
+ * LVG_ERR_NOT_CONVERGED).  A graph may have at most 2048*2048 vertices; the
+ * batch at most 2^31-1 entries.  The reference runs one graph per process
+ * (LouvainCPP.cpp:209); it has no batched form. */
+lvg_status lvg_batch_run(lvg_ctx* ctx, const int32_t* src, const int32_t* dst, const float* w,
+                         const int64_t* entry_off, const int32_t* vertex_off, int32_t n_graphs,
+                         int32_t* part_out, double* q_out, int32_t* levels_out, int32_t* comms_out,
+                         int32_t* status_out);
+
 /* Largest community count lvg_modularity_fp64_noalloc accepts. */
 #define LVG_NOALLOC_MAX_COMMS (1 << 18)
 

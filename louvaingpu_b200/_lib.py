@@ -96,6 +96,7 @@ SIGNATURES = {
     "lvg_move_stats": (i32, [P, ctypes.POINTER(dbl), ctypes.POINTER(i64)]),
     "lvg_kernel_launches": (i32, [ctypes.POINTER(i64)]),
     "lvg_memory": (i32, [P, ctypes.POINTER(i64), ctypes.POINTER(i64)]),
+    "lvg_batch_run": (i32, [P, P, P, P, P, P, i32, P, P, P, P, P]),
     "lvg_modularity_fp64_noalloc": (i32, [P, P, P, i64, P, i32, P, ctypes.POINTER(dbl)]),
 }
 

@@ -8,7 +8,9 @@
 // the device between levels (no host round trip, LouvainCPP.cpp:390-412,477-499).
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
+#include <numeric>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -773,3 +775,327 @@ lvg_status lvg_memory(const lvg_ctx* c, int64_t* capacity, int64_t* peak) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Batched runs (no counterpart in the reference, which runs one graph per
+// process, LouvainCPP.cpp:209): every level of every graph in one set of
+// launches over the disjoint union of the graphs still running.
+namespace {
+
+struct BatchLevel {
+  std::vector<int32_t> act;     // original graph of each level graph
+  std::vector<int32_t> vbase;   // [G+1] vertex ranges of the level graphs
+};
+
+void batch_run(lvg_ctx* c, const int32_t* lsrc, const int32_t* ldst, const float* w, const int64_t* eoff,
+               const int32_t* voff, int32_t G0, int32_t* part_out, double* q_out, int32_t* levels_out,
+               int32_t* comms_out, int32_t* status_out) {
+  cudaStream_t s = c->stream;
+  const int64_t E0 = eoff[G0];
+  const int32_t V0 = voff[G0];
+  for (int32_t g = 0; g < G0; ++g) {
+    require(eoff[g + 1] >= eoff[g] && voff[g + 1] >= voff[g], LVG_ERR_INVALID_ARG, "offsets must not decrease");
+    require((int64_t)(voff[g + 1] - voff[g]) <= (int64_t)kGroup * kGroup, LVG_ERR_CAPACITY,
+            "a batched graph may have at most 2048*2048 vertices");
+  }
+  require(E0 < ((int64_t)1 << 31), LVG_ERR_CAPACITY, "a batch may hold at most 2^31-1 entries");
+  drop_graphs(c);
+  c->loaded = false;
+  c->have_state = false;
+  size_t need = c->cfg.arena_bytes > 0 ? (size_t)c->cfg.arena_bytes : arena_estimate(V0, E0, true) + 256 * (size_t)G0 + 8 * (size_t)V0;
+  c->arena.reserve(need);
+  Arena& a = c->arena;
+  // level-0 union list with global vertex ids
+  int32_t* src0 = a.lo_n<int32_t>(E0);
+  int32_t* dst0 = a.lo_n<int32_t>(E0);
+  float* w0 = a.lo_n<float>(E0);
+  int32_t* gid0 = a.lo_n<int32_t>(V0);
+  int32_t* local0 = a.lo_n<int32_t>(V0);
+  {
+    HiScope hs(a);
+    int32_t* ls = a.hi_n<int32_t>(E0);
+    int32_t* ld = a.hi_n<int32_t>(E0);
+    int64_t* deoff = a.hi_n<int64_t>(G0 + 1);
+    int32_t* dvoff = a.hi_n<int32_t>(G0 + 1);
+    uint32_t* bad = a.hi_n<uint32_t>(1);
+    LVG_CUDA(cudaMemcpyAsync(ls, lsrc, sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(ld, ldst, sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(w0, w, sizeof(float) * E0, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(deoff, eoff, sizeof(int64_t) * (G0 + 1), cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(dvoff, voff, sizeof(int32_t) * (G0 + 1), cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), s));
+    batch_globalize(ls, ld, w0, E0, deoff, dvoff, G0, src0, dst0, bad, s);
+    batch_vgid(dvoff, G0, V0, gid0, s);
+    uint32_t h = 0;
+    LVG_CUDA(cudaMemcpyAsync(&h, bad, sizeof h, cudaMemcpyDeviceToHost, s));
+    sync(c);
+    require(h == 0, LVG_ERR_INVALID_ARG, "edge list has a vertex id out of its graph or a negative / non-finite weight");
+  }
+  {
+    std::vector<int32_t> l0(V0);
+    for (int32_t g = 0; g < G0; ++g)
+      for (int32_t v = voff[g]; v < voff[g + 1]; ++v) l0[v] = v - voff[g];
+    LVG_CUDA(cudaMemcpyAsync(local0, l0.data(), sizeof(int32_t) * V0, cudaMemcpyHostToDevice, s));
+    sync(c);
+  }
+  const size_t base_lo = a.lo;
+  std::vector<double> mod(G0, 0.0);
+  std::vector<int32_t> levels(G0, 0), comms(G0, 0), status(G0, 0);
+  BatchLevel L;
+  L.act.resize(G0);
+  std::iota(L.act.begin(), L.act.end(), 0);
+  L.vbase.assign(voff, voff + G0 + 1);
+  const int32_t *lsrc_d = src0, *ldst_d = dst0;
+  const float* lw_d = w0;
+  int64_t E = E0;
+  c->levels.clear();
+  for (int level = 0;; ++level) {
+    const int32_t G = (int32_t)L.act.size();
+    const int32_t V = L.vbase[G];
+    LevelGraph& g = c->g;
+    g = LevelGraph();
+    g.V = V;
+    g.E = E;
+    g.src = lsrc_d;
+    g.dst = ldst_d;
+    g.w = lw_d;
+    // per-level graph arrays
+    int32_t* vbase_d = a.lo_n<int32_t>(G + 1);
+    int32_t* vgid = a.lo_n<int32_t>(V);
+    double* gm = a.lo_n<double>(G);
+    LVG_CUDA(cudaMemcpyAsync(vbase_d, L.vbase.data(), sizeof(int32_t) * (G + 1), cudaMemcpyHostToDevice, s));
+    batch_vgid(vbase_d, G, V, vgid, s);
+    batch_m(lsrc_d, lw_d, E, vgid, gm, G, s);
+    g.gm = gm;
+    g.vgid = vgid;
+    build_level(g, c->tune, a, s);
+    CommState& st = c->st;
+    alloc_state(g, st, a);
+    // commit plan: groups of 2048 communities per graph
+    std::vector<int32_t> blk_g, blk_c0, gblk0(G + 1);
+    for (int32_t j = 0; j < G; ++j) {
+      gblk0[j] = (int32_t)blk_g.size();
+      for (int32_t c0 = L.vbase[j]; c0 < L.vbase[j + 1]; c0 += kGroup) {
+        blk_g.push_back(j);
+        blk_c0.push_back(c0);
+      }
+    }
+    gblk0[G] = (int32_t)blk_g.size();
+    BatchPlan bp;
+    bp.nblk = (int64_t)blk_g.size();
+    int32_t* d_blk_g = a.lo_n<int32_t>(bp.nblk);
+    int32_t* d_blk_c0 = a.lo_n<int32_t>(bp.nblk);
+    int32_t* d_gblk0 = a.lo_n<int32_t>(G + 1);
+    double* partials = a.lo_n<double>(bp.nblk);
+    LVG_CUDA(cudaMemcpyAsync(d_blk_g, blk_g.data(), sizeof(int32_t) * bp.nblk, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(d_blk_c0, blk_c0.data(), sizeof(int32_t) * bp.nblk, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(d_gblk0, gblk0.data(), sizeof(int32_t) * (G + 1), cudaMemcpyHostToDevice, s));
+    bp.vbase = vbase_d;
+    bp.blk_g = d_blk_g;
+    bp.blk_c0 = d_blk_c0;
+    bp.gblk0 = d_gblk0;
+    st.partials = partials;
+    // per-graph control
+    BatchCtl C;
+    C.q_prev = a.lo_n<double>(G);
+    C.cur = a.lo_n<double>(G);
+    C.lower = a.lo_n<double>(G);
+    C.q_ret = a.lo_n<double>(G);
+    int32_t* ints = a.lo_n<int32_t>(6 * (int64_t)G + 1);
+    C.pass = ints;
+    C.stop_now = ints + G;
+    C.done = ints + 2 * G;
+    C.status = ints + 3 * G;
+    C.passes = ints + 4 * G;
+    C.ndone = ints + 6 * G;
+    C.pass_min = c->cfg.pass_min_gain;
+    C.max_passes = c->cfg.max_passes;
+    st.gid = vgid;
+    st.gdone = C.done;
+    batch_init(g, st, s);
+    reset_ctl(st, 0.0, c->cfg.pass_min_gain, -1, s);
+    batch_commit(0, bp, gm, st, C, s);
+    batch_ctl(1, bp, st, C, G, s);
+    std::vector<double> q0(G), hv(G);
+    LVG_CUDA(cudaMemcpyAsync(q0.data(), C.q_prev, sizeof(double) * G, cudaMemcpyDeviceToHost, s));
+    sync(c);
+    for (int32_t j = 0; j < G; ++j) hv[j] = level == 0 ? q0[j] : mod[L.act[j]];   // lower (LouvainCPP.cpp:356,446)
+    LVG_CUDA(cudaMemcpyAsync(C.lower, hv.data(), sizeof(double) * G, cudaMemcpyHostToDevice, s));
+    std::fill(hv.begin(), hv.end(), -1.0);                                        // curMod = -1
+    LVG_CUDA(cudaMemcpyAsync(C.cur, hv.data(), sizeof(double) * G, cudaMemcpyHostToDevice, s));
+    // a graph without entries keeps its identity partition after one level
+    // (LouvainCPP.cpp:211-230): its pass loop is over before it starts
+    std::vector<int32_t> empty(G, 0);
+    int32_t n_empty = 0;
+    if (level == 0)
+      for (int32_t j = 0; j < G; ++j) n_empty += (empty[j] = eoff[j + 1] == eoff[j] ? 1 : 0);
+    {
+      std::vector<int32_t> iv(6 * (size_t)G + 1, 0);
+      for (int32_t j = 0; j < G; ++j) {
+        iv[j] = 1;                                                                 // pass 1
+        iv[2 * G + j] = empty[j];                                                  // done
+      }
+      iv[6 * G] = n_empty;                                                         // ndone
+      LVG_CUDA(cudaMemcpyAsync(ints, iv.data(), sizeof(int32_t) * iv.size(), cudaMemcpyHostToDevice, s));
+    }
+    // pass loop of all graphs
+    if (n_empty < G) {
+      L2Window l2(c, st);
+      const int chunk = c->cfg.passes_per_sync > 0 ? c->cfg.passes_per_sync : 4;
+      PassCtl h;
+      int launched = 0;
+      for (;;) {
+        for (int p = 0; p < chunk; ++p) {
+          launch_moves(g, st, s, &c->side);
+          batch_commit(1, bp, gm, st, C, s);
+          batch_ctl(0, bp, st, C, G, s);
+          ++launched;
+        }
+        LVG_CUDA(cudaMemcpyAsync(&h, st.ctl, sizeof h, cudaMemcpyDeviceToHost, s));
+        sync(c);
+        if (h.done) break;
+        if (h.err) throw Error(LVG_ERR_CAPACITY, "neighbour-community table probe limit exceeded");
+        if (launched >= kHardPassCap) throw Error(LVG_ERR_NOT_CONVERGED, "hard pass cap reached");
+      }
+    }
+    launch_merge_deltas(g, st, s);
+    batch_commit(2, bp, gm, st, C, s);
+    batch_ctl(2, bp, st, C, G, s);
+    std::vector<double> qret(G);
+    std::vector<int32_t> passes(G), stat(G);
+    LVG_CUDA(cudaMemcpyAsync(qret.data(), C.q_ret, sizeof(double) * G, cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaMemcpyAsync(passes.data(), C.passes, sizeof(int32_t) * G, cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaMemcpyAsync(stat.data(), C.status, sizeof(int32_t) * G, cudaMemcpyDeviceToHost, s));
+    // renumber, compose, decide who goes on
+    const size_t run_hi = a.hi;
+    int32_t* part = a.hi_n<int32_t>(V);
+    uint32_t* pos = a.hi_n<uint32_t>(V + 1);
+    int32_t Ctot = renumber_pos(g, st.comm, part, pos, a, s);
+    int32_t* cbase_d = a.hi_n<int32_t>(G + 1);
+    gather_u32(pos, vbase_d, G + 1, cbase_d, s);
+    std::vector<int32_t> cbase(G + 1);
+    LVG_CUDA(cudaMemcpyAsync(cbase.data(), cbase_d, sizeof(int32_t) * (G + 1), cudaMemcpyDeviceToHost, s));
+    int64_t* ecnt_d = a.hi_n<int64_t>(G);
+    batch_count(lsrc_d, E, vgid, ecnt_d, G, s);
+    std::vector<int64_t> ecnt(G);
+    LVG_CUDA(cudaMemcpyAsync(ecnt.data(), ecnt_d, sizeof(int64_t) * G, cudaMemcpyDeviceToHost, s));
+    std::vector<int32_t> lidx(G0, -1);
+    for (int32_t j = 0; j < G; ++j) lidx[L.act[j]] = j;
+    int32_t* lidx_d = a.hi_n<int32_t>(G0);
+    LVG_CUDA(cudaMemcpyAsync(lidx_d, lidx.data(), sizeof(int32_t) * G0, cudaMemcpyHostToDevice, s));
+    batch_compose(local0, gid0, V0, lidx_d, vbase_d, cbase_d, part, s);
+    sync(c);
+    (void)Ctot;
+    BatchLevel N;
+    std::vector<int32_t> shift(G, INT_MIN);
+    int64_t E_keep = 0;
+    N.vbase.push_back(0);
+    for (int32_t j = 0; j < G; ++j) {
+      const int32_t g0 = L.act[j];
+      const int32_t Cj = cbase[j + 1] - cbase[j];
+      levels[g0] = level + 1;
+      comms[g0] = Cj;
+      bool stop = stat[j] != LVG_OK || empty[j];
+      if (stop) status[g0] = stat[j];
+      if (!stop && level > 0 && (qret[j] - mod[g0]) < c->cfg.level_min_gain) stop = true;   // LouvainCPP.cpp:466
+      if (!stop && c->cfg.max_levels >= 0 && level + 1 >= c->cfg.max_levels) {
+        stop = true;
+        status[g0] = LVG_ERR_NOT_CONVERGED;
+      }
+      mod[g0] = qret[j];
+      if (!stop) {
+        shift[j] = N.vbase.back() - cbase[j];
+        N.act.push_back(g0);
+        N.vbase.push_back(N.vbase.back() + Cj);
+        E_keep += ecnt[j];
+      }
+    }
+    (void)passes;
+    if (N.act.empty()) {
+      a.hi = run_hi;
+      break;
+    }
+    int32_t* shift_d = a.hi_n<int32_t>(G);
+    LVG_CUDA(cudaMemcpyAsync(shift_d, shift.data(), sizeof(int32_t) * G, cudaMemcpyHostToDevice, s));
+    int32_t *os = nullptr, *od = nullptr;
+    float* ow = nullptr;
+    int64_t n = batch_induce(g, part, vgid, shift_d, N.vbase.back(), E_keep, &os, &od, &ow, a, s);
+    a.lo = base_lo;
+    int32_t* ns = a.lo_n<int32_t>(n);
+    int32_t* nd = a.lo_n<int32_t>(n);
+    float* nw = a.lo_n<float>(n);
+    if (n > 0) {
+      LVG_CUDA(cudaMemcpyAsync(ns, os, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+      LVG_CUDA(cudaMemcpyAsync(nd, od, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+      LVG_CUDA(cudaMemcpyAsync(nw, ow, sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+    }
+    sync(c);
+    a.hi = run_hi;
+    lsrc_d = ns;
+    ldst_d = nd;
+    lw_d = nw;
+    E = n;
+    L = std::move(N);
+  }
+  // per-graph FP64 Newman modularity of the final partitions
+  {
+    std::vector<int32_t> coff(G0 + 1, 0);
+    for (int32_t g0 = 0; g0 < G0; ++g0) coff[g0 + 1] = coff[g0] + comms[g0];
+    const int32_t Ctot = coff[G0];
+    std::vector<int32_t> cg(std::max(Ctot, 1), 0), blk_g, blk_c0, gblk0(G0 + 1);
+    for (int32_t g0 = 0; g0 < G0; ++g0) {
+      gblk0[g0] = (int32_t)blk_g.size();
+      for (int32_t k = coff[g0]; k < coff[g0 + 1]; ++k) cg[k] = g0;
+      for (int32_t c0 = coff[g0]; c0 < coff[g0 + 1]; c0 += kGroup) {
+        blk_g.push_back(g0);
+        blk_c0.push_back(c0);
+      }
+    }
+    gblk0[G0] = (int32_t)blk_g.size();
+    HiScope hs(a);
+    BatchPlan cp;
+    cp.nblk = (int64_t)blk_g.size();
+    int32_t* coff_d = a.hi_n<int32_t>(G0 + 1);
+    int32_t* cg_d = a.hi_n<int32_t>(std::max(Ctot, 1));
+    int32_t* bg_d = a.hi_n<int32_t>(std::max<int64_t>(cp.nblk, 1));
+    int32_t* bc_d = a.hi_n<int32_t>(std::max<int64_t>(cp.nblk, 1));
+    int32_t* gb_d = a.hi_n<int32_t>(G0 + 1);
+    double* q_d = a.hi_n<double>(G0);
+    LVG_CUDA(cudaMemcpyAsync(coff_d, coff.data(), sizeof(int32_t) * (G0 + 1), cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(cg_d, cg.data(), sizeof(int32_t) * cg.size(), cudaMemcpyHostToDevice, s));
+    if (cp.nblk > 0) {
+      LVG_CUDA(cudaMemcpyAsync(bg_d, blk_g.data(), sizeof(int32_t) * cp.nblk, cudaMemcpyHostToDevice, s));
+      LVG_CUDA(cudaMemcpyAsync(bc_d, blk_c0.data(), sizeof(int32_t) * cp.nblk, cudaMemcpyHostToDevice, s));
+    }
+    LVG_CUDA(cudaMemcpyAsync(gb_d, gblk0.data(), sizeof(int32_t) * (G0 + 1), cudaMemcpyHostToDevice, s));
+    cp.vbase = coff_d;
+    cp.blk_g = bg_d;
+    cp.blk_c0 = bc_d;
+    cp.gblk0 = gb_d;
+    batch_modularity(src0, dst0, w0, E0, gid0, local0, cp, cg_d, Ctot, G0, q_d, a, s);
+    if (q_out) LVG_CUDA(cudaMemcpyAsync(q_out, q_d, sizeof(double) * G0, cudaMemcpyDeviceToHost, s));
+    if (part_out && V0 > 0)
+      LVG_CUDA(cudaMemcpyAsync(part_out, local0, sizeof(int32_t) * V0, cudaMemcpyDeviceToHost, s));
+    sync(c);
+  }
+  if (levels_out) std::copy(levels.begin(), levels.end(), levels_out);
+  if (comms_out) std::copy(comms.begin(), comms.end(), comms_out);
+  if (status_out) std::copy(status.begin(), status.end(), status_out);
+  c->g = LevelGraph();
+  c->st = CommState();
+}
+
+}  // namespace
+
+extern "C" lvg_status lvg_batch_run(lvg_ctx* c, const int32_t* src, const int32_t* dst, const float* w,
+                                    const int64_t* entry_off, const int32_t* vertex_off, int32_t n_graphs,
+                                    int32_t* part_out, double* q_out, int32_t* levels_out, int32_t* comms_out,
+                                    int32_t* status_out) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(n_graphs >= 1 && entry_off && vertex_off, LVG_ERR_INVALID_ARG, "need at least one graph and offsets");
+    require(entry_off[0] == 0 && vertex_off[0] == 0, LVG_ERR_INVALID_ARG, "offsets must start at 0");
+    require(entry_off[n_graphs] == 0 || (src && dst && w), LVG_ERR_INVALID_ARG, "null edge array");
+    batch_run(c, src, dst, w, entry_off, vertex_off, n_graphs, part_out, q_out, levels_out, comms_out, status_out);
+  });
+}

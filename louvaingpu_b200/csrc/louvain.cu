@@ -24,6 +24,15 @@ struct HubPartial {
   int32_t c, n;
 };
 
+// Static per-vertex facts of a level, copied in degree-class item order so
+// that a class kernel streams them instead of gathering them by vertex id.
+struct VInfo {
+  double kfrac;
+  double k;
+  float loopw;
+  int32_t vid_loop;   // vertex id << 1 | has_loop
+};
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -129,9 +138,14 @@ __global__ void csr_emit_kernel(const uint64_t* keys, const float* vals, int64_t
 // Sort-free build: a level list that is strictly sorted by (src, dst) and
 // symmetric with bitwise-equal weights doubles into each entry twice, so the
 // merged CSR row of u is its list row without the self loop, weights 2w.
+// Entries per row; runs of equal rows inside a warp add once.  Grid covers E
+// in whole warps.
 __global__ void row_count_kernel(const int32_t* src, int64_t E, int64_t* rowcnt) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
-    atomicAdd((unsigned long long*)&rowcnt[src[e]], 1ull);
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool valid = e < E;
+  int64_t u = valid ? src[e] : -1;
+  double n = seg_warp_sum<int64_t>(valid ? 1.0 : 0.0, u);
+  if (seg_warp_last<int64_t>(u, valid)) atomicAdd((unsigned long long*)&rowcnt[u], (unsigned long long)n);
 }
 
 enum : uint32_t { kNotSorted = 1u, kNotSymmetric = 2u };
@@ -297,6 +311,8 @@ struct MoveArgs {
   double* din;
   int32_t* dsize;
   PassCtl* ctl;
+  const int32_t* gid;    // batched runs: graph of each vertex (nullptr for one graph)
+  const int32_t* gdone;  // batched runs: 1 once a graph's level loop has stopped
 };
 
 // Candidate order: higher gain first, then lower community id
@@ -328,8 +344,29 @@ __device__ __forceinline__ void warp_best(double& bg, int32_t& bc, double& bw) {
 // (OneLevelKernel.cu:407-410), remove/insert into the delta buffers
 // (OneLevelKernel.cu:52-78, 412-421) and the isolated-merge candidate
 // (OneLevelKernel.cu:142-169).
+__device__ __forceinline__ void apply_decision_kl(const MoveArgs& P, int32_t i, int32_t own, int32_t bc, double bw,
+                                                  int32_t nseg, double ki, float loopw) {
+  if (P.gdone && P.gdone[P.gid[i]]) return;   // that graph's pass loop has stopped
+  int32_t raw = bc == kNone ? own : bc;
+  int32_t so = P.size[own], sb = P.size[raw];
+  int32_t best = raw;
+  if (so == 1 && sb == 1 && raw > own) best = own;
+  P.next[i] = best;
+  P.cand[i] = (so == 1 && nseg == 1 && raw != own && own < raw) ? raw : -1;
+  if (best != own) {
+    double iw = __dadd_rn(bw, (double)loopw);
+    atomicAdd(&P.dtot[own], -ki);
+    atomicAdd(&P.dtot[best], ki);
+    atomicAdd(&P.din[own], -iw);
+    atomicAdd(&P.din[best], iw);
+    atomicAdd(&P.dsize[own], -1);
+    atomicAdd(&P.dsize[best], 1);
+  }
+}
+
 __device__ __forceinline__ void apply_decision(const MoveArgs& P, int32_t i, int32_t own, int32_t bc, double bw,
                                                int32_t nseg) {
+  if (P.gdone && P.gdone[P.gid[i]]) return;   // that graph's pass loop has stopped
   int32_t raw = bc == kNone ? own : bc;
   int32_t so = P.size[own], sb = P.size[raw];
   int32_t best = raw;
@@ -429,6 +466,7 @@ struct EllArgs {
   const int32_t* col;   // [n * G] neighbour of each slot, -1 for padding
   const float* w;       // [n * G]
   const int32_t* list;  // [n] vertex of each item
+  const VInfo* info;    // [n] static facts of each item's vertex, in item order
   int64_t n;
 };
 
@@ -480,11 +518,12 @@ __global__ void __launch_bounds__(kThreads) move_thread_kernel(MoveArgs P, EllAr
       c[4 * q] = a.x; c[4 * q + 1] = a.y; c[4 * q + 2] = a.z; c[4 * q + 3] = a.w;
       w[4 * q] = b.x; w[4 * q + 1] = b.y; w[4 * q + 2] = b.z; w[4 * q + 3] = b.w;
     }
-    const int32_t i = L.list[j];
+    const VInfo vi = L.info[j];
+    const int32_t i = vi.vid_loop >> 1;
 #pragma unroll
     for (int q = 0; q < D; ++q) c[q] = c[q] >= 0 ? P.comm[c[q]] : kNone;
     const int32_t own = P.comm[i];
-    const double kf = P.kfrac[i];
+    const double kf = vi.kfrac;
     bitonic_sort<D>(c, w);
     double bg = 0.0, bw = 0.0, run = 0.0;
     int32_t bc = kNone;
@@ -503,8 +542,30 @@ __global__ void __launch_bounds__(kThreads) move_thread_kernel(MoveArgs P, EllAr
         if (g > 0.0 && g > bg) { bg = g; bc = c[q]; bw = run; }
       }
     }
-    nseg += (P.has_loop[i] && !sawown) ? 1 : 0;
-    apply_decision(P, i, own, bc, bw, nseg);
+    nseg += ((vi.vid_loop & 1) && !sawown) ? 1 : 0;
+    apply_decision_kl(P, i, own, bc, bw, nseg, vi.k, vi.loopw);
+  }
+}
+
+// k/2m; in a batched run m is the vertex's own graph's (gm[vgid[i]]).
+__global__ void kfrac_kernel(int32_t V, const double* k, double m, const double* gm, const int32_t* vgid,
+                             double* kfrac) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+    double mi = gm ? gm[vgid[i]] : m;
+    kfrac[i] = mi > 0.0 ? __ddiv_rn(k[i], __dmul_rn(2.0, mi)) : 0.0;   // OneLevelKernel.cu:307
+  }
+}
+
+__global__ void vinfo_fill_kernel(const int32_t* list, int64_t n, const double* kfrac, const double* k,
+                                  const float* loopw, const uint8_t* has_loop, VInfo* info) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    int32_t i = list[j];
+    VInfo v;
+    v.kfrac = kfrac[i];
+    v.k = k[i];
+    v.loopw = loopw[i];
+    v.vid_loop = (i << 1) | (has_loop[i] ? 1 : 0);
+    info[j] = v;
   }
 }
 
@@ -1107,6 +1168,8 @@ MoveArgs move_args(const LevelGraph& g, CommState& st) {
   P.next = st.next; P.cand = st.cand;
   P.dtot = st.dtot; P.din = st.din; P.dsize = st.dsize;
   P.ctl = st.ctl;
+  P.gid = st.gid;
+  P.gdone = st.gdone;
   return P;
 }
 
@@ -1147,7 +1210,7 @@ static bool build_csr_fast(LevelGraph& g, Arena& a, cudaStream_t s) {
   uint32_t* flags = a.hi_n<uint32_t>(1);
   LVG_CUDA(cudaMemsetAsync(rowstart, 0, sizeof(int64_t) * (V + 1), s));
   LVG_CUDA(cudaMemsetAsync(flags, 0, sizeof(uint32_t), s));
-  row_count_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, E, rowstart);
+  row_count_kernel<<<grid_for(E, kThreads), kThreads, 0, s>>>(g.src, E, rowstart);
   LVG_LAUNCH();
   scan_i64(rowstart, rowstart, V, a, s);
   list_check_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, g.w, E, rowstart, flags);
@@ -1279,6 +1342,20 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
       ell_fill_kernel<<<sm_grid(nb * G, kThreads), kThreads, 0, s>>>(g.blist + g.bstart[b], g.off, g.col, g.cw, nb,
                                                                       G, g.ell_col + g.ell_base[b],
                                                                       g.ell_w + g.ell_base[b]);
+      LVG_LAUNCH();
+    }
+  }
+  // k/2m and the class-ordered vertex facts of the thread kernels
+  if (V > 0) {
+    kfrac_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, g.k, g.m, g.gm, g.vgid, g.kfrac);
+    LVG_LAUNCH();
+  }
+  {
+    int64_t nitems = g.bstart[kB32] + g.nbucket[kB32] - g.bstart[kB4];
+    g.ell_info = a.lo_n<VInfo>(nitems);
+    if (nitems > 0) {
+      vinfo_fill_kernel<<<sm_grid(nitems, kThreads), kThreads, 0, s>>>(g.blist + g.bstart[kB4], nitems, g.kfrac, g.k,
+                                                                       g.loopw, g.has_loop, g.ell_info);
       LVG_LAUNCH();
     }
   }
@@ -1472,6 +1549,7 @@ static void launch_thread(const LevelGraph& g, MoveArgs P, int bucket, cudaStrea
   L.col = g.ell_col + g.ell_base[bucket];
   L.w = g.ell_w + g.ell_base[bucket];
   L.list = g.blist + g.bstart[bucket];
+  L.info = g.ell_info + (g.bstart[bucket] - g.bstart[kB4]);
   int64_t blocks = std::min<int64_t>((L.n + kThreads - 1) / kThreads, (int64_t)sm_count() * 8);
   move_thread_kernel<D><<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, 0, s>>>(P, L);
   LVG_LAUNCH();
@@ -1721,6 +1799,434 @@ void modularity_fp64_scratch(const int32_t* src, const int32_t* dst, const float
 void compose(int32_t* composed, const int32_t* part_level, int64_t n, cudaStream_t s) {
   if (n <= 0) return;
   compose_kernel<<<sm_grid(n, kThreads), kThreads, 0, s>>>(composed, part_level, n);
+  LVG_LAUNCH();
+}
+
+}  // namespace lvg
+
+// ============================================================================
+// Batched runs: many independent graphs as one disjoint-union level graph.
+// Graphs occupy contiguous vertex ranges vbase[j]..vbase[j+1]; everything a
+// single run keeps as a scalar (m, the pass control, Q, the level break) is
+// kept per graph, and the Q of a graph is summed on the same fixed tree as a
+// single run over its own communities.
+namespace lvg {
+namespace {
+
+__global__ void batch_globalize_kernel(const int32_t* lsrc, const int32_t* ldst, const float* w, int64_t E,
+                                       const int64_t* eoff, const int32_t* voff, int32_t G, int32_t* gsrc,
+                                       int32_t* gdst, uint32_t* bad) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = G - 1;
+    while (lo < hi) {  // last graph whose first entry is <= e
+      int mid = (lo + hi + 1) >> 1;
+      if (eoff[mid] <= e) lo = mid; else hi = mid - 1;
+    }
+    int32_t n = voff[lo + 1] - voff[lo];
+    int32_t a = lsrc[e], b = ldst[e];
+    float x = w[e];
+    if (a < 0 || a >= n || b < 0 || b >= n || !(x >= 0.0f) || isinf(x)) atomicOr(bad, 1u);
+    gsrc[e] = a + voff[lo];
+    gdst[e] = b + voff[lo];
+  }
+}
+
+__global__ void vgid_fill_kernel(const int32_t* vbase, int32_t G, int32_t V, int32_t* vgid) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = G - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (vbase[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    vgid[i] = lo;
+  }
+}
+
+// m of every graph: runs of entries of one graph inside a warp add once.
+__global__ void batch_m_kernel(const int32_t* src, const float* w, int64_t E, const int32_t* vgid, double* gm) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool valid = e < E;
+  int64_t g = valid ? vgid[src[e]] : -1;
+  double x = seg_warp_sum<int64_t>(valid ? (double)w[e] : 0.0, g);
+  if (seg_warp_last<int64_t>(g, valid)) atomicAdd(&gm[g], x);
+}
+
+__global__ void batch_init_kernel(int32_t V, const double* k, const float* loopw, int32_t* comm, int32_t* next,
+                                  double* tot, double* in, int32_t* size, double* dtot, double* din, int32_t* dsize,
+                                  int32_t* cand) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
+    comm[i] = (int32_t)i;
+    next[i] = (int32_t)i;
+    tot[i] = k[i];
+    in[i] = (double)loopw[i];
+    size[i] = 1;
+    dtot[i] = 0.0; din[i] = 0.0; dsize[i] = 0;
+    cand[i] = -1;
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kRedThreads) batch_commit_kernel(
+    const int32_t* blk_g, const int32_t* blk_c0, const int32_t* vbase, const double* gm, int32_t* comm,
+    const int32_t* next, double* tot, double* in, int32_t* size, double* dtot, double* din, int32_t* dsize,
+    double* partials, BatchCtl C) {
+  __shared__ double ws[8];
+  const int32_t g = blk_g[blockIdx.x];
+  const int64_t c0 = blk_c0[blockIdx.x];
+  const int64_t cend = vbase[g + 1];
+  const int64_t base = c0 + threadIdx.x;
+  if (MODE == kCommitPass) {
+    if (C.done[g]) return;
+    bool stop = __dsub_rn(C.q_prev[g], C.cur[g]) < C.pass_min;
+    bool capped = C.max_passes >= 0 && C.pass[g] >= C.max_passes;
+    if (stop || capped) {
+      for (int j = 0; j < 8; ++j) {
+        int64_t c = base + (int64_t)j * 256;
+        if (c < cend) { dtot[c] = 0.0; din[c] = 0.0; dsize[c] = 0; }
+      }
+      if (c0 == vbase[g] && threadIdx.x == 0) C.stop_now[g] = stop ? 1 : 2;
+      return;
+    }
+  }
+  const double m = gm[g];
+  const double twom = __dmul_rn(2.0, m);
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    int64_t c = base + (int64_t)j * 256;
+    if (c < cend) {
+      double t, x;
+      if (MODE != kCommitInit) {
+        t = __dadd_rn(tot[c], dtot[c]);
+        x = __dadd_rn(in[c], din[c]);
+        tot[c] = t; in[c] = x;
+        size[c] += dsize[c];
+        dtot[c] = 0.0; din[c] = 0.0; dsize[c] = 0;
+        comm[c] = next[c];
+      } else {
+        t = tot[c]; x = in[c];
+      }
+      s = __dadd_rn(s, q_term(x, t, m, twom));
+    }
+  }
+  double r = block_tree256(s, ws);
+  if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+
+enum { kBatchCtlPass = 0, kBatchCtlInit = 1, kBatchCtlRet = 2 };
+
+template <int MODE>
+__global__ void __launch_bounds__(kRedThreads) batch_ctl_kernel(const int32_t* gblk0, const double* partials,
+                                                                BatchCtl C, int32_t G, PassCtl* ctl) {
+  __shared__ double ws[8];
+  __shared__ int flag;
+  const int32_t g = blockIdx.x;
+  if (MODE == kBatchCtlPass) {
+    if (threadIdx.x == 0) flag = C.done[g] ? 2 : (C.stop_now[g] ? 1 : 0);
+    __syncthreads();
+    int f = flag;
+    if (f == 2) return;
+    if (f == 1) {
+      if (threadIdx.x == 0) {
+        C.status[g] = C.stop_now[g] == 2 ? LVG_ERR_NOT_CONVERGED : LVG_OK;
+        C.passes[g] = C.pass[g];
+        C.stop_now[g] = 0;
+        C.done[g] = 1;
+        __threadfence();
+        if (atomicAdd(C.ndone, 1) + 1 == G) ctl->done = 1;
+      }
+      return;
+    }
+  }
+  double q = group_sum_block<double>(partials + gblk0[g], gblk0[g + 1] - gblk0[g], ws);
+  if (threadIdx.x == 0) {
+    if (MODE == kBatchCtlPass) {
+      double cur = C.q_prev[g];
+      if (cur < C.lower[g]) cur = C.lower[g];
+      C.cur[g] = cur;
+      C.q_prev[g] = q;
+      C.pass[g] += 1;
+    } else if (MODE == kBatchCtlInit) {
+      C.q_prev[g] = q;
+    } else {
+      C.q_ret[g] = q;
+    }
+  }
+}
+
+__global__ void batch_keys_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                  const int32_t* part, const int32_t* vgid, const int32_t* shift, int B,
+                                  uint64_t* keys, float* vals) {
+  const uint64_t sentinel = (B >= 32) ? ~0ull : ((1ull << (2 * B)) - 1);
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    int32_t j = vgid[src[e]];
+    int32_t sh = shift[j];
+    if (sh == INT_MIN) {            // graph finished at this level: dropped
+      keys[e] = sentinel;
+      vals[e] = 0.0f;
+      continue;
+    }
+    uint64_t a = (uint32_t)(part[src[e]] + sh), b = (uint32_t)(part[dst[e]] + sh);
+    keys[e] = (a << B) | b;
+    float x = w[e];
+    vals[e] = x == 0.0f ? 1.0f : x;   // InducedGraphKernel.cu:38-39
+  }
+}
+
+__global__ void gather_u32_kernel(const uint32_t* pos, const int32_t* idx, int32_t n, int32_t* out) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+    out[j] = (int32_t)pos[idx[j]];
+}
+
+__global__ void batch_count_kernel(const int32_t* src, int64_t E, const int32_t* vgid, int64_t* cnt) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool valid = e < E;
+  int64_t g = valid ? vgid[src[e]] : -1;
+  double x = seg_warp_sum<int64_t>(valid ? 1.0 : 0.0, g);
+  if (seg_warp_last<int64_t>(g, valid)) atomicAdd((unsigned long long*)&cnt[g], (unsigned long long)x);
+}
+
+__global__ void batch_compose_kernel(int32_t* local0, const int32_t* gid0, int64_t n, const int32_t* lidx,
+                                     const int32_t* vbase, const int32_t* cbase, const int32_t* part) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    int32_t j = lidx[gid0[v]];
+    if (j >= 0) local0[v] = part[vbase[j] + local0[v]] - cbase[j];
+  }
+}
+
+// Newman modularity per graph over its level-0 entries (global community
+// ids coff[g] + local id).
+__global__ void batch_nm_accum_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                      const int32_t* gid0, const int32_t* local0, const int32_t* coff, double* Kc,
+                                      double* Ain) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    int32_t g = gid0[src[e]];
+    double x = (double)w[e];
+    int32_t a = coff[g] + local0[src[e]], b = coff[g] + local0[dst[e]];
+    atomicAdd(&Kc[a], x);
+    atomicAdd(&Kc[b], x);
+    if (a == b) atomicAdd(&Ain[a], 2.0 * x);
+  }
+}
+
+// Per-graph fixed-tree sums: block b sums x over communities blk_c0[b] ..
+// min(+2048, end of its graph), the same tree as one graph's tree_sum_f64.
+__global__ void __launch_bounds__(kRedThreads) batch_group_kernel(const double* x, const int32_t* blk_g,
+                                                                  const int32_t* blk_c0, const int32_t* cbeg,
+                                                                  double* partials) {
+  __shared__ double ws[8];
+  const int32_t g = blk_g[blockIdx.x];
+  const int64_t c0 = blk_c0[blockIdx.x];
+  double r = group_sum_block<double>(x + c0, (int64_t)cbeg[g + 1] - c0, ws);
+  if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+
+__global__ void __launch_bounds__(kRedThreads) batch_finish_kernel(const double* partials, const int32_t* gblk0,
+                                                                   double* out) {
+  __shared__ double ws[8];
+  const int32_t g = blockIdx.x;
+  const int32_t n = gblk0[g + 1] - gblk0[g];
+  double r = n == 1 ? partials[gblk0[g]] : group_sum_block<double>(partials + gblk0[g], n, ws);
+  if (threadIdx.x == 0) out[g] = n == 0 ? 0.0 : r;
+}
+
+__global__ void batch_nm_term_kernel(const double* Kc, const double* Ain, const int32_t* cg, int32_t C,
+                                     const double* twoW, double* t) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C; c += (int64_t)gridDim.x * blockDim.x) {
+    double tw = twoW[cg[c]];
+    double f = __ddiv_rn(Kc[c], tw);
+    t[c] = tw > 0.0 ? __dsub_rn(__ddiv_rn(Ain[c], tw), __dmul_rn(f, f)) : 0.0;
+  }
+}
+
+}  // namespace
+
+void batch_globalize(const int32_t* lsrc, const int32_t* ldst, const float* w, int64_t E, const int64_t* eoff,
+                     const int32_t* voff, int32_t G, int32_t* gsrc, int32_t* gdst, uint32_t* bad, cudaStream_t s) {
+  if (E == 0) return;
+  batch_globalize_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(lsrc, ldst, w, E, eoff, voff, G, gsrc, gdst, bad);
+  LVG_LAUNCH();
+}
+
+void batch_vgid(const int32_t* vbase, int32_t G, int32_t V, int32_t* vgid, cudaStream_t s) {
+  if (V == 0) return;
+  vgid_fill_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(vbase, G, V, vgid);
+  LVG_LAUNCH();
+}
+
+void batch_m(const int32_t* src, const float* w, int64_t E, const int32_t* vgid, double* gm, int32_t G,
+             cudaStream_t s) {
+  LVG_CUDA(cudaMemsetAsync(gm, 0, sizeof(double) * std::max(G, 1), s));
+  if (E == 0) return;
+  batch_m_kernel<<<grid_for(E, kThreads), kThreads, 0, s>>>(src, w, E, vgid, gm);
+  LVG_LAUNCH();
+}
+
+void batch_init(const LevelGraph& g, CommState& st, cudaStream_t s) {
+  if (g.V == 0) return;
+  batch_init_kernel<<<sm_grid(g.V, kThreads), kThreads, 0, s>>>(g.V, g.k, g.loopw, st.comm, st.next, st.tot, st.in,
+                                                                st.size, st.dtot, st.din, st.dsize, st.cand);
+  LVG_LAUNCH();
+}
+
+void batch_commit(int mode, const BatchPlan& bp, const double* gm, CommState& st, const BatchCtl& C,
+                  cudaStream_t s) {
+  const unsigned nb = (unsigned)bp.nblk;
+  if (nb == 0) return;
+  if (mode == kCommitInit)
+    batch_commit_kernel<kCommitInit><<<nb, kRedThreads, 0, s>>>(bp.blk_g, bp.blk_c0, bp.vbase, gm, st.comm, st.next,
+                                                                st.tot, st.in, st.size, st.dtot, st.din, st.dsize,
+                                                                st.partials, C);
+  else if (mode == kCommitPass)
+    batch_commit_kernel<kCommitPass><<<nb, kRedThreads, 0, s>>>(bp.blk_g, bp.blk_c0, bp.vbase, gm, st.comm, st.next,
+                                                                st.tot, st.in, st.size, st.dtot, st.din, st.dsize,
+                                                                st.partials, C);
+  else
+    batch_commit_kernel<kCommitForce><<<nb, kRedThreads, 0, s>>>(bp.blk_g, bp.blk_c0, bp.vbase, gm, st.comm,
+                                                                 st.next, st.tot, st.in, st.size, st.dtot, st.din,
+                                                                 st.dsize, st.partials, C);
+  LVG_LAUNCH();
+}
+
+void batch_ctl(int mode, const BatchPlan& bp, const CommState& st, const BatchCtl& C, int32_t G, cudaStream_t s) {
+  if (G == 0) return;
+  if (mode == 0) batch_ctl_kernel<kBatchCtlPass><<<G, kRedThreads, 0, s>>>(bp.gblk0, st.partials, C, G, st.ctl);
+  else if (mode == 1) batch_ctl_kernel<kBatchCtlInit><<<G, kRedThreads, 0, s>>>(bp.gblk0, st.partials, C, G, st.ctl);
+  else batch_ctl_kernel<kBatchCtlRet><<<G, kRedThreads, 0, s>>>(bp.gblk0, st.partials, C, G, st.ctl);
+  LVG_LAUNCH();
+}
+
+void launch_merge_deltas(const LevelGraph& g, CommState& st, cudaStream_t s) {
+  if (g.V == 0) return;
+  merge_kernel<<<sm_grid(g.V, kThreads), kThreads, 0, s>>>(g.V, st.comm, st.next, st.cand, g.k, g.loopw, st.dtot,
+                                                          st.din, st.dsize);
+  LVG_LAUNCH();
+}
+
+int32_t renumber_pos(const LevelGraph& g, const int32_t* comm, int32_t* part, uint32_t* pos, Arena& a,
+                     cudaStream_t s) {
+  const int32_t V = g.V;
+  if (V == 0) return 0;
+  HiScope hs(a);
+  int32_t* minidx = a.hi_n<int32_t>(V);
+  uint32_t* flag = a.hi_n<uint32_t>(V + 1);
+  LVG_CUDA(cudaMemsetAsync(minidx, 0x7f, sizeof(int32_t) * V, s));
+  min_member_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, comm, minidx);
+  LVG_LAUNCH();
+  head_flag_kernel<<<grid_for(V, kThreads), kThreads, 0, s>>>(V, comm, minidx, flag);
+  LVG_LAUNCH();
+  scan_u32(flag, pos, V, a, s);
+  renumber_apply_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, comm, flag, pos, minidx);
+  LVG_LAUNCH();
+  gather_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, comm, minidx, part);
+  LVG_LAUNCH();
+  uint32_t C = 0;
+  LVG_CUDA(cudaMemcpyAsync(&C, pos + V, sizeof C, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  return (int32_t)C;
+}
+
+int64_t batch_induce(const LevelGraph& g, const int32_t* part, const int32_t* vgid, const int32_t* shift,
+                     int32_t C_next, int64_t E_keep, int32_t** out_src, int32_t** out_dst, float** out_w, Arena& a,
+                     cudaStream_t s) {
+  const int64_t E = g.E;
+  if (E >= ((int64_t)1 << 32)) throw Error(LVG_ERR_CAPACITY, "level edge list exceeds 2^32-1 entries");
+  int32_t* osrc = a.hi_n<int32_t>(E_keep);
+  int32_t* odst = a.hi_n<int32_t>(E_keep);
+  float* ow = a.hi_n<float>(E_keep);
+  int64_t cnt = 0;
+  {
+    HiScope hs(a);
+    const int B = std::max(1, bits_for((int64_t)C_next + 1));
+    uint64_t* k0 = a.hi_n<uint64_t>(E);
+    float* v0 = a.hi_n<float>(E);
+    uint64_t* k1 = a.hi_n<uint64_t>(E);
+    float* v1 = a.hi_n<float>(E);
+    uint32_t* head = a.hi_n<uint32_t>(E_keep + 1);
+    uint32_t* pos = a.hi_n<uint32_t>(E_keep + 1);
+    double* wsum = a.hi_n<double>(E_keep);
+    if (E > 0) {
+      batch_keys_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, g.w, E, part, vgid, shift, B, k0, v0);
+      LVG_LAUNCH();
+    }
+    int which = radix_sort_pairs(k0, v0, k1, v1, E, 2 * B, a, s);
+    uint64_t* keys = which ? k1 : k0;
+    float* vals = which ? v1 : v0;
+    if (E_keep > 0) {
+      run_head_kernel<<<sm_grid(E_keep, kThreads), kThreads, 0, s>>>(keys, E_keep, head);
+      LVG_LAUNCH();
+    }
+    scan_u32(head, pos, E_keep, a, s);
+    uint32_t n_out = 0;
+    LVG_CUDA(cudaMemcpyAsync(&n_out, pos + E_keep, sizeof n_out, cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaStreamSynchronize(s));
+    cnt = n_out;
+    LVG_CUDA(cudaMemsetAsync(wsum, 0, sizeof(double) * std::max<int64_t>(cnt, 1), s));
+    if (E_keep > 0) {
+      run_sum_kernel<<<grid_for(E_keep, kThreads), kThreads, 0, s>>>(keys, vals, E_keep, B, pos, head, osrc, odst,
+                                                                       wsum);
+      LVG_LAUNCH();
+    }
+    if (cnt > 0) {
+      to_float_kernel<<<sm_grid(cnt, kThreads), kThreads, 0, s>>>(wsum, ow, cnt);
+      LVG_LAUNCH();
+    }
+    LVG_CUDA(cudaStreamSynchronize(s));
+  }
+  *out_src = osrc;
+  *out_dst = odst;
+  *out_w = ow;
+  return cnt;
+}
+
+void gather_u32(const uint32_t* pos, const int32_t* idx, int32_t n, int32_t* out, cudaStream_t s) {
+  if (n == 0) return;
+  gather_u32_kernel<<<sm_grid(n, kThreads), kThreads, 0, s>>>(pos, idx, n, out);
+  LVG_LAUNCH();
+}
+
+void batch_count(const int32_t* src, int64_t E, const int32_t* vgid, int64_t* cnt, int32_t G, cudaStream_t s) {
+  LVG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int64_t) * std::max(G, 1), s));
+  if (E == 0) return;
+  batch_count_kernel<<<grid_for(E, kThreads), kThreads, 0, s>>>(src, E, vgid, cnt);
+  LVG_LAUNCH();
+}
+
+void batch_compose(int32_t* local0, const int32_t* gid0, int64_t n, const int32_t* lidx, const int32_t* vbase,
+                   const int32_t* cbase, const int32_t* part, cudaStream_t s) {
+  if (n == 0) return;
+  batch_compose_kernel<<<sm_grid(n, kThreads), kThreads, 0, s>>>(local0, gid0, n, lidx, vbase, cbase, part);
+  LVG_LAUNCH();
+}
+
+void batch_modularity(const int32_t* src, const int32_t* dst, const float* w, int64_t E, const int32_t* gid0,
+                      const int32_t* local0, const BatchPlan& cp, const int32_t* cg, int32_t Ctot, int32_t G,
+                      double* q, Arena& a, cudaStream_t s) {
+  HiScope hs(a);
+  double* Kc = a.hi_n<double>(Ctot);
+  double* Ain = a.hi_n<double>(Ctot);
+  double* t = a.hi_n<double>(Ctot);
+  double* partials = a.hi_n<double>(cp.nblk);
+  double* twoW = a.hi_n<double>(G);
+  LVG_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * std::max(Ctot, 1), s));
+  LVG_CUDA(cudaMemsetAsync(Ain, 0, sizeof(double) * std::max(Ctot, 1), s));
+  if (E > 0) {
+    batch_nm_accum_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, gid0, local0, cp.vbase, Kc, Ain);
+    LVG_LAUNCH();
+  }
+  if (cp.nblk > 0) {
+    batch_group_kernel<<<(unsigned)cp.nblk, kRedThreads, 0, s>>>(Kc, cp.blk_g, cp.blk_c0, cp.vbase, partials);
+    LVG_LAUNCH();
+  }
+  batch_finish_kernel<<<G, kRedThreads, 0, s>>>(partials, cp.gblk0, twoW);
+  LVG_LAUNCH();
+  if (Ctot > 0) {
+    batch_nm_term_kernel<<<sm_grid(Ctot, kThreads), kThreads, 0, s>>>(Kc, Ain, cg, Ctot, twoW, t);
+    LVG_LAUNCH();
+    batch_group_kernel<<<(unsigned)cp.nblk, kRedThreads, 0, s>>>(t, cp.blk_g, cp.blk_c0, cp.vbase, partials);
+    LVG_LAUNCH();
+  }
+  batch_finish_kernel<<<G, kRedThreads, 0, s>>>(partials, cp.gblk0, q);
   LVG_LAUNCH();
 }
 

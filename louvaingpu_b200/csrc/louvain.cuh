@@ -47,6 +47,8 @@ struct LevelGraph {
   uint8_t* has_loop = nullptr;
   double m = 0.0;                 // sum of input weights (NeighbourCompute.cu:46)
   bool sorted_symmetric = false;  // CSR built without sorting (list sorted and symmetric)
+  const double* gm = nullptr;     // batched runs: m of each graph (device)
+  const int32_t* vgid = nullptr;  // batched runs: graph of each vertex (device)
   int32_t* blist = nullptr;       // vertices grouped by degree class, in index order inside a class
   int64_t nbucket[kNumBuckets] = {};
   int64_t bstart[kNumBuckets] = {};
@@ -56,6 +58,7 @@ struct LevelGraph {
   int32_t* ell_col = nullptr;
   float* ell_w = nullptr;
   int64_t ell_base[kNumBuckets] = {};
+  struct VInfo* ell_info = nullptr;  // per item of the classes up to 32, from bstart[kB4]; filled by init_state
   // tiles of the small-degree bucket
   int32_t* tile_start = nullptr;  // [ntiles+1] first bucket index of each tile
   int64_t ntiles = 0;
@@ -92,6 +95,8 @@ struct CommState {
   PassCtl* ctl = nullptr;
   int64_t ngroups = 0;
   size_t hot_bytes = 0;           // tot | comm | size, contiguous from tot
+  const int32_t* gid = nullptr;   // batched runs: graph of each vertex
+  int32_t* gdone = nullptr;       // batched runs: per-graph stop flags
 };
 
 struct Tuning {
@@ -153,6 +158,66 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
 void modularity_fp64_scratch(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
                              const int32_t* part, double* Kc, double* Ain, double* t, double* partials,
                              double* twoW_q, cudaStream_t s);
+
+// ---------------------------------------------------------------- batched runs
+// Per-graph pass control of a batched run (device arrays of the level's graphs).
+struct BatchCtl {
+  double* q_prev;
+  double* cur;
+  double* lower;
+  double* q_ret;
+  int32_t* pass;
+  int32_t* stop_now;
+  int32_t* done;
+  int32_t* status;
+  int32_t* passes;
+  int32_t* ndone;
+  double pass_min;
+  int32_t max_passes;
+};
+
+// Commit blocks of a batched level: block b sums communities
+// blk_c0[b]..+2048 of graph blk_g[b]; graph j owns blocks gblk0[j]..gblk0[j+1].
+struct BatchPlan {
+  const int32_t* vbase = nullptr;   // [G+1]
+  const int32_t* blk_g = nullptr;
+  const int32_t* blk_c0 = nullptr;
+  const int32_t* gblk0 = nullptr;   // [G+1]
+  int64_t nblk = 0;
+};
+
+void batch_globalize(const int32_t* lsrc, const int32_t* ldst, const float* w, int64_t E, const int64_t* eoff,
+                     const int32_t* voff, int32_t G, int32_t* gsrc, int32_t* gdst, uint32_t* bad, cudaStream_t s);
+void batch_vgid(const int32_t* vbase, int32_t G, int32_t V, int32_t* vgid, cudaStream_t s);
+void batch_m(const int32_t* src, const float* w, int64_t E, const int32_t* vgid, double* gm, int32_t G,
+             cudaStream_t s);
+void batch_init(const LevelGraph& g, CommState& st, cudaStream_t s);
+// mode: 0 init (Q only), 1 pass (per-graph ΔQ test + commit), 2 force commit
+void batch_commit(int mode, const BatchPlan& bp, const double* gm, CommState& st, const BatchCtl& C,
+                  cudaStream_t s);
+// mode: 0 end of pass, 1 Q of the state into q_prev, 2 into q_ret
+void batch_ctl(int mode, const BatchPlan& bp, const CommState& st, const BatchCtl& C, int32_t G, cudaStream_t s);
+void launch_merge_deltas(const LevelGraph& g, CommState& st, cudaStream_t s);
+// renumber() that also leaves the head-flag scan in pos[0..V] (pos[v] = new
+// ids of the communities whose smallest member is below v).
+int32_t renumber_pos(const LevelGraph& g, const int32_t* comm, int32_t* part, uint32_t* pos, Arena& a,
+                     cudaStream_t s);
+// Coarsen the graphs still running: part[v] + shift[graph] (INT_MIN: dropped).
+int64_t batch_induce(const LevelGraph& g, const int32_t* part, const int32_t* vgid, const int32_t* shift,
+                     int32_t C_next, int64_t E_keep, int32_t** out_src, int32_t** out_dst, float** out_w, Arena& a,
+                     cudaStream_t s);
+// out[j] = pos[idx[j]]
+void gather_u32(const uint32_t* pos, const int32_t* idx, int32_t n, int32_t* out, cudaStream_t s);
+// entries of the list per graph
+void batch_count(const int32_t* src, int64_t E, const int32_t* vgid, int64_t* cnt, int32_t G, cudaStream_t s);
+void batch_compose(int32_t* local0, const int32_t* gid0, int64_t n, const int32_t* lidx, const int32_t* vbase,
+                   const int32_t* cbase, const int32_t* part, cudaStream_t s);
+// FP64 Newman modularity of every graph: community ids coff[g] + local0[v]
+// with coff = cp.vbase, cp the 2048-groups of each graph's communities,
+// cg[c] = graph of community c; q[g] on the device, summed on the fixed tree.
+void batch_modularity(const int32_t* src, const int32_t* dst, const float* w, int64_t E, const int32_t* gid0,
+                      const int32_t* local0, const BatchPlan& cp, const int32_t* cg, int32_t Ctot, int32_t G,
+                      double* q, Arena& a, cudaStream_t s);
 
 // part_out[i] = part_level[composed[i]] for i < n.
 void compose(int32_t* composed, const int32_t* part_level, int64_t n, cudaStream_t s);

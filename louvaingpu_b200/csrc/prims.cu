@@ -2,7 +2,7 @@
 //
 // Radix sort (replaces thrust::sort_by_key on zip keys, NeighbourCompute.cu:82,
 // InducedGraphKernel.cu:91): 8-bit digits, reduce-then-scan.  Per digit pass a
-// histogram kernel counts digits per 4096-key tile, an exclusive scan over the
+// histogram kernel counts digits per 2048-key tile, an exclusive scan over the
 // digit-major [256][tiles] table yields every tile's global digit offsets, and
 // a scatter kernel ranks the tile's keys stably in shared memory (warp
 // __match_any_sync multisplit) and writes them to their global positions.
@@ -101,8 +101,8 @@ void finish_impl(const double* p, int64_t n, double* d_out, Arena& a, cudaStream
 
 // ---------------------------------------------------------------------------
 constexpr int kRsThreads = 256;
-constexpr int kRsItems = 16;
-constexpr int kRsTile = kRsThreads * kRsItems;  // 4096 keys
+constexpr int kRsItems = 8;
+constexpr int kRsTile = kRsThreads * kRsItems;  // 2048 keys
 constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kRadix = 256;
 

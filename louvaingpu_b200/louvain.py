@@ -42,6 +42,39 @@ class RunResult:
     status: int
 
 
+@dataclass
+class BatchResult:
+    """Per-graph results of a batched run (graph g owns vertices
+    vertex_off[g]..vertex_off[g+1] of `partition`, ids local to the graph)."""
+    partition: np.ndarray
+    vertex_off: np.ndarray
+    q_final: np.ndarray
+    n_levels: np.ndarray
+    n_comms: np.ndarray
+    status: np.ndarray
+
+    def __len__(self):
+        return len(self.q_final)
+
+    def part(self, g):
+        return self.partition[self.vertex_off[g]:self.vertex_off[g + 1]]
+
+
+def pack_graphs(graphs):
+    """[(n, src, dst, w), ...] -> concatenated src, dst, w (local ids) and the
+    entry and vertex offsets lvg_batch_run takes."""
+    n = np.array([int(g[0]) for g in graphs], np.int64)
+    cnt = np.array([len(g[1]) for g in graphs], np.int64)
+    voff = np.zeros(len(graphs) + 1, np.int64)
+    eoff = np.zeros(len(graphs) + 1, np.int64)
+    np.cumsum(n, out=voff[1:])
+    np.cumsum(cnt, out=eoff[1:])
+    if voff[-1] >= 2 ** 31:
+        raise ValueError("a batch holds at most 2^31-1 vertices")
+    cat = (lambda k, t: np.concatenate([np.asarray(g[k], t) for g in graphs]) if graphs else np.zeros(0, t))
+    return cat(1, np.int32), cat(2, np.int32), cat(3, np.float32), eoff, voff.astype(np.int32)
+
+
 class Louvain:
     def __init__(self, device=0, pass_min_gain=1e-7, level_min_gain=1e-7, max_passes=-1, max_levels=-1,
                  arena_bytes=0, tile_max_degree=0, block_max_degree=0, passes_per_sync=0, use_graphs=True, l2_persist=True):
@@ -135,6 +168,26 @@ class Louvain:
         r = _lib.LvgResult()
         self._check(self._L.lvg_run(self._h, ctypes.byref(r)))
         return RunResult(r.n_levels, r.n_comms, r.q_final, r.pass_entries, r.status)
+
+    def run_batch(self, graphs=None, packed=None):
+        """Whole dendrograms of many independent graphs in shared launches
+        (lvg_batch_run).  `graphs`: [(n, src, dst, w), ...] with ids local to
+        each graph, or `packed` = (src, dst, w, entry_off, vertex_off) as
+        pack_graphs returns it.  Each graph's result equals its own run()."""
+        src, dst, w, eoff, voff = packed if packed is not None else pack_graphs(graphs)
+        src = np.ascontiguousarray(src, np.int32)
+        dst = np.ascontiguousarray(dst, np.int32)
+        w = np.ascontiguousarray(w, np.float32)
+        eoff = np.ascontiguousarray(eoff, np.int64)
+        voff = np.ascontiguousarray(voff, np.int32)
+        G = len(voff) - 1
+        part = np.zeros(int(voff[-1]), np.int32)
+        q = np.zeros(G, np.float64)
+        levels, comms, status = (np.zeros(G, np.int32) for _ in range(3))
+        self._check(self._L.lvg_batch_run(self._h, _p(src), _p(dst), _p(w), _p(eoff), _p(voff), G, _p(part),
+                                          _p(q), _p(levels), _p(comms), _p(status)))
+        self.n_vertices = 0
+        return BatchResult(part, voff, q, levels, comms, status)
 
     # ------------------------------------------------------------------ results
     @property
