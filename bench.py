@@ -1,7 +1,7 @@
 """Benchmark of the Louvain hot path: edges/s per Louvain pass.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload lfr|sbm10k|rmat<scale>]
-                    [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload lfr|sbm10k|rmat<scale>|batched]
+                    [--impl ours|reference] [--graphs G]
 
 Workload (default): the LFR-style graph n = 2^20 (power-law degrees, exponent
 2.5 on [5, 5000]; community sizes exponent 1.5 on [50, 50000]; mu = 0.3; unit
@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--workload", default="lfr")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--graphs", type=int, default=8192, help="batched workload: number of graphs")
+    ap.add_argument("--batch-entries", type=float, default=2.5e8,
+                    help="batched workload: expected entries per packed sub-batch")
     return ap.parse_args()
 
 
@@ -302,12 +305,153 @@ def run_ours(args, world, rank, local, pg):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- batched form
+def batched_plan(count, seed, max_entries):
+    """The batched workload's graphs (SBM parameters) and their split into
+    packed sub-batches of at most about max_entries expected entries."""
+    from louvaingpu_b200 import graphgen
+    params = graphgen.batched_sbm_params(count, seed=seed)
+    groups, cur, acc = [], [], 0.0
+    for p in params:
+        n, B = p["n"], p["blocks"]
+        k = np.arange(B + 1, dtype=np.int64)
+        sizes = np.diff(n * k // B).astype(np.float64)
+        pin = float((sizes * (sizes - 1) / 2).sum())
+        e = 2.0 * (pin * min(p["p_in"], 1.0) + (n * (n - 1) / 2 - pin) * min(p["p_out"], 1.0))
+        if cur and acc + e > max_entries:
+            groups.append(cur)
+            cur, acc = [], 0.0
+        cur.append(p)
+        acc += e
+    if cur:
+        groups.append(cur)
+    return params, groups
+
+
+def run_batched(args, world, rank, local, pg):
+    """graphs/s of the batched form (lvg_batch_run_device over packed
+    sub-batches) against the plain per-graph loop on the same GPU."""
+    import torch
+    from louvaingpu_b200 import Louvain, graphgen, kernel_launches
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    params, groups = batched_plan(args.graphs, 3 + rank, args.batch_entries)
+    dgs = [graphgen.sbm_batch_device(g, device=local) for g in groups]
+    torch.cuda.synchronize()
+    G = sum(d.n_graphs for d in dgs)
+    E = sum(d.n_entries for d in dgs)
+    V = sum(d.n_vertices for d in dgs)
+    lv = Louvain(device=local)
+    lv.set_stream(stream.cuda_stream)
+
+    def batched_step():
+        return [lv.run_batch_device(d.src, d.dst, d.w, d.entry_off, d.vertex_off) for d in dgs]
+
+    clocks = Clocks(local)
+    clocks.start()
+    for _ in range(args.warmup):
+        batched_step()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    l0 = kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        res = batched_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = kernel_launches() - l0
+    t_ms = e0.elapsed_time(e1)
+    # plain loop: one context, one graph at a time, same device-resident lists
+    pl = Louvain(device=local)
+    pl.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    mism, dq_max = 0, 0.0
+    plain_q = []
+    for d, r in zip(dgs, res):
+        for g in range(d.n_graphs):
+            sp, dp, wp, e, n = d.graph_ptrs(g)
+            pl.load_edges_device(sp, dp, wp, e, n)
+            rr = pl.run()
+            part = pl.partition()
+            plain_q.append(rr.q_final)
+            if not np.array_equal(part, r.part(g)):
+                mism += 1
+            dq_max = max(dq_max, abs(rr.q_final - r.q_final[g]))
+    p1.record(stream)
+    torch.cuda.synchronize()
+    t_plain = p0.elapsed_time(p1)
+    clk = clocks.stop()
+    del pl
+    if pg:
+        tt = torch.tensor([t_ms, t_plain], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_ms, t_plain = float(tt[0].item()), float(tt[1].item())
+    value = G * args.steps * world / (t_ms / 1e3)
+    plain = G * world / (t_plain / 1e3)
+    # e2e: the host-buffer entry point on the first sub-batch, from pinned memory
+    d0 = dgs[0]
+    hs, hd, hw = (torch.from_numpy(x).pin_memory() for x in d0.to_host())
+    packed = (hs.numpy(), hd.numpy(), hw.numpy(), d0.entry_off, d0.vertex_off)
+    lv.run_batch(packed=packed)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        lv.run_batch(packed=packed)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = f0.elapsed_time(f1)
+    e2e = d0.n_graphs * args.steps * world / (t_e2e / 1e3)
+    del lv
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        small = [p for p in params if p["n"] <= 5000][:256]
+        t0 = time.perf_counter()
+        for p in small:
+            n, s_, d_, w_ = graphgen.sbm(p["n"], p["blocks"], p["p_in"], p["p_out"], 1, 4, seed=p["seed"] % (2 ** 62))
+            O.Run(n, s_, d_, w_, n_threads=1)
+        cpu_t = time.perf_counter() - t0
+        cpu = {"value": len(small) / cpu_t, "unit": "graphs/s", "cores": 1, "kind": "port",
+               "sample": f"{len(small)} graphs of the batched distribution with n <= 5000 (host SBM generator, "
+                         f"generation included), one thread"}
+    line = {
+        "metric": "graphs/s batched vs plain at dQ<=1e-3", "value": value, "unit": "graphs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+        "config": {"workload": "batched SBMs", "graphs": G, "entries": E, "vertices": V,
+                   "n_range": [64, 200000], "blocks": [4, 400], "avg_degree": [8, 32], "intra_fraction": 0.7,
+                   "weights": "integer 1..4", "sub_batches": len(dgs), "seed": 3,
+                   "inputs": "device-resident packed lists (device generator)",
+                   "l2": "inputs larger than L2"},
+        "plain": {"value": plain, "unit": "graphs/s", "ms_per_sweep": t_plain,
+                  "speedup_batched_over_plain": value / plain,
+                  "partitions_differing": mism, "max_abs_dq": dq_max},
+        "roofline": None,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": "graphs/s", "graphs": d0.n_graphs, "sample": "first sub-batch",
+                "h2d_bytes_per_step": 12 * d0.n_entries + 12 * (d0.n_graphs + 1),
+                "d2h_bytes_per_step": 4 * d0.n_vertices + 20 * d0.n_graphs},
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
     try:
         if args.impl == "reference":
             run_reference(args, world, rank, pg)
+        elif args.workload == "batched":
+            run_batched(args, world, rank, local, pg)
         else:
             run_ours(args, world, rank, local, pg)
     finally:

@@ -189,6 +189,14 @@ lvg_status lvg_batch_run(lvg_ctx* ctx, const int32_t* src, const int32_t* dst, c
                          int32_t* part_out, double* q_out, int32_t* levels_out, int32_t* comms_out,
                          int32_t* status_out);
 
+/* lvg_batch_run with the packed list already in device memory (d_src, d_dst,
+ * d_w: device pointers, read during the call; d_w is used in place).  The
+ * offsets and the outputs stay on the host. */
+lvg_status lvg_batch_run_device(lvg_ctx* ctx, const int32_t* d_src, const int32_t* d_dst, const float* d_w,
+                                const int64_t* entry_off, const int32_t* vertex_off, int32_t n_graphs,
+                                int32_t* part_out, double* q_out, int32_t* levels_out, int32_t* comms_out,
+                                int32_t* status_out);
+
 /* Largest community count lvg_modularity_fp64_noalloc accepts. */
 #define LVG_NOALLOC_MAX_COMMS (1 << 18)
 

@@ -97,7 +97,20 @@ SIGNATURES = {
     "lvg_kernel_launches": (i32, [ctypes.POINTER(i64)]),
     "lvg_memory": (i32, [P, ctypes.POINTER(i64), ctypes.POINTER(i64)]),
     "lvg_batch_run": (i32, [P, P, P, P, P, P, i32, P, P, P, P, P]),
+    "lvg_batch_run_device": (i32, [P, P, P, P, P, P, i32, P, P, P, P, P]),
     "lvg_modularity_fp64_noalloc": (i32, [P, P, P, i64, P, i32, P, ctypes.POINTER(dbl)]),
+}
+
+# Device generators declared in include/lvg_gen.h (same library).
+GEN_SIGNATURES = {
+    "lvg_gen_rmat": (i32, [i32, P, i32, i32, dbl, dbl, dbl, i32, i32, ctypes.c_uint64, ctypes.POINTER(P)]),
+    "lvg_gen_sbm_batch": (i32, [i32, P, i32, P, P, P, P, i32, i32, P, ctypes.POINTER(P)]),
+    "lvg_dgraph_info": (i32, [P, ctypes.POINTER(i32), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
+    "lvg_dgraph_arrays": (i32, [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P)]),
+    "lvg_dgraph_offsets": (i32, [P, P, P]),
+    "lvg_dgraph_copy_to_host": (i32, [P, P, P, P]),
+    "lvg_dgraph_free": (None, [P]),
+    "lvg_gen_last_error": (ctypes.c_char_p, []),
 }
 
 _lib = None
@@ -110,7 +123,7 @@ def load():
         if not os.path.exists(LIB_PATH):
             raise ImportError(f"{LIB_PATH} is missing: build it with `python -m louvaingpu_b200.build`")
         L = ctypes.CDLL(LIB_PATH)
-        for name, (res, args) in SIGNATURES.items():
+        for name, (res, args) in list(SIGNATURES.items()) + list(GEN_SIGNATURES.items()):
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args

@@ -787,9 +787,9 @@ struct BatchLevel {
   std::vector<int32_t> vbase;   // [G+1] vertex ranges of the level graphs
 };
 
-void batch_run(lvg_ctx* c, const int32_t* lsrc, const int32_t* ldst, const float* w, const int64_t* eoff,
-               const int32_t* voff, int32_t G0, int32_t* part_out, double* q_out, int32_t* levels_out,
-               int32_t* comms_out, int32_t* status_out) {
+void batch_run(lvg_ctx* c, bool dev_input, const int32_t* lsrc, const int32_t* ldst, const float* w,
+               const int64_t* eoff, const int32_t* voff, int32_t G0, int32_t* part_out, double* q_out,
+               int32_t* levels_out, int32_t* comms_out, int32_t* status_out) {
   cudaStream_t s = c->stream;
   const int64_t E0 = eoff[G0];
   const int32_t V0 = voff[G0];
@@ -802,25 +802,35 @@ void batch_run(lvg_ctx* c, const int32_t* lsrc, const int32_t* ldst, const float
   drop_graphs(c);
   c->loaded = false;
   c->have_state = false;
-  size_t need = c->cfg.arena_bytes > 0 ? (size_t)c->cfg.arena_bytes : arena_estimate(V0, E0, true) + 256 * (size_t)G0 + 8 * (size_t)V0;
+  size_t need = c->cfg.arena_bytes > 0 ? (size_t)c->cfg.arena_bytes
+                                       : arena_estimate(V0, E0, true) + 256 * (size_t)G0 + 8 * (size_t)V0;
+  if (dev_input && c->cfg.arena_bytes <= 0) need -= 4 * (size_t)E0;   // the weights are used in place
   c->arena.reserve(need);
   Arena& a = c->arena;
   // level-0 union list with global vertex ids
   int32_t* src0 = a.lo_n<int32_t>(E0);
   int32_t* dst0 = a.lo_n<int32_t>(E0);
-  float* w0 = a.lo_n<float>(E0);
+  float* w0 = dev_input ? const_cast<float*>(w) : a.lo_n<float>(E0);
   int32_t* gid0 = a.lo_n<int32_t>(V0);
   int32_t* local0 = a.lo_n<int32_t>(V0);
   {
     HiScope hs(a);
-    int32_t* ls = a.hi_n<int32_t>(E0);
-    int32_t* ld = a.hi_n<int32_t>(E0);
+    const int32_t* ls = lsrc;
+    const int32_t* ld = ldst;
+    if (!dev_input) {
+      int32_t* hs_ = a.hi_n<int32_t>(E0);
+      int32_t* hd_ = a.hi_n<int32_t>(E0);
+      if (E0 > 0) {
+        LVG_CUDA(cudaMemcpyAsync(hs_, lsrc, sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
+        LVG_CUDA(cudaMemcpyAsync(hd_, ldst, sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
+        LVG_CUDA(cudaMemcpyAsync(w0, w, sizeof(float) * E0, cudaMemcpyHostToDevice, s));
+      }
+      ls = hs_;
+      ld = hd_;
+    }
     int64_t* deoff = a.hi_n<int64_t>(G0 + 1);
     int32_t* dvoff = a.hi_n<int32_t>(G0 + 1);
     uint32_t* bad = a.hi_n<uint32_t>(1);
-    LVG_CUDA(cudaMemcpyAsync(ls, lsrc, sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
-    LVG_CUDA(cudaMemcpyAsync(ld, ldst, sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
-    LVG_CUDA(cudaMemcpyAsync(w0, w, sizeof(float) * E0, cudaMemcpyHostToDevice, s));
     LVG_CUDA(cudaMemcpyAsync(deoff, eoff, sizeof(int64_t) * (G0 + 1), cudaMemcpyHostToDevice, s));
     LVG_CUDA(cudaMemcpyAsync(dvoff, voff, sizeof(int32_t) * (G0 + 1), cudaMemcpyHostToDevice, s));
     LVG_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), s));
@@ -1096,6 +1106,21 @@ extern "C" lvg_status lvg_batch_run(lvg_ctx* c, const int32_t* src, const int32_
     require(n_graphs >= 1 && entry_off && vertex_off, LVG_ERR_INVALID_ARG, "need at least one graph and offsets");
     require(entry_off[0] == 0 && vertex_off[0] == 0, LVG_ERR_INVALID_ARG, "offsets must start at 0");
     require(entry_off[n_graphs] == 0 || (src && dst && w), LVG_ERR_INVALID_ARG, "null edge array");
-    batch_run(c, src, dst, w, entry_off, vertex_off, n_graphs, part_out, q_out, levels_out, comms_out, status_out);
+    batch_run(c, false, src, dst, w, entry_off, vertex_off, n_graphs, part_out, q_out, levels_out, comms_out,
+              status_out);
+  });
+}
+
+extern "C" lvg_status lvg_batch_run_device(lvg_ctx* c, const int32_t* d_src, const int32_t* d_dst,
+                                           const float* d_w, const int64_t* entry_off, const int32_t* vertex_off,
+                                           int32_t n_graphs, int32_t* part_out, double* q_out, int32_t* levels_out,
+                                           int32_t* comms_out, int32_t* status_out) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(n_graphs >= 1 && entry_off && vertex_off, LVG_ERR_INVALID_ARG, "need at least one graph and offsets");
+    require(entry_off[0] == 0 && vertex_off[0] == 0, LVG_ERR_INVALID_ARG, "offsets must start at 0");
+    require(entry_off[n_graphs] == 0 || (d_src && d_dst && d_w), LVG_ERR_INVALID_ARG, "null edge array");
+    batch_run(c, true, d_src, d_dst, d_w, entry_off, vertex_off, n_graphs, part_out, q_out, levels_out, comms_out,
+              status_out);
   });
 }

@@ -99,3 +99,82 @@ def batched_sbm_params(count, seed=3, n_lo=64, n_hi=200000):
         out.append(dict(n=n, blocks=blocks, p_in=p_in, p_out=p_out, w_lo=1, w_hi=4,
                         seed=int(rng.integers(0, 2**62))))
     return out
+
+
+# ---------------------------------------------------------------- device side
+class DeviceGraphs:
+    """Graph(s) generated into device memory by liblvg (include/lvg_gen.h).
+
+    src/dst/w are device pointers (ints) of the packed list; entry_off and
+    vertex_off are host arrays (n_graphs + 1).  Freed by close() or on
+    garbage collection."""
+
+    def __init__(self, handle):
+        from . import _lib
+        self._L = _lib.load()
+        self._h = handle
+        g, e, v = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+        self._L.lvg_dgraph_info(self._h, ctypes.byref(g), ctypes.byref(e), ctypes.byref(v))
+        self.n_graphs, self.n_entries, self.n_vertices = g.value, e.value, v.value
+        s, d, w = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        self._L.lvg_dgraph_arrays(self._h, ctypes.byref(s), ctypes.byref(d), ctypes.byref(w))
+        self.src, self.dst, self.w = s.value or 0, d.value or 0, w.value or 0
+        self.entry_off = np.zeros(self.n_graphs + 1, np.int64)
+        self.vertex_off = np.zeros(self.n_graphs + 1, np.int32)
+        self._L.lvg_dgraph_offsets(self._h, self.entry_off.ctypes.data_as(ctypes.c_void_p),
+                                   self.vertex_off.ctypes.data_as(ctypes.c_void_p))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.lvg_dgraph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def graph_ptrs(self, g):
+        """(src, dst, w, n_entries, n_vertices) of graph g: device pointers."""
+        e0, e1 = int(self.entry_off[g]), int(self.entry_off[g + 1])
+        return (self.src + 4 * e0, self.dst + 4 * e0, self.w + 4 * e0, e1 - e0,
+                int(self.vertex_off[g + 1] - self.vertex_off[g]))
+
+    def to_host(self):
+        """Copy the packed list back: (src, dst, w) numpy arrays."""
+        src, dst = np.zeros(self.n_entries, np.int32), np.zeros(self.n_entries, np.int32)
+        w = np.zeros(self.n_entries, np.float32)
+        vp = lambda x: x.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        _gen_check(self._L.lvg_dgraph_copy_to_host(self._h, vp(src), vp(dst), vp(w)))
+        return src, dst, w
+
+
+def _gen_check(status):
+    from . import _lib
+    if status != 0:
+        raise _lib.LvgError(status, _lib.load().lvg_gen_last_error().decode())
+
+
+def rmat_device(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, w_lo=1, w_hi=16, seed=2, device=0, stream=None):
+    """R-MAT generated on the device; equals rmat() with the same arguments."""
+    from . import _lib
+    h = ctypes.c_void_p()
+    _gen_check(_lib.load().lvg_gen_rmat(int(device), ctypes.c_void_p(stream or 0), int(scale), int(edge_factor),
+                                        float(a), float(b), float(c), int(w_lo), int(w_hi), int(seed),
+                                        ctypes.byref(h)))
+    return DeviceGraphs(h)
+
+
+def sbm_batch_device(params, w_lo=1, w_hi=4, device=0, stream=None):
+    """Packed batch of SBMs on the device; params as batched_sbm_params gives
+    them (dicts with n, blocks, p_in, p_out, seed)."""
+    from . import _lib
+    G = len(params)
+    n = np.array([p["n"] for p in params], np.int32)
+    bl = np.array([p["blocks"] for p in params], np.int32)
+    pi = np.array([p["p_in"] for p in params], np.float64)
+    po = np.array([p["p_out"] for p in params], np.float64)
+    sd = np.array([p["seed"] for p in params], np.uint64)
+    h = ctypes.c_void_p()
+    vp = lambda x: x.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    _gen_check(_lib.load().lvg_gen_sbm_batch(int(device), ctypes.c_void_p(stream or 0), G, vp(n), vp(bl), vp(pi),
+                                             vp(po), int(w_lo), int(w_hi), vp(sd), ctypes.byref(h)))
+    return DeviceGraphs(h)

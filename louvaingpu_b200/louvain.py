@@ -189,6 +189,21 @@ class Louvain:
         self.n_vertices = 0
         return BatchResult(part, voff, q, levels, comms, status)
 
+    def run_batch_device(self, src_ptr, dst_ptr, w_ptr, entry_off, vertex_off):
+        """run_batch over a packed list already in device memory (device
+        pointers; e.g. graphgen.DeviceGraphs.src/dst/w and its offsets)."""
+        eoff = np.ascontiguousarray(entry_off, np.int64)
+        voff = np.ascontiguousarray(vertex_off, np.int32)
+        G = len(voff) - 1
+        part = np.zeros(int(voff[-1]), np.int32)
+        q = np.zeros(G, np.float64)
+        levels, comms, status = (np.zeros(G, np.int32) for _ in range(3))
+        self._check(self._L.lvg_batch_run_device(self._h, ctypes.c_void_p(src_ptr), ctypes.c_void_p(dst_ptr),
+                                                 ctypes.c_void_p(w_ptr), _p(eoff), _p(voff), G, _p(part), _p(q),
+                                                 _p(levels), _p(comms), _p(status)))
+        self.n_vertices = 0
+        return BatchResult(part, voff, q, levels, comms, status)
+
     # ------------------------------------------------------------------ results
     @property
     def n_levels(self):

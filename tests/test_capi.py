@@ -31,13 +31,23 @@ def test_header_declares_entry_points():
 
 
 def test_library_exports_every_declared_symbol(lib):
-    for name in declared("lvg.h"):
-        assert hasattr(lib, name), name
+    for header in ("lvg.h", "lvg_gen.h"):
+        for name in declared(header):
+            assert hasattr(lib, name), name
 
 
 def test_python_binding_covers_every_symbol():
     from louvaingpu_b200 import _lib
     assert sorted(_lib.SIGNATURES) == declared("lvg.h")
+    assert sorted(_lib.GEN_SIGNATURES) == declared("lvg_gen.h")
+
+
+def test_generator_argument_errors_without_device(lib):
+    out = ctypes.c_void_p()
+    assert lib.lvg_gen_rmat(0, None, 0, 16, 0.57, 0.19, 0.19, 1, 16, 1, ctypes.byref(out)) == 1
+    assert lib.lvg_gen_rmat(0, None, 10, 16, 0.57, 0.19, 0.19, 1, 16, 1, None) == 1
+    assert lib.lvg_gen_sbm_batch(0, None, 0, None, None, None, None, 1, 4, None, ctypes.byref(out)) == 1
+    assert lib.lvg_dgraph_info(None, None, None, None) == 1
 
 
 def test_status_strings_and_config_defaults(lib):
