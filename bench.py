@@ -1,6 +1,6 @@
 """Benchmark of the Louvain hot path: edges/s per Louvain pass.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload lfr|sbm10k|rmat<scale>|batched]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload lfr|sbm10k|rmat<scale>|batched|serving]
                     [--impl ours|reference] [--graphs G]
 
 Workload (default): the LFR-style graph n = 2^20 (power-law degrees, exponent
@@ -31,6 +31,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "edges/s per Louvain pass"
+DEVICE_GEN_SCALE = 20     # R-MAT graphs this large are generated on the device
+CPU_SAMPLE_RMAT_SCALE = 20  # the CPU baseline of larger R-MAT graphs runs on this scale
 UNIT = "edges/s"
 
 
@@ -44,7 +46,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--graphs", type=int, default=8192, help="batched workload: number of graphs")
     ap.add_argument("--batch-entries", type=float, default=2.5e8,
-                    help="batched workload: expected entries per packed sub-batch")
+                    help="batched/serving workloads: entries per packed sub-batch")
+    ap.add_argument("--requests", type=int, default=5000, help="serving workload: requests")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serving workload: Poisson arrivals per second")
+    ap.add_argument("--pool", type=int, default=2048, help="serving workload: distinct small graphs")
+    ap.add_argument("--giants", type=int, default=4, help="serving workload: distinct R-MAT scale-22 graphs")
+    ap.add_argument("--slots", type=int, default=4, help="serving workload: server slots")
     return ap.parse_args()
 
 
@@ -62,9 +69,17 @@ def make_graph(workload):
         return n, s, d, w, desc, 1e-6
     if workload.startswith("rmat"):
         scale = int(workload[4:])
-        n, s, d, w = graphgen.rmat(scale)
+        if scale >= DEVICE_GEN_SCALE:
+            # generated on the device (equal to the host generator), copied back once
+            dg = graphgen.rmat_device(scale)
+            n = dg.n_vertices
+            s, d, w = dg.to_host()
+            dg.close()
+        else:
+            n, s, d, w = graphgen.rmat(scale)
         desc = dict(workload=f"R-MAT scale {scale}", n_vertices=n, edge_factor=16, abcd=[0.57, 0.19, 0.19, 0.05],
-                    weights="integer 1..16", seed=2)
+                    self_loops="dropped", duplicates="merged, weights summed", weights="integer 1..16", seed=2,
+                    label_noise="none")
         return n, s, d, w, desc, 1e-7
     raise SystemExit(f"unknown workload {workload}")
 
@@ -245,7 +260,8 @@ def run_ours(args, world, rank, local, pg):
             "peak_source": peak_kind, "traffic": profiled_traffic(args.workload),
             "kernel": "move kernels of one pass (all degree buckets)", "algorithmic_bytes": b_pass,
             "move_ms_per_pass": t_move * 1e3}
-    del lv
+    del lv, ds, dd, dw
+    torch.cuda.empty_cache()
     # ---------------------------------------------------------------- e2e
     hs = torch.from_numpy(s).pin_memory()
     hd = torch.from_numpy(d).pin_memory()
@@ -285,9 +301,16 @@ def run_ours(args, world, rank, local, pg):
     cpu = None
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, secs = cpu_baseline(n, s, d, w, level_min, threads)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"one whole dendrogram run of the workload ({secs:.1f} s)"}
+        if args.workload.startswith("rmat") and int(args.workload[4:]) > CPU_SAMPLE_RMAT_SCALE:
+            from louvaingpu_b200 import graphgen
+            del s, d, w, hs, hd, hw
+            cn, cs, cd, cw = graphgen.rmat(CPU_SAMPLE_RMAT_SCALE)
+            v, secs = cpu_baseline(cn, cs, cd, cw, level_min, threads)
+            sample = f"one whole dendrogram run of R-MAT scale {CPU_SAMPLE_RMAT_SCALE} (same generator; {secs:.1f} s)"
+        else:
+            v, secs = cpu_baseline(n, s, d, w, level_min, threads)
+            sample = f"one whole dendrogram run of the workload ({secs:.1f} s)"
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -444,6 +467,118 @@ def run_batched(args, world, rank, local, pg):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- serving form
+def run_serving(args, world, rank, local, pg):
+    """Poisson request stream served by the continuous-batching server
+    (louvaingpu_b200.serving) against the plain per-request path on the same
+    GPU, same arrival times: graphs/s and p50/p99/p99.9 latency."""
+    import hashlib
+    import torch
+    from louvaingpu_b200 import Louvain, graphgen, kernel_launches
+    from louvaingpu_b200.serving import Server
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(17 + rank)
+    # request pool: SBMs of the batched distribution and R-MAT scale-22 giants
+    params, groups = batched_plan(args.pool, 5 + rank, args.batch_entries)
+    pool = [graphgen.sbm_batch_device(g, device=local) for g in groups]
+    small = [(d, g) for d in pool for g in range(d.n_graphs)]
+    giants = [graphgen.rmat_device(22, edge_factor=16, seed=100 + k, device=local) for k in range(args.giants)]
+    torch.cuda.synchronize()
+    R = args.requests
+    is_giant = rng.random(R) < 0.02
+    pick = rng.integers(0, 1 << 30, R)
+    reqs = []
+    for i in range(R):
+        if is_giant[i] and giants:
+            x = giants[pick[i] % len(giants)]
+            reqs.append((x.src, x.dst, x.w, x.n_entries, x.n_vertices))
+        else:
+            d, g = small[pick[i] % len(small)]
+            reqs.append(d.graph_ptrs(g))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, R))
+    free = torch.cuda.mem_get_info()[0]
+    budget = int(min(150e9, free - 6e9))
+    digest = lambda a: hashlib.blake2b(a.tobytes(), digest_size=8).hexdigest()  # noqa: E731
+
+    clocks = Clocks(local)
+    clocks.start()
+    # served: submit at the arrival times, results collected at the end
+    with Server(n_slots=args.slots, hbm_budget=budget, max_batch_entries=int(args.batch_entries)) as srv:
+        warm = [reqs[k] for k in range(min(64, R))]
+        for s_, d_, w_, e_, n_ in warm:                       # warm-up requests (not timed)
+            srv.submit(s_, d_, w_, e_, n_)
+        srv.drain()
+        srv.poll(1 << 20)
+        l0 = kernel_launches()
+        base = time.perf_counter()
+        t_ref = None
+        for i in range(R):
+            wait = arrivals[i] - (time.perf_counter() - base)
+            if wait > 0:
+                time.sleep(wait)
+            s_, d_, w_, e_, n_ = reqs[i]
+            srv.submit(s_, d_, w_, e_, n_, part_out=np.empty(n_, np.int32), tag=i)
+        srv.drain()
+        wall = time.perf_counter() - base
+        launches = kernel_launches() - l0
+        out = srv.poll(R + 16)
+        stats = srv.stats()
+    out.sort(key=lambda r: r.tag)
+    first = min(r.t_submit for r in out)
+    served_lat = np.array([r.latency for r in out])
+    served_span = max(r.t_done for r in out) - first
+    served_digest = [digest(r.part) for r in out]
+    served_q = np.array([r.q_final for r in out])
+    bad_status = sum(1 for r in out if r.status != 0)
+    # plain: one context, one request at a time, same arrival times
+    pl = Louvain(device=local)
+    torch.cuda.synchronize()
+    plain_lat = np.zeros(R)
+    mism, dq_max = 0, 0.0
+    base = time.perf_counter()
+    for i in range(R):
+        wait = arrivals[i] - (time.perf_counter() - base)
+        if wait > 0:
+            time.sleep(wait)
+        s_, d_, w_, e_, n_ = reqs[i]
+        pl.load_edges_device(s_, d_, w_, e_, n_)
+        res = pl.run()
+        part = pl.partition()
+        plain_lat[i] = (time.perf_counter() - base) - arrivals[i]
+        if digest(part) != served_digest[i]:
+            mism += 1
+        dq_max = max(dq_max, abs(res.q_final - served_q[i]))
+    plain_span = time.perf_counter() - base
+    clk = clocks.stop()
+    del pl
+    if rank != 0:
+        return
+    pct = lambda a: {"p50_ms": float(np.percentile(a, 50) * 1e3), "p99_ms": float(np.percentile(a, 99) * 1e3),
+                     "p999_ms": float(np.percentile(a, 99.9) * 1e3)}  # noqa: E731
+    value = R * world / served_span
+    line = {
+        "metric": "graphs/s served (continuous batching) with p50/p99/p99.9 latency", "value": value,
+        "unit": "graphs/s", "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": served_span * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+        "config": {"workload": "Poisson request stream", "requests": R, "arrival_rate_per_s": args.rate,
+                   "giant_fraction": 0.02, "giants": "R-MAT scale 22, edge factor 16, weights 1..16",
+                   "giant_graphs_distinct": len(giants), "small": "SBMs of the batched distribution",
+                   "small_pool_graphs": len(small), "hbm_budget_bytes": budget, "slots": args.slots,
+                   "max_batch_entries": int(args.batch_entries), "l2": "inputs larger than L2"},
+        "served": dict(pct(served_lat), graphs_per_s=value, span_s=served_span, batches=stats["batches"],
+                       failed=bad_status, wall_s=wall),
+        "plain": dict(pct(plain_lat), graphs_per_s=R / plain_span, span_s=plain_span),
+        "speedup_served_over_plain": value / (R / plain_span),
+        "same_alone_and_in_mix": {"partitions_differing": mism, "max_abs_dq": dq_max},
+        "roofline": None, "cpu_baseline": None,
+        "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(sum(r[4] for r in reqs) * 4),
+                "note": "inputs device-resident (device generator); partitions returned to the host"},
+        "clocks": clk, "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
@@ -452,6 +587,8 @@ def main():
             run_reference(args, world, rank, pg)
         elif args.workload == "batched":
             run_batched(args, world, rank, local, pg)
+        elif args.workload == "serving":
+            run_serving(args, world, rank, local, pg)
         else:
             run_ours(args, world, rank, local, pg)
     finally:

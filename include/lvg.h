@@ -197,6 +197,68 @@ lvg_status lvg_batch_run_device(lvg_ctx* ctx, const int32_t* d_src, const int32_
                                 int32_t* part_out, double* q_out, int32_t* levels_out, int32_t* comms_out,
                                 int32_t* status_out);
 
+/* lvg_batch_run over graphs held in separate device buffers: graph g has
+ * n_entries[g] entries at d_src[g], d_dst[g], d_w[g] (device pointers, ids
+ * local to the graph) and n_vertices[g] vertices.  The pointer and size arrays
+ * are host arrays; outputs as in lvg_batch_run (part_out packed graph after
+ * graph). */
+lvg_status lvg_batch_run_graphs(lvg_ctx* ctx, int32_t n_graphs, const int32_t* const* d_src,
+                                const int32_t* const* d_dst, const float* const* d_w, const int64_t* n_entries,
+                                const int32_t* n_vertices, int32_t* part_out, double* q_out, int32_t* levels_out,
+                                int32_t* comms_out, int32_t* status_out);
+
+/* Reserve the context's device arena now (at least `bytes`), so that later
+ * calls that fit in it allocate nothing.  Only before a graph is loaded. */
+lvg_status lvg_reserve(lvg_ctx* ctx, int64_t bytes);
+
+/* Device bytes a batched run of n_graphs graphs with these totals reserves
+ * (the arena lvg_batch_run sizes itself to when lvg_config.arena_bytes is 0). */
+lvg_status lvg_batch_footprint(int64_t n_vertices, int64_t n_entries, int32_t n_graphs, int64_t* bytes);
+
+/* ------------------------------------------------------------- serving ----
+ * A request server over device-resident graphs (continuous batching).
+ * n_slots worker contexts, each on its own host thread and CUDA stream, split
+ * an HBM budget evenly (each slot's arena is reserved once).  A free slot
+ * takes the queued requests in arrival order as one batched run, as many as
+ * fit its arena (lvg_batch_footprint), at most max_batch_entries entries and
+ * max_batch_graphs graphs; slots run concurrently, so requests that arrive
+ * while others are on the GPU start as soon as a slot frees up.  Each
+ * request's result is exactly what lvg_run gives for its graph alone. */
+typedef struct lvg_server lvg_server;
+
+typedef struct {
+  int64_t id;           /* lvg_server_submit's id */
+  int64_t tag;          /* the caller's tag */
+  int32_t status;       /* LVG_OK, LVG_ERR_NOT_CONVERGED, or the batch's error */
+  int32_t n_levels;
+  int32_t n_comms;
+  int32_t batch_graphs; /* graphs in the batched run that served it */
+  double q_final;       /* FP64 Newman modularity of the final partition */
+  int64_t t_submit_ns;  /* steady-clock times since lvg_server_create */
+  int64_t t_start_ns;
+  int64_t t_done_ns;
+} lvg_serve_result;
+
+lvg_status lvg_server_create(const lvg_config* cfg, int32_t n_slots, int64_t hbm_budget_bytes,
+                             int64_t max_batch_entries, int32_t max_batch_graphs, lvg_server** out);
+/* Queue one graph.  d_src/d_dst/d_w: device arrays complete on the device
+ * before the call and kept alive until the result is polled; part_out: host
+ * array of n_vertices ints written before the result is posted (nullable). */
+lvg_status lvg_server_submit(lvg_server* srv, const int32_t* d_src, const int32_t* d_dst, const float* d_w,
+                             int64_t n_entries, int32_t n_vertices, int32_t* part_out, int64_t tag,
+                             int64_t* id_out);
+/* Move up to max finished results into out; *n_out = how many. */
+lvg_status lvg_server_poll(lvg_server* srv, lvg_serve_result* out, int32_t max, int32_t* n_out);
+/* Wait until every submitted request has finished (timeout_ms < 0: no limit);
+ * LVG_ERR_STATE on timeout. */
+lvg_status lvg_server_drain(lvg_server* srv, int64_t timeout_ms);
+/* Counters: submitted, completed, batched runs, device bytes reserved. */
+lvg_status lvg_server_stats(lvg_server* srv, int64_t* submitted, int64_t* completed, int64_t* batches,
+                            int64_t* reserved_bytes);
+const char* lvg_server_last_error(const lvg_server* srv);
+/* Stops the workers after the queue is empty and frees every slot. */
+lvg_status lvg_server_destroy(lvg_server* srv);
+
 /* Largest community count lvg_modularity_fp64_noalloc accepts. */
 #define LVG_NOALLOC_MAX_COMMS (1 << 18)
 

@@ -65,6 +65,21 @@ class LvgResult(ctypes.Structure):
     ]
 
 
+class LvgServeResult(ctypes.Structure):
+    _fields_ = [
+        ("id", ctypes.c_int64),
+        ("tag", ctypes.c_int64),
+        ("status", ctypes.c_int32),
+        ("n_levels", ctypes.c_int32),
+        ("n_comms", ctypes.c_int32),
+        ("batch_graphs", ctypes.c_int32),
+        ("q_final", ctypes.c_double),
+        ("t_submit_ns", ctypes.c_int64),
+        ("t_start_ns", ctypes.c_int64),
+        ("t_done_ns", ctypes.c_int64),
+    ]
+
+
 # Every entry point declared in include/lvg.h, with its ctypes signature.
 P = ctypes.c_void_p
 i32, i64, dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
@@ -98,6 +113,17 @@ SIGNATURES = {
     "lvg_memory": (i32, [P, ctypes.POINTER(i64), ctypes.POINTER(i64)]),
     "lvg_batch_run": (i32, [P, P, P, P, P, P, i32, P, P, P, P, P]),
     "lvg_batch_run_device": (i32, [P, P, P, P, P, P, i32, P, P, P, P, P]),
+    "lvg_batch_run_graphs": (i32, [P, i32, P, P, P, P, P, P, P, P, P, P]),
+    "lvg_batch_footprint": (i32, [i64, i64, i32, ctypes.POINTER(i64)]),
+    "lvg_reserve": (i32, [P, i64]),
+    "lvg_server_create": (i32, [ctypes.POINTER(LvgConfig), i32, i64, i64, i32, ctypes.POINTER(P)]),
+    "lvg_server_submit": (i32, [P, P, P, P, i64, i32, P, i64, ctypes.POINTER(i64)]),
+    "lvg_server_poll": (i32, [P, ctypes.POINTER(LvgServeResult), i32, ctypes.POINTER(i32)]),
+    "lvg_server_drain": (i32, [P, i64]),
+    "lvg_server_stats": (i32, [P, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64),
+                               ctypes.POINTER(i64)]),
+    "lvg_server_last_error": (ctypes.c_char_p, [P]),
+    "lvg_server_destroy": (i32, [P]),
     "lvg_modularity_fp64_noalloc": (i32, [P, P, P, i64, P, i32, P, ctypes.POINTER(dbl)]),
 }
 

@@ -787,16 +787,31 @@ struct BatchLevel {
   std::vector<int32_t> vbase;   // [G+1] vertex ranges of the level graphs
 };
 
-void batch_run(lvg_ctx* c, bool dev_input, const int32_t* lsrc, const int32_t* ldst, const float* w,
-               const int64_t* eoff, const int32_t* voff, int32_t G0, int32_t* part_out, double* q_out,
-               int32_t* levels_out, int32_t* comms_out, int32_t* status_out) {
+// Input of a batched run: graph g has vertex_off[g+1]-vertex_off[g] vertices
+// and entry_off[g+1]-entry_off[g] entries at src[g], dst[g], w[g] (device
+// pointers, or host pointers when `host` is set).
+struct BatchInput {
+  int32_t G = 0;
+  const int64_t* eoff = nullptr;
+  const int32_t* voff = nullptr;
+  std::vector<const int32_t*> src, dst;
+  std::vector<const float*> w;
+  bool host = false;
+};
+
+void batch_run(lvg_ctx* c, const BatchInput& in, int32_t* part_out, double* q_out, int32_t* levels_out,
+               int32_t* comms_out, int32_t* status_out) {
   cudaStream_t s = c->stream;
+  const int32_t G0 = in.G;
+  const int64_t* eoff = in.eoff;
+  const int32_t* voff = in.voff;
   const int64_t E0 = eoff[G0];
   const int32_t V0 = voff[G0];
   for (int32_t g = 0; g < G0; ++g) {
     require(eoff[g + 1] >= eoff[g] && voff[g + 1] >= voff[g], LVG_ERR_INVALID_ARG, "offsets must not decrease");
     require((int64_t)(voff[g + 1] - voff[g]) <= (int64_t)kGroup * kGroup, LVG_ERR_CAPACITY,
             "a batched graph may have at most 2048*2048 vertices");
+    require(eoff[g + 1] == eoff[g] || (in.src[g] && in.dst[g] && in.w[g]), LVG_ERR_INVALID_ARG, "null edge array");
   }
   require(E0 < ((int64_t)1 << 31), LVG_ERR_CAPACITY, "a batch may hold at most 2^31-1 entries");
   drop_graphs(c);
@@ -804,49 +819,64 @@ void batch_run(lvg_ctx* c, bool dev_input, const int32_t* lsrc, const int32_t* l
   c->have_state = false;
   size_t need = c->cfg.arena_bytes > 0 ? (size_t)c->cfg.arena_bytes
                                        : arena_estimate(V0, E0, true) + 256 * (size_t)G0 + 8 * (size_t)V0;
-  if (dev_input && c->cfg.arena_bytes <= 0) need -= 4 * (size_t)E0;   // the weights are used in place
   c->arena.reserve(need);
   Arena& a = c->arena;
   // level-0 union list with global vertex ids
   int32_t* src0 = a.lo_n<int32_t>(E0);
   int32_t* dst0 = a.lo_n<int32_t>(E0);
-  float* w0 = dev_input ? const_cast<float*>(w) : a.lo_n<float>(E0);
+  float* w0 = a.lo_n<float>(E0);
   int32_t* gid0 = a.lo_n<int32_t>(V0);
   int32_t* local0 = a.lo_n<int32_t>(V0);
   {
     HiScope hs(a);
-    const int32_t* ls = lsrc;
-    const int32_t* ld = ldst;
-    if (!dev_input) {
-      int32_t* hs_ = a.hi_n<int32_t>(E0);
-      int32_t* hd_ = a.hi_n<int32_t>(E0);
-      if (E0 > 0) {
-        LVG_CUDA(cudaMemcpyAsync(hs_, lsrc, sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
-        LVG_CUDA(cudaMemcpyAsync(hd_, ldst, sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
-        LVG_CUDA(cudaMemcpyAsync(w0, w, sizeof(float) * E0, cudaMemcpyHostToDevice, s));
+    std::vector<const void*> ptrs(3 * (size_t)G0);
+    if (in.host) {
+      // stage the host lists (graph by graph, in entry order) and point into the copy
+      int32_t* ss = a.hi_n<int32_t>(E0);
+      int32_t* sd = a.hi_n<int32_t>(E0);
+      float* sw = a.hi_n<float>(E0);
+      bool packed = G0 > 0 && in.src[0] && in.dst[0] && in.w[0];
+      for (int32_t g = 0; packed && g < G0; ++g)
+        packed = in.src[g] == in.src[0] + eoff[g] && in.dst[g] == in.dst[0] + eoff[g] && in.w[g] == in.w[0] + eoff[g];
+      if (packed && E0 > 0) {   // one copy per array
+        LVG_CUDA(cudaMemcpyAsync(ss, in.src[0], sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
+        LVG_CUDA(cudaMemcpyAsync(sd, in.dst[0], sizeof(int32_t) * E0, cudaMemcpyHostToDevice, s));
+        LVG_CUDA(cudaMemcpyAsync(sw, in.w[0], sizeof(float) * E0, cudaMemcpyHostToDevice, s));
       }
-      ls = hs_;
-      ld = hd_;
+      for (int32_t g = 0; g < G0; ++g) {
+        const int64_t e0 = eoff[g], n = eoff[g + 1] - eoff[g];
+        if (n > 0 && !packed) {
+          LVG_CUDA(cudaMemcpyAsync(ss + e0, in.src[g], sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+          LVG_CUDA(cudaMemcpyAsync(sd + e0, in.dst[g], sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+          LVG_CUDA(cudaMemcpyAsync(sw + e0, in.w[g], sizeof(float) * n, cudaMemcpyHostToDevice, s));
+        }
+        ptrs[g] = ss + e0;
+        ptrs[G0 + g] = sd + e0;
+        ptrs[2 * G0 + g] = sw + e0;
+      }
+    } else {
+      for (int32_t g = 0; g < G0; ++g) {
+        ptrs[g] = in.src[g];
+        ptrs[G0 + g] = in.dst[g];
+        ptrs[2 * G0 + g] = in.w[g];
+      }
     }
+    const void** dptrs = a.hi_n<const void*>(3 * (int64_t)G0);
     int64_t* deoff = a.hi_n<int64_t>(G0 + 1);
     int32_t* dvoff = a.hi_n<int32_t>(G0 + 1);
     uint32_t* bad = a.hi_n<uint32_t>(1);
+    LVG_CUDA(cudaMemcpyAsync(dptrs, ptrs.data(), sizeof(void*) * ptrs.size(), cudaMemcpyHostToDevice, s));
     LVG_CUDA(cudaMemcpyAsync(deoff, eoff, sizeof(int64_t) * (G0 + 1), cudaMemcpyHostToDevice, s));
     LVG_CUDA(cudaMemcpyAsync(dvoff, voff, sizeof(int32_t) * (G0 + 1), cudaMemcpyHostToDevice, s));
     LVG_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), s));
-    batch_globalize(ls, ld, w0, E0, deoff, dvoff, G0, src0, dst0, bad, s);
+    batch_globalize((const int32_t* const*)dptrs, (const int32_t* const*)(dptrs + G0),
+                    (const float* const*)(dptrs + 2 * G0), E0, deoff, dvoff, G0, src0, dst0, w0, bad, s);
     batch_vgid(dvoff, G0, V0, gid0, s);
+    batch_local_ids(gid0, dvoff, V0, local0, s);
     uint32_t h = 0;
     LVG_CUDA(cudaMemcpyAsync(&h, bad, sizeof h, cudaMemcpyDeviceToHost, s));
     sync(c);
     require(h == 0, LVG_ERR_INVALID_ARG, "edge list has a vertex id out of its graph or a negative / non-finite weight");
-  }
-  {
-    std::vector<int32_t> l0(V0);
-    for (int32_t g = 0; g < G0; ++g)
-      for (int32_t v = voff[g]; v < voff[g + 1]; ++v) l0[v] = v - voff[g];
-    LVG_CUDA(cudaMemcpyAsync(local0, l0.data(), sizeof(int32_t) * V0, cudaMemcpyHostToDevice, s));
-    sync(c);
   }
   const size_t base_lo = a.lo;
   std::vector<double> mod(G0, 0.0);
@@ -1097,18 +1127,84 @@ void batch_run(lvg_ctx* c, bool dev_input, const int32_t* lsrc, const int32_t* l
 
 }  // namespace
 
+namespace {
+BatchInput packed_input(const int32_t* src, const int32_t* dst, const float* w, const int64_t* entry_off,
+                        const int32_t* vertex_off, int32_t n_graphs, bool host) {
+  require(n_graphs >= 1 && entry_off && vertex_off, LVG_ERR_INVALID_ARG, "need at least one graph and offsets");
+  require(entry_off[0] == 0 && vertex_off[0] == 0, LVG_ERR_INVALID_ARG, "offsets must start at 0");
+  require(entry_off[n_graphs] == 0 || (src && dst && w), LVG_ERR_INVALID_ARG, "null edge array");
+  BatchInput in;
+  in.G = n_graphs;
+  in.eoff = entry_off;
+  in.voff = vertex_off;
+  in.host = host;
+  in.src.resize(n_graphs);
+  in.dst.resize(n_graphs);
+  in.w.resize(n_graphs);
+  for (int32_t g = 0; g < n_graphs; ++g) {
+    const int64_t e0 = entry_off[g];
+    in.src[g] = src ? src + e0 : nullptr;
+    in.dst[g] = dst ? dst + e0 : nullptr;
+    in.w[g] = w ? w + e0 : nullptr;
+  }
+  return in;
+}
+}  // namespace
+
 extern "C" lvg_status lvg_batch_run(lvg_ctx* c, const int32_t* src, const int32_t* dst, const float* w,
                                     const int64_t* entry_off, const int32_t* vertex_off, int32_t n_graphs,
                                     int32_t* part_out, double* q_out, int32_t* levels_out, int32_t* comms_out,
                                     int32_t* status_out) {
   return guarded(c, [&] {
     check_ctx(c);
-    require(n_graphs >= 1 && entry_off && vertex_off, LVG_ERR_INVALID_ARG, "need at least one graph and offsets");
-    require(entry_off[0] == 0 && vertex_off[0] == 0, LVG_ERR_INVALID_ARG, "offsets must start at 0");
-    require(entry_off[n_graphs] == 0 || (src && dst && w), LVG_ERR_INVALID_ARG, "null edge array");
-    batch_run(c, false, src, dst, w, entry_off, vertex_off, n_graphs, part_out, q_out, levels_out, comms_out,
-              status_out);
+    BatchInput in = packed_input(src, dst, w, entry_off, vertex_off, n_graphs, true);
+    batch_run(c, in, part_out, q_out, levels_out, comms_out, status_out);
   });
+}
+
+extern "C" lvg_status lvg_batch_run_graphs(lvg_ctx* c, int32_t n_graphs, const int32_t* const* d_src,
+                                           const int32_t* const* d_dst, const float* const* d_w,
+                                           const int64_t* n_entries, const int32_t* n_vertices, int32_t* part_out,
+                                           double* q_out, int32_t* levels_out, int32_t* comms_out,
+                                           int32_t* status_out) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(n_graphs >= 1 && d_src && d_dst && d_w && n_entries && n_vertices, LVG_ERR_INVALID_ARG,
+            "need at least one graph and its arrays");
+    std::vector<int64_t> eoff(n_graphs + 1, 0);
+    std::vector<int32_t> voff(n_graphs + 1, 0);
+    for (int32_t g = 0; g < n_graphs; ++g) {
+      require(n_entries[g] >= 0 && n_vertices[g] >= 0, LVG_ERR_INVALID_ARG, "negative size");
+      require((int64_t)voff[g] + n_vertices[g] < ((int64_t)1 << 31), LVG_ERR_CAPACITY,
+              "a batch may hold at most 2^31-1 vertices");
+      eoff[g + 1] = eoff[g] + n_entries[g];
+      voff[g + 1] = voff[g] + n_vertices[g];
+    }
+    BatchInput in;
+    in.G = n_graphs;
+    in.eoff = eoff.data();
+    in.voff = voff.data();
+    in.src.assign(d_src, d_src + n_graphs);
+    in.dst.assign(d_dst, d_dst + n_graphs);
+    in.w.assign(d_w, d_w + n_graphs);
+    batch_run(c, in, part_out, q_out, levels_out, comms_out, status_out);
+  });
+}
+
+extern "C" lvg_status lvg_reserve(lvg_ctx* c, int64_t bytes) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(bytes >= 0, LVG_ERR_INVALID_ARG, "negative size");
+    require(!c->loaded, LVG_ERR_STATE, "reserve before loading a graph");
+    c->arena.reserve((size_t)bytes);
+  });
+}
+
+extern "C" lvg_status lvg_batch_footprint(int64_t n_vertices, int64_t n_entries, int32_t n_graphs, int64_t* bytes) {
+  if (!bytes || n_vertices < 0 || n_entries < 0 || n_graphs < 0) return LVG_ERR_INVALID_ARG;
+  *bytes = (int64_t)(arena_estimate(n_vertices, n_entries, true) + 256 * (size_t)n_graphs +
+                     8 * (size_t)n_vertices);
+  return LVG_OK;
 }
 
 extern "C" lvg_status lvg_batch_run_device(lvg_ctx* c, const int32_t* d_src, const int32_t* d_dst,
@@ -1117,10 +1213,7 @@ extern "C" lvg_status lvg_batch_run_device(lvg_ctx* c, const int32_t* d_src, con
                                            int32_t* comms_out, int32_t* status_out) {
   return guarded(c, [&] {
     check_ctx(c);
-    require(n_graphs >= 1 && entry_off && vertex_off, LVG_ERR_INVALID_ARG, "need at least one graph and offsets");
-    require(entry_off[0] == 0 && vertex_off[0] == 0, LVG_ERR_INVALID_ARG, "offsets must start at 0");
-    require(entry_off[n_graphs] == 0 || (d_src && d_dst && d_w), LVG_ERR_INVALID_ARG, "null edge array");
-    batch_run(c, true, d_src, d_dst, d_w, entry_off, vertex_off, n_graphs, part_out, q_out, levels_out, comms_out,
-              status_out);
+    BatchInput in = packed_input(d_src, d_dst, d_w, entry_off, vertex_off, n_graphs, false);
+    batch_run(c, in, part_out, q_out, levels_out, comms_out, status_out);
   });
 }

@@ -12,6 +12,7 @@
 // round-to-nearest intrinsics so it rounds exactly as the CPU oracle does.
 #include <algorithm>
 #include <climits>
+#include <mutex>
 #include <vector>
 
 #include "louvain.cuh"
@@ -1141,13 +1142,12 @@ __global__ void compose_kernel(int32_t* composed, const int32_t* part_level, int
 }
 
 int sm_count() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
+  static const int sms = [] {   // thread-safe one-time initialisation
+    int dev = 0, n = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+  }();
   return sms;
 }
 
@@ -1520,7 +1520,9 @@ void launch_q(const LevelGraph& g, CommState& st, double* dst, cudaStream_t s) {
 
 // Dynamic shared memory limits of the move kernels, set before any capture.
 static void set_move_attributes(int block_log) {
+  static std::mutex mu;
   static int done_log = -1;
+  std::lock_guard<std::mutex> lock(mu);   // contexts on several host threads
   if (done_log >= block_log) return;
   LVG_CUDA(cudaFuncSetAttribute(move_tile_kernel<int>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(TileSmem<int>)));
@@ -1742,10 +1744,14 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
   LVG_CUDA(cudaMemsetAsync(Ain, 0, sizeof(double) * std::max(C, 1), s));
   if (E > 0 && C <= kNmSmemMax) {
     size_t smem = sizeof(double) * 2 * (size_t)C;
+    static std::mutex mu;
     static size_t attr = 0;
-    if (smem > 48 * 1024 && smem > attr) {
-      LVG_CUDA(cudaFuncSetAttribute(nm_accum_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr = smem;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      if (smem > 48 * 1024 && smem > attr) {
+        LVG_CUDA(cudaFuncSetAttribute(nm_accum_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = smem;
+      }
     }
     nm_accum_smem_kernel<<<sm_grid(E, kThreads), kThreads, smem, s>>>(src, dst, w, E, part, C, Kc, Ain);
     LVG_LAUNCH();
@@ -1813,21 +1819,25 @@ void compose(int32_t* composed, const int32_t* part_level, int64_t n, cudaStream
 namespace lvg {
 namespace {
 
-__global__ void batch_globalize_kernel(const int32_t* lsrc, const int32_t* ldst, const float* w, int64_t E,
-                                       const int64_t* eoff, const int32_t* voff, int32_t G, int32_t* gsrc,
-                                       int32_t* gdst, uint32_t* bad) {
+// Level-0 union list: graph g's entries come from its own arrays (psrc[g],
+// pdst[g], pw[g]) and its ids are moved up by voff[g].
+__global__ void batch_globalize_kernel(const int32_t* const* psrc, const int32_t* const* pdst,
+                                       const float* const* pw, int64_t E, const int64_t* eoff, const int32_t* voff,
+                                       int32_t G, int32_t* gsrc, int32_t* gdst, float* gw, uint32_t* bad) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
     int lo = 0, hi = G - 1;
     while (lo < hi) {  // last graph whose first entry is <= e
       int mid = (lo + hi + 1) >> 1;
       if (eoff[mid] <= e) lo = mid; else hi = mid - 1;
     }
+    const int64_t j = e - eoff[lo];
     int32_t n = voff[lo + 1] - voff[lo];
-    int32_t a = lsrc[e], b = ldst[e];
-    float x = w[e];
+    int32_t a = psrc[lo][j], b = pdst[lo][j];
+    float x = pw[lo][j];
     if (a < 0 || a >= n || b < 0 || b >= n || !(x >= 0.0f) || isinf(x)) atomicOr(bad, 1u);
     gsrc[e] = a + voff[lo];
     gdst[e] = b + voff[lo];
+    gw[e] = x;
   }
 }
 
@@ -1843,6 +1853,11 @@ __global__ void vgid_fill_kernel(const int32_t* vbase, int32_t G, int32_t V, int
 }
 
 // m of every graph: runs of entries of one graph inside a warp add once.
+__global__ void local_ids_kernel(const int32_t* gid, const int32_t* voff, int32_t V, int32_t* local) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x)
+    local[i] = (int32_t)i - voff[gid[i]];
+}
+
 __global__ void batch_m_kernel(const int32_t* src, const float* w, int64_t E, const int32_t* vgid, double* gm) {
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   bool valid = e < E;
@@ -2041,16 +2056,24 @@ __global__ void batch_nm_term_kernel(const double* Kc, const double* Ain, const 
 
 }  // namespace
 
-void batch_globalize(const int32_t* lsrc, const int32_t* ldst, const float* w, int64_t E, const int64_t* eoff,
-                     const int32_t* voff, int32_t G, int32_t* gsrc, int32_t* gdst, uint32_t* bad, cudaStream_t s) {
+void batch_globalize(const int32_t* const* psrc, const int32_t* const* pdst, const float* const* pw, int64_t E,
+                     const int64_t* eoff, const int32_t* voff, int32_t G, int32_t* gsrc, int32_t* gdst, float* gw,
+                     uint32_t* bad, cudaStream_t s) {
   if (E == 0) return;
-  batch_globalize_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(lsrc, ldst, w, E, eoff, voff, G, gsrc, gdst, bad);
+  batch_globalize_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(psrc, pdst, pw, E, eoff, voff, G, gsrc, gdst, gw,
+                                                                    bad);
   LVG_LAUNCH();
 }
 
 void batch_vgid(const int32_t* vbase, int32_t G, int32_t V, int32_t* vgid, cudaStream_t s) {
   if (V == 0) return;
   vgid_fill_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(vbase, G, V, vgid);
+  LVG_LAUNCH();
+}
+
+void batch_local_ids(const int32_t* gid, const int32_t* voff, int32_t V, int32_t* local, cudaStream_t s) {
+  if (V == 0) return;
+  local_ids_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(gid, voff, V, local);
   LVG_LAUNCH();
 }
 

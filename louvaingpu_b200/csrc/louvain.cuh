@@ -186,9 +186,14 @@ struct BatchPlan {
   int64_t nblk = 0;
 };
 
-void batch_globalize(const int32_t* lsrc, const int32_t* ldst, const float* w, int64_t E, const int64_t* eoff,
-                     const int32_t* voff, int32_t G, int32_t* gsrc, int32_t* gdst, uint32_t* bad, cudaStream_t s);
+// Union list of the graphs' own lists (device pointer arrays of G entries);
+// *bad |= 1 on an id outside its graph or a negative / non-finite weight.
+void batch_globalize(const int32_t* const* psrc, const int32_t* const* pdst, const float* const* pw, int64_t E,
+                     const int64_t* eoff, const int32_t* voff, int32_t G, int32_t* gsrc, int32_t* gdst, float* gw,
+                     uint32_t* bad, cudaStream_t s);
 void batch_vgid(const int32_t* vbase, int32_t G, int32_t V, int32_t* vgid, cudaStream_t s);
+// local[i] = i - voff[gid[i]]
+void batch_local_ids(const int32_t* gid, const int32_t* voff, int32_t V, int32_t* local, cudaStream_t s);
 void batch_m(const int32_t* src, const float* w, int64_t E, const int32_t* vgid, double* gm, int32_t G,
              cudaStream_t s);
 void batch_init(const LevelGraph& g, CommState& st, cudaStream_t s);

@@ -6,6 +6,8 @@
 // digit-major [256][tiles] table yields every tile's global digit offsets, and
 // a scatter kernel ranks the tile's keys stably in shared memory (warp
 // __match_any_sync multisplit) and writes them to their global positions.
+#include <mutex>
+
 #include "prims.cuh"
 
 namespace lvg {
@@ -245,12 +247,11 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
                      cudaStream_t s) {
   if (n >= ((int64_t)1 << 32)) throw Error(LVG_ERR_CAPACITY, "radix sort limited to 2^32-1 entries");
   if (n <= 1 || bits <= 0) return 0;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static std::once_flag attr_once;
+  std::call_once(attr_once, [] {
     LVG_CUDA(cudaFuncSetAttribute(rs_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(RsSmem)));
-    attr_set = true;
-  }
+  });
   HiScope hs(a);
   int64_t ntiles = (n + kRsTile - 1) / kRsTile;
   uint32_t* hist = a.hi_n<uint32_t>(kRadix * ntiles + 1);
