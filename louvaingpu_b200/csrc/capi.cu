@@ -117,6 +117,7 @@ size_t arena_estimate(int64_t V, int64_t E, bool copy_list) {
   b += 16 * (size_t)E + 80 * (size_t)V;     // CSR (<= 2E entries) + per-vertex + state
   b += 88 * (size_t)E + 24 * (size_t)V;     // build scratch: 2 x 2E x 12 B sort, head/pos, wsum
   b += 16 * (size_t)E;                      // hub tables (degree-bounded) and per-level partitions
+  b += 32 * (size_t)V + (size_t)E / 4;      // first-pass chunk lists and partials
   b += (size_t)64 << 20;
   return b;
 }
@@ -267,7 +268,8 @@ void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int
         c->mev.push_back(ev);
       }
       LVG_CUDA(cudaEventRecord(c->mev[e], s));
-      if (use_graphs) LVG_CUDA(cudaGraphLaunch(c->g_moves, s));
+      if (launched == 0) launch_moves_singleton(c->g, c->st, s, &c->side);   // state is singletons
+      else if (use_graphs) LVG_CUDA(cudaGraphLaunch(c->g_moves, s));
       else launch_moves(c->g, c->st, s, &c->side);
       LVG_CUDA(cudaEventRecord(c->mev[e + 1], s));
       if (use_graphs) LVG_CUDA(cudaGraphLaunch(c->g_commit, s));
@@ -986,7 +988,8 @@ void batch_run(lvg_ctx* c, const BatchInput& in, int32_t* part_out, double* q_ou
       int launched = 0;
       for (;;) {
         for (int p = 0; p < chunk; ++p) {
-          launch_moves(g, st, s, &c->side);
+          if (launched == 0) launch_moves_singleton(g, st, s, &c->side);   // from batch_init's singletons
+          else launch_moves(g, st, s, &c->side);
           batch_commit(1, bp, gm, st, C, s);
           batch_ctl(0, bp, st, C, G, s);
           ++launched;

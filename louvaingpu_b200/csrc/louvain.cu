@@ -548,6 +548,138 @@ __global__ void __launch_bounds__(kThreads) move_thread_kernel(MoveArgs P, EllAr
   }
 }
 
+// ------------------------------------------------------- singleton first pass
+// The first pass of every level starts from singletons (comm[i] = i,
+// tot[i] = k[i], size[i] = 1: InitKernel.cu:213-236, OneLevelKernel.cu:87).
+// Then every neighbour is its own candidate community with W = w(i,j) (the
+// CSR has one entry per neighbour), own is never a neighbour, and the number
+// of distinct neighbour communities is the degree (+1 for a self loop).  The
+// best candidate is a plain argmax over the row -- higher gain, then lower
+// community -- which splits into independent pieces: no tables, no
+// community gather.  Decisions are the general kernels' bit for bit.
+template <int D>
+__global__ void __launch_bounds__(kThreads) sp_thread_kernel(MoveArgs P, EllArgs L) {
+  if (P.ctl->done) return;
+  for (int64_t j = blockIdx.x * (int64_t)kThreads + threadIdx.x; j < L.n; j += (int64_t)gridDim.x * kThreads) {
+    int32_t c[D];
+    float w[D];
+    double t[D];
+    const int4* cp = reinterpret_cast<const int4*>(L.col + j * D);
+    const float4* wp = reinterpret_cast<const float4*>(L.w + j * D);
+#pragma unroll
+    for (int q = 0; q < D / 4; ++q) {
+      int4 a = __ldcs(cp + q);
+      float4 b = __ldcs(wp + q);
+      c[4 * q] = a.x; c[4 * q + 1] = a.y; c[4 * q + 2] = a.z; c[4 * q + 3] = a.w;
+      w[4 * q] = b.x; w[4 * q + 1] = b.y; w[4 * q + 2] = b.z; w[4 * q + 3] = b.w;
+    }
+    const VInfo vi = L.info[j];
+    const int32_t i = vi.vid_loop >> 1;
+    const double kf = vi.kfrac;
+#pragma unroll
+    for (int q = 0; q < D; ++q) t[q] = c[q] >= 0 ? P.tot[c[q]] : 0.0;   // independent gathers
+    double bg = 0.0, bw = 0.0;
+    int32_t bc = kNone;
+    int deg = 0;
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+      if (c[q] >= 0) {
+        ++deg;
+        const double W = (double)w[q];
+        if (W != 0.0) {                                            // OneLevelKernel.cu:303
+          const double g = __dsub_rn(W, __dmul_rn(t[q], kf));      // OneLevelKernel.cu:307-313
+          if (g > 0.0 && better(g, c[q], bg, bc)) { bg = g; bc = c[q]; bw = W; }
+        }
+      }
+    }
+    apply_decision_kl(P, i, i, bc, bw, deg + (vi.vid_loop & 1), vi.k, vi.loopw);
+  }
+}
+
+// Rows longer than 32: warp-sized chunks of kSpChunk entries.  A row of one
+// chunk is decided by its warp; longer rows leave a partial per chunk for
+// sp_combine_kernel.
+constexpr int kSpChunk = 512;
+
+__global__ void __launch_bounds__(kThreads) sp_chunk_kernel(MoveArgs P, const int2* chunks, int64_t nch,
+                                                            HubPartial* part) {
+  if (P.ctl->done) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (kThreads / 32);
+  for (int64_t q = blockIdx.x * (int64_t)(kThreads / 32) + (threadIdx.x >> 5); q < nch; q += nwarps) {
+    const int2 ch = chunks[q];
+    const int32_t i = ch.x;
+    const int64_t row = P.off[i], deg = P.off[i + 1] - row;
+    const int64_t beg = row + (int64_t)ch.y * kSpChunk;
+    const int64_t end = min(beg + (int64_t)kSpChunk, row + deg);
+    const double kf = P.kfrac[i];
+    double bg = 0.0, bw = 0.0;
+    int32_t bc = kNone;
+    for (int64_t e0 = beg; e0 < end; e0 += 4 * 32) {
+      int32_t c[4];
+      float w[4];
+      double t[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t e = e0 + u * 32 + lane;
+        c[u] = e < end ? __ldcs(P.col + e) : kNone;
+        w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) t[u] = c[u] != kNone ? P.tot[c[u]] : 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double W = (double)w[u];
+        if (c[u] != kNone && W != 0.0) {
+          const double g = __dsub_rn(W, __dmul_rn(t[u], kf));
+          if (g > 0.0 && better(g, c[u], bg, bc)) { bg = g; bc = c[u]; bw = W; }
+        }
+      }
+    }
+    warp_best(bg, bc, bw);
+    if (lane == 0) {
+      if (deg <= kSpChunk) apply_decision(P, i, i, bc, bw, (int32_t)deg + (P.has_loop[i] ? 1 : 0));
+      else part[q] = HubPartial{bg, bw, bc, 0};
+    }
+  }
+}
+
+__global__ void sp_combine_kernel(MoveArgs P, const int2* multi, int64_t nmulti, const HubPartial* part) {
+  if (P.ctl->done) return;
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < nmulti; x += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t i = multi[x].x, first = multi[x].y;
+    const int64_t deg = P.off[i + 1] - P.off[i];
+    const int32_t n = (int32_t)((deg + kSpChunk - 1) / kSpChunk);
+    double g = 0.0, w = 0.0;
+    int32_t c = kNone;
+    for (int32_t k = 0; k < n; ++k) {
+      const HubPartial h = part[first + k];
+      if (better(h.g, h.c, g, c)) { g = h.g; c = h.c; w = h.w; }
+    }
+    apply_decision(P, i, i, c, w, (int32_t)deg + (P.has_loop[i] ? 1 : 0));
+  }
+}
+
+// Chunk lists of the rows longer than 32 (the classes from kBTile on).
+__global__ void sp_count_kernel(const int32_t* list, int64_t n, const int64_t* off, uint32_t* cnt, uint32_t* multi) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t i = list[j];
+    const int64_t nc = (off[i + 1] - off[i] + kSpChunk - 1) / kSpChunk;
+    cnt[j] = (uint32_t)nc;
+    multi[j] = nc > 1 ? 1u : 0u;
+  }
+}
+
+__global__ void sp_fill_kernel(const int32_t* list, int64_t n, const int64_t* off, const uint32_t* first,
+                               const uint32_t* mpos, int2* chunks, int2* multi) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t i = list[j];
+    const uint32_t f = first[j], nc = first[j + 1] - f;
+    for (uint32_t k = 0; k < nc; ++k) chunks[f + k] = make_int2(i, (int)k);
+    if (mpos[j + 1] != mpos[j]) multi[mpos[j]] = make_int2(i, (int)f);
+  }
+}
+
 // k/2m; in a batched run m is the vertex's own graph's (gm[vgid[i]]).
 __global__ void kfrac_kernel(int32_t V, const double* k, double m, const double* gm, const int32_t* vgid,
                              double* kfrac) {
@@ -1452,6 +1584,33 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
     LVG_CUDA(cudaMemsetAsync(g.hub_sawown, 0, sizeof(uint32_t) * nhub, s));
     LVG_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
   }
+  // singleton first pass: warp chunks of the rows longer than 32
+  g.sp_nchunk = 0;
+  g.sp_nmulti = 0;
+  {
+    const int64_t nl = g.nbucket[kBTile] + g.nbucket[kBBlock] + g.nbucket[kBHub];
+    const int32_t* llist = g.blist + g.bstart[kBTile];
+    if (nl > 0) {
+      HiScope hs(a);
+      uint32_t* cnt = a.hi_n<uint32_t>(nl + 1);
+      uint32_t* mul = a.hi_n<uint32_t>(nl + 1);
+      sp_count_kernel<<<sm_grid(nl, kThreads), kThreads, 0, s>>>(llist, nl, g.off, cnt, mul);
+      LVG_LAUNCH();
+      scan_u32(cnt, cnt, nl, a, s);
+      scan_u32(mul, mul, nl, a, s);
+      uint32_t tot[2] = {0, 0};
+      LVG_CUDA(cudaMemcpyAsync(&tot[0], cnt + nl, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      LVG_CUDA(cudaMemcpyAsync(&tot[1], mul + nl, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      LVG_CUDA(cudaStreamSynchronize(s));
+      g.sp_nchunk = tot[0];
+      g.sp_nmulti = tot[1];
+      g.sp_chunk = a.lo_n<int2>(g.sp_nchunk);
+      g.sp_multi = a.lo_n<int2>(g.sp_nmulti);
+      g.sp_part = a.lo_n<HubPartial>(g.sp_nmulti > 0 ? g.sp_nchunk : 0);
+      sp_fill_kernel<<<sm_grid(nl, kThreads), kThreads, 0, s>>>(llist, nl, g.off, cnt, mul, g.sp_chunk, g.sp_multi);
+      LVG_LAUNCH();
+    }
+  }
   g.block_log = block_table_log(t);
   set_move_attributes(g.block_log);
 }
@@ -1607,6 +1766,49 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
       LVG_CUDA(cudaEventRecord(ss->join[k], ss->side[k]));
       LVG_CUDA(cudaStreamWaitEvent(s, ss->join[k], 0));
     }
+  }
+}
+
+template <int D>
+static void launch_sp_thread(const LevelGraph& g, MoveArgs P, int bucket, cudaStream_t s) {
+  EllArgs L;
+  L.n = g.nbucket[bucket];
+  if (L.n == 0) return;
+  L.col = g.ell_col + g.ell_base[bucket];
+  L.w = g.ell_w + g.ell_base[bucket];
+  L.list = g.blist + g.bstart[bucket];
+  L.info = g.ell_info + (g.bstart[bucket] - g.bstart[kB4]);
+  int64_t blocks = std::min<int64_t>((L.n + kThreads - 1) / kThreads, (int64_t)sm_count() * 8);
+  sp_thread_kernel<D><<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, 0, s>>>(P, L);
+  LVG_LAUNCH();
+}
+
+void launch_moves_singleton(const LevelGraph& g, CommState& st, cudaStream_t s, const SideStreams* ss) {
+  MoveArgs P = move_args(g, st);
+  cudaStream_t sc = s;
+  if (ss) {
+    LVG_CUDA(cudaEventRecord(ss->fork, s));
+    LVG_CUDA(cudaStreamWaitEvent(ss->side[0], ss->fork, 0));
+    sc = ss->side[0];
+  }
+  if (g.sp_nchunk > 0) {
+    const int64_t blocks = std::min<int64_t>((g.sp_nchunk + kThreads / 32 - 1) / (kThreads / 32),
+                                             (int64_t)sm_count() * 16);
+    sp_chunk_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, 0, sc>>>(P, g.sp_chunk, g.sp_nchunk,
+                                                                                 g.sp_part);
+    LVG_LAUNCH();
+    if (g.sp_nmulti > 0) {
+      sp_combine_kernel<<<sm_grid(g.sp_nmulti, kThreads), kThreads, 0, sc>>>(P, g.sp_multi, g.sp_nmulti, g.sp_part);
+      LVG_LAUNCH();
+    }
+  }
+  launch_sp_thread<32>(g, P, kB32, s);
+  launch_sp_thread<16>(g, P, kB16, s);
+  launch_sp_thread<8>(g, P, kB8, s);
+  launch_sp_thread<4>(g, P, kB4, s);
+  if (ss) {
+    LVG_CUDA(cudaEventRecord(ss->join[0], ss->side[0]));
+    LVG_CUDA(cudaStreamWaitEvent(s, ss->join[0], 0));
   }
 }
 

@@ -78,6 +78,13 @@ struct LevelGraph {
   int64_t* seg_beg = nullptr;
   int32_t* hub_seg0 = nullptr;    // [nhub+1] first segment of each hub
   struct HubPartial* hub_part = nullptr;
+  // singleton first pass: chunks {vertex, piece} of the rows longer than 32,
+  // rows of more than one chunk {vertex, first chunk}, per-chunk partials
+  int2* sp_chunk = nullptr;
+  int64_t sp_nchunk = 0;
+  int2* sp_multi = nullptr;
+  int64_t sp_nmulti = 0;
+  struct HubPartial* sp_part = nullptr;
 };
 
 struct CommState {
@@ -131,6 +138,9 @@ void launch_pass(const LevelGraph& g, CommState& st, cudaStream_t s, const SideS
 void launch_commit(const LevelGraph& g, CommState& st, cudaStream_t s);
 // Launch only the move kernels (decisions, accumulations into d*).
 void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const SideStreams* ss);
+// The move kernels of a pass from the singleton state (the first pass of a
+// level, right after init_state / batch_init): same decisions, no tables.
+void launch_moves_singleton(const LevelGraph& g, CommState& st, cudaStream_t s, const SideStreams* ss);
 // After the loop is done: isolated-vertex merge, final commit, ctl->q_ret.
 void launch_merge(const LevelGraph& g, CommState& st, cudaStream_t s);
 // Q of the committed state into *dst (device).
