@@ -64,6 +64,8 @@ struct lvg_ctx {
   std::vector<LevelRec> levels;
   std::vector<float> pass_ms;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t pev[6] = {};        // phase timing: build, renumber, induce (start, end)
+  float build_ms = 0.0f;          // build of the current level
   SideStreams side{};
   bool have_side = false;
   std::vector<cudaEvent_t> mev;   // move-phase events, two per pass
@@ -151,9 +153,13 @@ void ensure_graphs(lvg_ctx* c) {
 
 void prepare_level(lvg_ctx* c) {
   drop_graphs(c);
+  LVG_CUDA(cudaEventRecord(c->pev[0], c->stream));
   build_level(c->g, c->tune, c->arena, c->stream);
   alloc_state(c->g, c->st, c->arena);
   init_state(c->g, c->st, 0.0, c->cfg.pass_min_gain, c->cfg.max_passes, c->arena, c->stream);
+  LVG_CUDA(cudaEventRecord(c->pev[1], c->stream));
+  LVG_CUDA(cudaEventSynchronize(c->pev[1]));
+  c->build_ms = elapsed(c->pev[0], c->pev[1]);
   c->have_state = true;
   c->renumbered = false;
 }
@@ -166,10 +172,7 @@ void load_common(lvg_ctx* c, const int32_t* d_src, const int32_t* d_dst, const f
   c->dst0 = d_dst;
   c->w0 = d_w;
   c->composed = c->arena.lo_n<int32_t>(V);
-  std::vector<int32_t> iota(V);
-  for (int32_t i = 0; i < V; ++i) iota[i] = i;
-  LVG_CUDA(cudaMemcpyAsync(c->composed, iota.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, c->stream));
-  sync(c);
+  iota(c->composed, V, c->stream);
   c->base_lo = c->arena.lo;
   c->run_hi = c->arena.hi;
   c->levels.clear();
@@ -311,8 +314,11 @@ int32_t renumber_level(lvg_ctx* c) {
   c->run_hi = c->arena.hi;
   LVG_CUDA(cudaMemcpyAsync(labels, c->st.comm, sizeof(int32_t) * std::max(V, 1), cudaMemcpyDeviceToDevice,
                            c->stream));
+  LVG_CUDA(cudaEventRecord(c->pev[2], c->stream));
   int32_t C = renumber(c->g, c->st.comm, part, c->arena, c->stream);
   compose(c->composed, part, c->V0, c->stream);    // partitionAtLevel (LouvainCPP.cpp:82-106)
+  LVG_CUDA(cudaEventRecord(c->pev[3], c->stream));
+  LVG_CUDA(cudaEventSynchronize(c->pev[3]));
   c->d_part_cur = part;
   c->C_cur = C;
   c->renumbered = true;
@@ -324,6 +330,8 @@ int32_t renumber_level(lvg_ctx* c) {
   r.info.n_entries = c->g.E;
   r.info.nnz = c->g.nnz;
   r.info.n_comms = C;
+  r.info.ms_build = c->build_ms;
+  r.info.ms_renumber = elapsed(c->pev[2], c->pev[3]);
   c->levels.push_back(r);
   return C;
 }
@@ -333,6 +341,7 @@ void induce_level(lvg_ctx* c) {
   int32_t *os = nullptr, *od = nullptr;
   float* ow = nullptr;
   c->arena.hi = c->run_hi;
+  LVG_CUDA(cudaEventRecord(c->pev[4], c->stream));
   int64_t n = induce(c->g, c->d_part_cur, c->C_cur, &os, &od, &ow, c->arena, c->stream);
   // the next level's list moves down to the start of the level region
   c->arena.lo = c->base_lo;
@@ -344,7 +353,9 @@ void induce_level(lvg_ctx* c) {
     LVG_CUDA(cudaMemcpyAsync(nd, od, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
     LVG_CUDA(cudaMemcpyAsync(nw, ow, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
   }
+  LVG_CUDA(cudaEventRecord(c->pev[5], c->stream));
   sync(c);
+  if (!c->levels.empty()) c->levels.back().info.ms_induce = elapsed(c->pev[4], c->pev[5]);
   c->arena.hi = c->run_hi;
   int32_t C = c->C_cur;
   c->g = LevelGraph();
@@ -418,6 +429,7 @@ lvg_status lvg_create(const lvg_config* cfg, lvg_ctx** out) {
     c->stream = c->own_stream;
     LVG_CUDA(cudaEventCreate(&c->ev0));
     LVG_CUDA(cudaEventCreate(&c->ev1));
+    for (auto& e : c->pev) LVG_CUDA(cudaEventCreate(&e));
     for (int k = 0; k < 3; ++k) {
       LVG_CUDA(cudaStreamCreateWithFlags(&c->side.side[k], cudaStreamNonBlocking));
       LVG_CUDA(cudaEventCreateWithFlags(&c->side.join[k], cudaEventDisableTiming));
@@ -447,6 +459,8 @@ lvg_status lvg_destroy(lvg_ctx* c) {
   c->arena.release();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (auto& e : c->pev)
+    if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : c->mev) cudaEventDestroy(e);
   if (c->have_side) {
     for (int k = 0; k < 3; ++k) {

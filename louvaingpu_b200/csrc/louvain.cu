@@ -37,7 +37,7 @@ struct VInfo {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kHubChunk = 512;
+constexpr int kHubChunk = 2048;
 constexpr int kNone = INT_MAX;
 
 __device__ __forceinline__ uint32_t hash_c(int32_t c, int logT) {
@@ -151,25 +151,44 @@ __global__ void row_count_kernel(const int32_t* src, int64_t E, int64_t* rowcnt)
 
 enum : uint32_t { kNotSorted = 1u, kNotSymmetric = 2u };
 
+// Sortedness (exact) and symmetry of the list in one coalesced pass.  The
+// symmetry test compares order-free fingerprints: the sums mod 2^64 of two
+// independent 64-bit hashes of (src, dst, weight bits) over the non-loop
+// entries against the same sums of (dst, src, weight bits).  A strictly sorted
+// list has no repeated entry, so the sums agree when the list equals its
+// transpose; a list that is not symmetric passes only on a 128-bit collision.
+__device__ __forceinline__ uint64_t edge_hash(uint32_t u, uint32_t v, uint32_t wb, uint64_t key) {
+  return mix64(mix64((((uint64_t)u << 32) | v) ^ key) + (uint64_t)wb * 0x9E3779B97F4A7C15ull + key);
+}
+
 __global__ void list_check_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
-                                  const int64_t* rowstart, uint32_t* flags) {
+                                  uint32_t* flags, unsigned long long* sums) {
+  const uint64_t K1 = 0x243F6A8885A308D3ull, K2 = 0x13198A2E03707344ull;
+  uint64_t d1 = 0, d2 = 0;
+  bool unsorted = false;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
-    int32_t u = src[e], v = dst[e];
+    const int32_t u = src[e], v = dst[e];
     if (e + 1 < E) {
-      int32_t u2 = src[e + 1], v2 = dst[e + 1];
-      if (!(u2 > u || (u2 == u && v2 > v))) atomicOr(flags, kNotSorted);
+      const int32_t u2 = src[e + 1], v2 = dst[e + 1];
+      if (!(u2 > u || (u2 == u && v2 > v))) unsorted = true;
     }
     if (u != v) {
-      int64_t lo = rowstart[v], hi = rowstart[v + 1] - 1;
-      bool found = false;
-      while (lo <= hi) {
-        int64_t mid = (lo + hi) >> 1;
-        int32_t x = dst[mid];
-        if (x == u) { found = __float_as_uint(w[mid]) == __float_as_uint(w[e]); break; }
-        if (x < u) lo = mid + 1; else hi = mid - 1;
-      }
-      if (!found) atomicOr(flags, kNotSymmetric);
+      const uint32_t wb = __float_as_uint(w[e]);
+      d1 += edge_hash((uint32_t)u, (uint32_t)v, wb, K1) - edge_hash((uint32_t)v, (uint32_t)u, wb, K1);
+      d2 += edge_hash((uint32_t)u, (uint32_t)v, wb, K2) - edge_hash((uint32_t)v, (uint32_t)u, wb, K2);
     }
+  }
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    d1 += __shfl_down_sync(full, d1, o);
+    d2 += __shfl_down_sync(full, d2, o);
+  }
+  const bool any_unsorted = __any_sync(full, unsorted);
+  if ((threadIdx.x & 31) == 0) {
+    if (d1) atomicAdd(&sums[0], (unsigned long long)d1);
+    if (d2) atomicAdd(&sums[1], (unsigned long long)d2);
+    if (any_unsorted) atomicOr(flags, kNotSorted);
   }
 }
 
@@ -322,13 +341,6 @@ __device__ __forceinline__ bool better(double g2, int32_t c2, double g1, int32_t
   return g2 > g1 || (g2 == g1 && c2 < c1);
 }
 
-__device__ __forceinline__ void consider(int32_t c, double W, double kf, const double* tot, double& bg,
-                                         int32_t& bc, double& bw) {
-  if (W != 0.0) {                                                // OneLevelKernel.cu:303
-    double g = __dsub_rn(W, __dmul_rn(tot[c], kf));              // OneLevelKernel.cu:307-313
-    if (g > 0.0 && better(g, c, bg, bc)) { bg = g; bc = c; bw = W; }
-  }
-}
 
 __device__ __forceinline__ void warp_best(double& bg, int32_t& bc, double& bw) {
   const unsigned full = 0xffffffffu;
@@ -387,7 +399,8 @@ __device__ __forceinline__ void apply_decision(const MoveArgs& P, int32_t i, int
 }
 
 // Open-addressing insert of (c, w) into a table of 2^logT slots.
-__device__ __forceinline__ bool table_insert(int32_t* keys, double* vals, int logT, int32_t c, double w) {
+template <typename Acc>
+__device__ __forceinline__ bool table_insert(int32_t* keys, Acc* vals, int logT, int32_t c, Acc w) {
   uint32_t T = 1u << logT;
   uint32_t h = hash_c(c, logT);
   for (uint32_t p = 0; p < T; ++p) {
@@ -398,17 +411,36 @@ __device__ __forceinline__ bool table_insert(int32_t* keys, double* vals, int lo
   return false;
 }
 
-// Block per vertex (degree up to block_max), table in dynamic shared memory.
+// Entries [e0 + u*stride) of a row, u < 4: columns and weights first, then
+// the four community gathers, so that each thread keeps several loads in
+// flight; kNone marks entries past `end`.
+constexpr int kUnroll = 4;
+__device__ __forceinline__ void gather4(const MoveArgs& P, int64_t e0, int64_t stride, int64_t end, int32_t (&c)[4],
+                                        float (&w)[4]) {
+  int32_t col[kUnroll];
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    const int64_t e = e0 + u * stride;
+    col[u] = e < end ? __ldcs(P.col + e) : -1;
+    w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
+  }
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) c[u] = col[u] >= 0 ? P.comm[col[u]] : kNone;
+}
+
+// Block per vertex (degree up to block_max), table in dynamic shared memory;
+// int32 sums when the weights are integral (exact, half the table bytes).
+template <typename Acc>
 __global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int maxLog) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double rg[kThreads / 32], rw[kThreads / 32];
   __shared__ int32_t rc[kThreads / 32], rn[kThreads / 32], rs[kThreads / 32];
   if (P.ctl->done) return;
   const int Tmax = 1 << maxLog;
-  double* vals = reinterpret_cast<double*>(smem);
+  Acc* vals = reinterpret_cast<Acc*>(smem);
   int32_t* keys = reinterpret_cast<int32_t*>(vals + Tmax);
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int s = threadIdx.x; s < Tmax; s += kThreads) { keys[s] = -1; vals[s] = 0.0; }
+  for (int s = threadIdx.x; s < Tmax; s += kThreads) { keys[s] = -1; vals[s] = Acc(0); }
   __syncthreads();
   bool overflow = false;
   for (int64_t item = blockIdx.x; item < P.n; item += gridDim.x) {
@@ -418,23 +450,44 @@ __global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int ma
     int logT = min(maxLog, max(5, ceil_log2(2 * (end - beg))));
     int T = 1 << logT;
     bool sawown = false;
-    for (int64_t e = beg + threadIdx.x; e < end; e += kThreads) {
-      int32_t c = P.comm[__ldcs(P.col + e)];
-      sawown |= (c == own);
-      if (!table_insert(keys, vals, logT, c, (double)__ldcs(P.cw + e))) overflow = true;
+    for (int64_t e0 = beg + threadIdx.x; e0 < end; e0 += kUnroll * kThreads) {
+      int32_t c[kUnroll];
+      float wv[kUnroll];
+      gather4(P, e0, kThreads, end, c, wv);
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        if (c[u] != kNone) {
+          sawown |= (c[u] == own);
+          if (!table_insert<Acc>(keys, vals, logT, c[u], (Acc)wv[u])) overflow = true;
+        }
+      }
     }
     __syncthreads();
     double kf = P.kfrac[i];
     double bg = 0.0, bw = 0.0;
     int32_t bc = kNone;
     int nocc = 0;
-    for (int s = threadIdx.x; s < T; s += kThreads) {
-      int32_t c = keys[s];
-      if (c >= 0) {
-        ++nocc;
-        consider(c, vals[s], kf, P.tot, bg, bc, bw);
-        keys[s] = -1;
-        vals[s] = 0.0;
+    for (int s0 = threadIdx.x; s0 < T; s0 += kUnroll * kThreads) {
+      int32_t c[kUnroll];
+      double W[kUnroll], t[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int s = s0 + u * kThreads;
+        c[u] = s < T ? keys[s] : -1;
+        W[u] = c[u] >= 0 ? (double)vals[s] : 0.0;
+        if (c[u] >= 0) { keys[s] = -1; vals[s] = Acc(0); }
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) t[u] = (c[u] >= 0 && W[u] != 0.0) ? P.tot[c[u]] : 0.0;
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        if (c[u] >= 0) {
+          ++nocc;
+          if (W[u] != 0.0) {                                            // OneLevelKernel.cu:303
+            const double g = __dsub_rn(W[u], __dmul_rn(t[u], kf));      // OneLevelKernel.cu:307-313
+            if (g > 0.0 && better(g, c[u], bg, bc)) { bg = g; bc = c[u]; bw = W[u]; }
+          }
+        }
       }
     }
     warp_best(bg, bc, bw);
@@ -933,10 +986,17 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(MoveArgs P, HubArg
   double* vals = H.vals + H.toff[h];
   int logT = H.tlog[h];
   bool sawown = false, overflow = false;
-  for (int64_t e = beg + threadIdx.x; e < end; e += kThreads) {
-    int32_t c = P.comm[__ldcs(P.col + e)];
-    sawown |= (c == own);
-    if (!table_insert(keys, vals, logT, c, (double)__ldcs(P.cw + e))) overflow = true;
+  for (int64_t e0 = beg + threadIdx.x; e0 < end; e0 += kUnroll * kThreads) {
+    int32_t c[kUnroll];
+    float wv[kUnroll];
+    gather4(P, e0, kThreads, end, c, wv);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (c[u] != kNone) {
+        sawown |= (c[u] == own);
+        if (!table_insert<double>(keys, vals, logT, c[u], (double)wv[u])) overflow = true;
+      }
+    }
   }
   if (__syncthreads_or(sawown) && threadIdx.x == 0) atomicOr(&H.sawown[h], 1u);
   if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
@@ -963,13 +1023,29 @@ __global__ void __launch_bounds__(kThreads) hub_scan_kernel(MoveArgs P, HubArgs 
   double bg = 0.0, bw = 0.0;
   int32_t bc = kNone;
   int nocc = 0;
-  for (int64_t sl = b0 + threadIdx.x; sl < b1; sl += kThreads) {
-    int32_t c = keys[sl];
-    if (c >= 0) {
-      ++nocc;
-      consider(c, vals[sl], kf, P.tot, bg, bc, bw);
-      keys[sl] = -1;
-      vals[sl] = 0.0;
+  for (int64_t s0 = b0 + threadIdx.x; s0 < b1; s0 += kUnroll * kThreads) {
+    int32_t c[kUnroll];
+    double W[kUnroll], t[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int64_t sl = s0 + u * kThreads;
+      c[u] = sl < b1 ? keys[sl] : -1;
+      W[u] = c[u] >= 0 ? vals[sl] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) t[u] = (c[u] >= 0 && W[u] != 0.0) ? P.tot[c[u]] : 0.0;
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int64_t sl = s0 + u * kThreads;
+      if (c[u] >= 0) {
+        ++nocc;
+        if (W[u] != 0.0) {
+          const double g = __dsub_rn(W[u], __dmul_rn(t[u], kf));
+          if (g > 0.0 && better(g, c[u], bg, bc)) { bg = g; bc = c[u]; bw = W[u]; }
+        }
+        keys[sl] = -1;
+        vals[sl] = 0.0;
+      }
     }
   }
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1249,6 +1325,38 @@ __global__ void __launch_bounds__(kThreads) nm_accum_smem_kernel(const int32_t* 
   }
 }
 
+// Lanes of a warp holding the same key add their values before one atomic:
+// large communities (the last levels have few) would otherwise serialise on a
+// handful of addresses.  Every lane gets its group's sum; the lowest lane of
+// the group adds it.  Lanes with key < 0 take no part.
+__device__ __forceinline__ void warp_group_add(double* arr, int32_t key, double x) {
+  const unsigned full = 0xffffffffu;
+  const unsigned peers = __match_any_sync(full, key);
+  double sum = 0.0;
+#pragma unroll
+  for (int l = 0; l < 32; ++l) {
+    const double v = __shfl_sync(full, x, l);
+    if ((peers >> l) & 1u) sum += v;
+  }
+  if (key >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&arr[key], sum);
+}
+
+// Kc, Ain of modularity_fp64 for many communities: grid-stride over whole
+// warps, warp-aggregated atomics.
+__global__ void nm_accum_agg_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                    const int32_t* part, double* Kc, double* Ain) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e0 = blockIdx.x * (int64_t)blockDim.x; e0 < E; e0 += stride) {
+    const int64_t e = e0 + threadIdx.x;
+    const bool ok = e < E;
+    const double x = ok ? (double)w[e] : 0.0;
+    const int32_t a = ok ? part[src[e]] : -1, b = ok ? part[dst[e]] : -1;
+    warp_group_add(Kc, a, x);
+    warp_group_add(Kc, b, x);
+    warp_group_add(Ain, (ok && a == b) ? a : -1, 2.0 * x);
+  }
+}
+
 __global__ void nm_accum_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
                                 const int32_t* part, double* Kc, double* Ain) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
@@ -1266,6 +1374,11 @@ __global__ void nm_term_kernel(const double* Kc, const double* Ain, int32_t C, c
     double f = __ddiv_rn(Kc[c], tw);
     t[c] = tw > 0.0 ? __dsub_rn(__ddiv_rn(Ain[c], tw), __dmul_rn(f, f)) : 0.0;
   }
+}
+
+__global__ void iota_kernel(int32_t* x, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = (int32_t)i;
 }
 
 __global__ void compose_kernel(int32_t* composed, const int32_t* part_level, int64_t n) {
@@ -1339,18 +1452,18 @@ static bool build_csr_fast(LevelGraph& g, Arena& a, cudaStream_t s) {
   if (E >= ((int64_t)1 << 32) - 1) return false;
   HiScope hs(a);
   int64_t* rowstart = a.hi_n<int64_t>(V + 1);
-  uint32_t* flags = a.hi_n<uint32_t>(1);
+  unsigned long long* chk = a.hi_n<unsigned long long>(3);   // flags, two fingerprint sums
+  LVG_CUDA(cudaMemsetAsync(chk, 0, 3 * sizeof(unsigned long long), s));
+  list_check_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, g.w, E, (uint32_t*)chk, chk + 1);
+  LVG_LAUNCH();
+  unsigned long long h[3] = {0, 0, 0};
+  LVG_CUDA(cudaMemcpyAsync(h, chk, sizeof h, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  if (h[0] != 0 || h[1] != 0 || h[2] != 0) return false;
   LVG_CUDA(cudaMemsetAsync(rowstart, 0, sizeof(int64_t) * (V + 1), s));
-  LVG_CUDA(cudaMemsetAsync(flags, 0, sizeof(uint32_t), s));
   row_count_kernel<<<grid_for(E, kThreads), kThreads, 0, s>>>(g.src, E, rowstart);
   LVG_LAUNCH();
   scan_i64(rowstart, rowstart, V, a, s);
-  list_check_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, g.w, E, rowstart, flags);
-  LVG_LAUNCH();
-  uint32_t h = 0;
-  LVG_CUDA(cudaMemcpyAsync(&h, flags, sizeof h, cudaMemcpyDeviceToHost, s));
-  LVG_CUDA(cudaStreamSynchronize(s));
-  if (h != 0) return false;
   uint32_t* pos = a.hi_n<uint32_t>(E + 1);
   nonloop_flag_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(g.src, g.dst, E, pos);
   LVG_LAUNCH();
@@ -1688,7 +1801,9 @@ static void set_move_attributes(int block_log) {
   LVG_CUDA(cudaFuncSetAttribute(move_tile_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(TileSmem<double>)));
   size_t smem = ((size_t)1 << block_log) * (sizeof(double) + sizeof(int32_t));
-  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  smem = ((size_t)1 << block_log) * (sizeof(int32_t) + sizeof(int32_t));
+  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<int>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   done_log = block_log;
 }
 
@@ -1746,8 +1861,13 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     Q.list = g.blist + g.bstart[kBBlock];
     Q.n = g.nbucket[kBBlock];
     int lg = g.block_log;
-    size_t smem = ((size_t)1 << lg) * (sizeof(double) + sizeof(int32_t));
-    move_block_kernel<<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg);
+    if (g.int_acc) {
+      size_t smem = ((size_t)1 << lg) * (sizeof(int32_t) + sizeof(int32_t));
+      move_block_kernel<int><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg);
+    } else {
+      size_t smem = ((size_t)1 << lg) * (sizeof(double) + sizeof(int32_t));
+      move_block_kernel<double><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg);
+    }
     LVG_LAUNCH();
   }
   if (g.ntiles > 0) {
@@ -1958,7 +2078,7 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
     nm_accum_smem_kernel<<<sm_grid(E, kThreads), kThreads, smem, s>>>(src, dst, w, E, part, C, Kc, Ain);
     LVG_LAUNCH();
   } else if (E > 0) {
-    nm_accum_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
+    nm_accum_agg_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
     LVG_LAUNCH();
   }
   tree_sum_f64(Kc, C, twoW, a, s);
@@ -2002,6 +2122,12 @@ void modularity_fp64_scratch(const int32_t* src, const int32_t* dst, const float
   nm_term_kernel<<<sm_grid(C, kThreads), kThreads, 0, s>>>(Kc, Ain, C, twoW_q, t);
   LVG_LAUNCH();
   tree(t, twoW_q + 1);
+}
+
+void iota(int32_t* x, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  iota_kernel<<<sm_grid(n, kThreads), kThreads, 0, s>>>(x, n);
+  LVG_LAUNCH();
 }
 
 void compose(int32_t* composed, const int32_t* part_level, int64_t n, cudaStream_t s) {
@@ -2216,13 +2342,21 @@ __global__ void batch_compose_kernel(int32_t* local0, const int32_t* gid0, int64
 __global__ void batch_nm_accum_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
                                       const int32_t* gid0, const int32_t* local0, const int32_t* coff, double* Kc,
                                       double* Ain) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
-    int32_t g = gid0[src[e]];
-    double x = (double)w[e];
-    int32_t a = coff[g] + local0[src[e]], b = coff[g] + local0[dst[e]];
-    atomicAdd(&Kc[a], x);
-    atomicAdd(&Kc[b], x);
-    if (a == b) atomicAdd(&Ain[a], 2.0 * x);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e0 = blockIdx.x * (int64_t)blockDim.x; e0 < E; e0 += stride) {
+    const int64_t e = e0 + threadIdx.x;
+    const bool ok = e < E;
+    double x = 0.0;
+    int32_t a = -1, b = -1;
+    if (ok) {
+      const int32_t g = gid0[src[e]];
+      x = (double)w[e];
+      a = coff[g] + local0[src[e]];
+      b = coff[g] + local0[dst[e]];
+    }
+    warp_group_add(Kc, a, x);
+    warp_group_add(Kc, b, x);
+    warp_group_add(Ain, (ok && a == b) ? a : -1, 2.0 * x);
   }
 }
 

@@ -31,6 +31,9 @@ class LevelInfo:
     q_start: float
     q_level: float
     ms_passes: float
+    ms_build: float = 0.0
+    ms_renumber: float = 0.0
+    ms_induce: float = 0.0
 
 
 @dataclass
@@ -214,7 +217,8 @@ class Louvain:
     def level_info(self, level):
         i = _lib.LvgLevelInfo()
         self._check(self._L.lvg_get_level_info(self._h, int(level), ctypes.byref(i)))
-        return LevelInfo(i.n_vertices, i.n_entries, i.nnz, i.n_comms, i.passes, i.q_start, i.q_level, i.ms_passes)
+        return LevelInfo(i.n_vertices, i.n_entries, i.nnz, i.n_comms, i.passes, i.q_start, i.q_level, i.ms_passes,
+                         i.ms_build, i.ms_renumber, i.ms_induce)
 
     def level_partition(self, level):
         out = np.zeros(self.level_info(level).n_vertices, np.int32)

@@ -212,6 +212,37 @@ def test_unsorted_input_matches_sorted(Louvain, gen):
         np.testing.assert_array_equal(a.partition(), b.partition())
 
 
+@pytest.mark.parametrize("change", ["one_weight", "one_direction", "extra_entry"])
+def test_sorted_but_not_symmetric_takes_the_sorting_build(Louvain, oracle, gen, change):
+    """Sorted lists that are not symmetric (a weight differing between the two
+    directions, an edge listed one way, an entry without its mirror) must not
+    take the sort-free build: the CSR equals the oracle's."""
+    n, s, d, w = gen.sbm(2000, 20, 0.05, 0.002, 1, 3, seed=9)
+    s, d, w = s.copy(), d.copy(), w.copy()
+    e = int(np.flatnonzero(s < d)[len(s) // 5])
+    if change == "one_weight":
+        w[e] += 1.0
+    elif change == "one_direction":
+        keep = np.ones(len(s), bool)
+        keep[e] = False
+        s, d, w = s[keep], d[keep], w[keep]
+    else:
+        u, v = int(s[e]), int(d[e])
+        free = np.setdiff1d(np.arange(n), d[s == u])
+        x = int(free[free > u][0]) if np.any(free > u) else int(free[0])
+        s, d, w = np.append(s, u), np.append(d, x), np.append(w, 2.0)
+        order = np.lexsort((d, s))
+        s, d, w = s[order], d[order], w[order]
+    oc = oracle.Csr(n, s, d, w)
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        csr_equal(lv, oc)
+        res = lv.run()
+        r = oracle.Run(n, s, d, w)
+        np.testing.assert_array_equal(lv.partition(), r.final)
+        assert res.n_levels == len(r.levels)
+
+
 def test_invalid_input_is_an_error(Louvain):
     from louvaingpu_b200 import LvgError
     with Louvain() as lv:
