@@ -108,23 +108,35 @@ constexpr int kRsTile = kRsThreads * kRsItems;  // 2048 keys
 constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kRadix = 256;
 
-__global__ void __launch_bounds__(kRsThreads) rs_hist_kernel(const uint64_t* keys, int64_t n, int shift,
-                                                             uint32_t* hist, int64_t ntiles) {
-  __shared__ uint32_t h[kRsWarps][kRadix];
-  for (int i = threadIdx.x; i < kRsWarps * kRadix; i += kRsThreads) (&h[0][0])[i] = 0;
+// One pass over the keys gives the global histogram of every digit position.
+constexpr int kRsMaxPasses = 8;
+
+__global__ void __launch_bounds__(kRsThreads) rs_upfront_kernel(const uint64_t* keys, int64_t n, int npass,
+                                                                uint32_t* ghist) {
+  __shared__ uint32_t h[kRsMaxPasses][kRadix];
+  for (int i = threadIdx.x; i < kRsMaxPasses * kRadix; i += kRsThreads) (&h[0][0])[i] = 0;
   __syncthreads();
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int64_t base = (int64_t)blockIdx.x * kRsTile + (int64_t)w * (32 * kRsItems);
-#pragma unroll 4
-  for (int j = 0; j < kRsItems; ++j) {
-    int64_t idx = base + j * 32 + lane;
-    if (idx < n) atomicAdd(&h[w][(unsigned)(keys[idx] >> shift) & (kRadix - 1)], 1u);
+  for (int64_t i = blockIdx.x * (int64_t)kRsThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRsThreads) {
+    const uint64_t k = keys[i];
+    for (int p = 0; p < npass; ++p) atomicAdd(&h[p][(unsigned)(k >> (8 * p)) & (kRadix - 1)], 1u);
   }
   __syncthreads();
-  uint32_t c = 0;
-#pragma unroll
-  for (int k = 0; k < kRsWarps; ++k) c += h[k][threadIdx.x];
-  hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = c;
+  for (int p = 0; p < npass; ++p) {
+    const uint32_t c = h[p][threadIdx.x];
+    if (c) atomicAdd(&ghist[p * kRadix + threadIdx.x], c);
+  }
+}
+
+// Exclusive scan of each pass's global histogram (one block, thread = digit).
+__global__ void __launch_bounds__(kRsThreads) rs_gscan_kernel(uint32_t* ghist, int npass) {
+  for (int p = 0; p < npass; ++p) {
+    uint32_t tot;
+    const uint32_t v = ghist[p * kRadix + threadIdx.x];
+    const uint32_t x = block_exclusive_scan<uint32_t>(v, &tot);
+    __syncthreads();
+    ghist[p * kRadix + threadIdx.x] = x;
+    __syncthreads();
+  }
 }
 
 struct RsSmem {
@@ -133,62 +145,99 @@ struct RsSmem {
   uint32_t wc[kRsWarps][kRadix + 1];
   uint32_t dstart[kRadix];
   uint32_t gbase[kRadix];
+  uint32_t tile;
 };
 
-__global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t* kin, const float* vin,
-                                                                uint64_t* kout, float* vout, int64_t n,
-                                                                int shift, const uint32_t* offs,
-                                                                int64_t ntiles) {
+// Look-back words, one per (tile, digit): code in bits 56..63 (2p+1: this
+// tile's count, 2p+2: count of every tile up to this one, for pass p; codes of
+// earlier passes read as "not yet"), count in bits 0..31.
+constexpr int kRsSpinLimit = 1 << 22;
+
+__device__ __forceinline__ void rs_publish(unsigned long long* w, unsigned code, uint32_t count) {
+  atomicExch(w, ((unsigned long long)code << 56) | count);
+}
+
+// One LSD pass: a tile (taken in launch order from a counter) ranks its keys
+// by digit in shared memory, learns the keys of its digits in all earlier
+// tiles by decoupled look-back, and writes its keys out digit run by digit
+// run.  Stable: ranks follow key order inside a tile and tiles in order.
+__global__ void __launch_bounds__(kRsThreads) rs_onesweep_kernel(const uint64_t* kin, const float* vin,
+                                                                 uint64_t* kout, float* vout, int64_t n,
+                                                                 int shift, int pass, const uint32_t* gstart,
+                                                                 unsigned long long* look, uint32_t* counter,
+                                                                 uint32_t* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RsSmem& S = *reinterpret_cast<RsSmem*>(smem_raw);
   const unsigned full = 0xffffffffu;
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) S.tile = atomicAdd(counter, 1u);
   for (int i = threadIdx.x; i < kRsWarps * (kRadix + 1); i += kRsThreads) (&S.wc[0][0])[i] = 0;
   __syncthreads();
-  int64_t tile0 = (int64_t)blockIdx.x * kRsTile;
-  int64_t base = tile0 + (int64_t)w * (32 * kRsItems);
+  const int64_t tile = S.tile;
+  const int64_t tile0 = tile * kRsTile;
+  const int64_t base = tile0 + (int64_t)w * (32 * kRsItems);
   uint64_t k[kRsItems];
   float v[kRsItems];
   uint32_t rank[kRsItems];
   uint16_t dg[kRsItems];
-  unsigned lt = (1u << lane) - 1u;
+  const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
   for (int j = 0; j < kRsItems; ++j) {
-    int64_t idx = base + j * 32 + lane;
-    bool ok = idx < n;
+    const int64_t idx = base + j * 32 + lane;
+    const bool ok = idx < n;
     k[j] = ok ? kin[idx] : 0ull;
     v[j] = ok ? vin[idx] : 0.0f;
-    unsigned d = ok ? (unsigned)(k[j] >> shift) & (kRadix - 1) : (unsigned)kRadix;
+  }
+#pragma unroll
+  for (int j = 0; j < kRsItems; ++j) {
+    const int64_t idx = base + j * 32 + lane;
+    const unsigned d = idx < n ? (unsigned)(k[j] >> shift) & (kRadix - 1) : (unsigned)kRadix;
     dg[j] = (uint16_t)d;
-    unsigned peers = __match_any_sync(full, d);
-    uint32_t before = S.wc[w][d];
+    const unsigned peers = __match_any_sync(full, d);
+    const uint32_t before = S.wc[w][d];
     rank[j] = before + __popc(peers & lt);
     __syncwarp();
     if ((peers & lt) == 0) S.wc[w][d] = before + __popc(peers);
     __syncwarp();
   }
   __syncthreads();
-  // per digit (thread = digit): exclusive prefix over warps, tile count
+  // thread = digit: prefix over warps, tile count, look-back across tiles
+  const int d = threadIdx.x;
   uint32_t cnt = 0;
-  {
-    int d = threadIdx.x;
 #pragma unroll
-    for (int ww = 0; ww < kRsWarps; ++ww) {
-      uint32_t t = S.wc[ww][d];
-      S.wc[ww][d] = cnt;
-      cnt += t;
+  for (int ww = 0; ww < kRsWarps; ++ww) {
+    const uint32_t t = S.wc[ww][d];
+    S.wc[ww][d] = cnt;
+    cnt += t;
+  }
+  const unsigned agg = 2u * (unsigned)pass + 1u, inc = agg + 1u;
+  unsigned long long* mine = look + tile * kRadix + d;
+  uint32_t excl = 0;
+  if (tile == 0) {
+    rs_publish(mine, inc, cnt);
+  } else {
+    rs_publish(mine, agg, cnt);
+    int64_t j = tile - 1;
+    int spins = 0;
+    while (j >= 0) {
+      const unsigned long long x = *reinterpret_cast<volatile unsigned long long*>(look + j * kRadix + d);
+      const unsigned code = (unsigned)(x >> 56);
+      if (code == inc) { excl += (uint32_t)x; break; }
+      if (code == agg) { excl += (uint32_t)x; --j; continue; }
+      if (++spins > kRsSpinLimit) { atomicOr(err, 1u); break; }   // bounded wait: report, never hang
     }
+    rs_publish(mine, inc, excl + cnt);
   }
   uint32_t tot;
-  uint32_t start = block_exclusive_scan<uint32_t>(cnt, &tot);
-  S.dstart[threadIdx.x] = start;
-  S.gbase[threadIdx.x] = offs[(int64_t)threadIdx.x * ntiles + blockIdx.x];
+  const uint32_t start = block_exclusive_scan<uint32_t>(cnt, &tot);
+  S.dstart[d] = start;
+  S.gbase[d] = gstart[d] + excl;
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < kRsItems; ++j) {
-    unsigned d = dg[j];
-    if (d < (unsigned)kRadix) {
-      uint32_t pos = S.dstart[d] + S.wc[w][d] + rank[j];
+    const unsigned dd = dg[j];
+    if (dd < (unsigned)kRadix) {
+      const uint32_t pos = S.dstart[dd] + S.wc[w][dd] + rank[j];
       S.key[pos] = k[j];
       S.val[pos] = v[j];
     }
@@ -197,9 +246,9 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t* 
   int64_t tn = n - tile0;
   if (tn > kRsTile) tn = kRsTile;
   for (int p = threadIdx.x; p < tn; p += kRsThreads) {
-    uint64_t kk = S.key[p];
-    unsigned d = (unsigned)(kk >> shift) & (kRadix - 1);
-    uint32_t o = S.gbase[d] + ((uint32_t)p - S.dstart[d]);
+    const uint64_t kk = S.key[p];
+    const unsigned dd = (unsigned)(kk >> shift) & (kRadix - 1);
+    const uint32_t o = S.gbase[dd] + ((uint32_t)p - S.dstart[dd]);
     kout[o] = kk;
     vout[o] = S.val[p];
   }
@@ -249,25 +298,36 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
   if (n <= 1 || bits <= 0) return 0;
   static std::once_flag attr_once;
   std::call_once(attr_once, [] {
-    LVG_CUDA(cudaFuncSetAttribute(rs_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    LVG_CUDA(cudaFuncSetAttribute(rs_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(RsSmem)));
   });
+  const int npass = (std::min(bits, 64) + 7) / 8;
   HiScope hs(a);
-  int64_t ntiles = (n + kRsTile - 1) / kRsTile;
-  uint32_t* hist = a.hi_n<uint32_t>(kRadix * ntiles + 1);
+  const int64_t ntiles = (n + kRsTile - 1) / kRsTile;
+  unsigned long long* look = a.hi_n<unsigned long long>(ntiles * kRadix);
+  uint32_t* ghist = a.hi_n<uint32_t>(kRsMaxPasses * kRadix + kRsMaxPasses + 1);
+  uint32_t* counters = ghist + kRsMaxPasses * kRadix;
+  uint32_t* err = counters + kRsMaxPasses;
+  LVG_CUDA(cudaMemsetAsync(look, 0, sizeof(unsigned long long) * ntiles * kRadix, s));
+  LVG_CUDA(cudaMemsetAsync(ghist, 0, sizeof(uint32_t) * (kRsMaxPasses * kRadix + kRsMaxPasses + 1), s));
+  const int64_t ublocks = std::min<int64_t>((n + kRsThreads - 1) / kRsThreads, 148 * 8);
+  rs_upfront_kernel<<<(unsigned)ublocks, kRsThreads, 0, s>>>(k0, n, npass, ghist);
+  LVG_LAUNCH();
+  rs_gscan_kernel<<<1, kRsThreads, 0, s>>>(ghist, npass);
+  LVG_LAUNCH();
   int cur = 0;
   uint64_t* K[2] = {k0, k1};
   float* Vv[2] = {v0, v1};
-  for (int shift = 0; shift < bits; shift += 8) {
-    rs_hist_kernel<<<(unsigned)ntiles, kRsThreads, 0, s>>>(K[cur], n, shift, hist, ntiles);
-    LVG_LAUNCH();
-    scan_u32(hist, hist, kRadix * ntiles, a, s);
-    rs_scatter_kernel<<<(unsigned)ntiles, kRsThreads, sizeof(RsSmem), s>>>(K[cur], Vv[cur], K[cur ^ 1],
-                                                                           Vv[cur ^ 1], n, shift, hist,
-                                                                           ntiles);
+  for (int p = 0; p < npass; ++p) {
+    rs_onesweep_kernel<<<(unsigned)ntiles, kRsThreads, sizeof(RsSmem), s>>>(
+        K[cur], Vv[cur], K[cur ^ 1], Vv[cur ^ 1], n, 8 * p, p, ghist + p * kRadix, look, counters + p, err);
     LVG_LAUNCH();
     cur ^= 1;
   }
+  uint32_t h = 0;
+  LVG_CUDA(cudaMemcpyAsync(&h, err, sizeof h, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  if (h) throw Error(LVG_ERR_CUDA, "radix sort look-back did not complete");
   return cur;
 }
 
