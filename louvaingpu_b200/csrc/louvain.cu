@@ -612,40 +612,42 @@ __global__ void __launch_bounds__(kThreads) move_thread_kernel(MoveArgs P, EllAr
 // community gather.  Decisions are the general kernels' bit for bit.
 template <int D>
 __global__ void __launch_bounds__(kThreads) sp_thread_kernel(MoveArgs P, EllArgs L) {
+  // D lanes per vertex: lane s of a segment takes ELL slot s (coalesced row
+  // loads, one gather per lane, all in flight together), then a segment argmax.
   if (P.ctl->done) return;
-  for (int64_t j = blockIdx.x * (int64_t)kThreads + threadIdx.x; j < L.n; j += (int64_t)gridDim.x * kThreads) {
-    int32_t c[D];
-    float w[D];
-    double t[D];
-    const int4* cp = reinterpret_cast<const int4*>(L.col + j * D);
-    const float4* wp = reinterpret_cast<const float4*>(L.w + j * D);
-#pragma unroll
-    for (int q = 0; q < D / 4; ++q) {
-      int4 a = __ldcs(cp + q);
-      float4 b = __ldcs(wp + q);
-      c[4 * q] = a.x; c[4 * q + 1] = a.y; c[4 * q + 2] = a.z; c[4 * q + 3] = a.w;
-      w[4 * q] = b.x; w[4 * q + 1] = b.y; w[4 * q + 2] = b.z; w[4 * q + 3] = b.w;
-    }
-    const VInfo vi = L.info[j];
-    const int32_t i = vi.vid_loop >> 1;
-    const double kf = vi.kfrac;
-#pragma unroll
-    for (int q = 0; q < D; ++q) t[q] = c[q] >= 0 ? P.tot[c[q]] : 0.0;   // independent gathers
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, sl = lane % D;
+  const int64_t per_warp = 32 / D;
+  const int64_t nwarps = (int64_t)gridDim.x * (kThreads / 32);
+  const int64_t ngroups = (L.n + per_warp - 1) / per_warp;
+  for (int64_t grp = blockIdx.x * (int64_t)(kThreads / 32) + (threadIdx.x >> 5); grp < ngroups; grp += nwarps) {
+    const int64_t j = grp * per_warp + lane / D;             // item of this lane's segment
+    const bool ok = j < L.n;
+    const int32_t c = ok ? __ldcs(L.col + j * D + sl) : -1;
+    const float wv = ok ? __ldcs(L.w + j * D + sl) : 0.0f;
+    const double kf = ok ? L.info[j].kfrac : 0.0;
+    const double t = c >= 0 ? P.tot[c] : 0.0;
     double bg = 0.0, bw = 0.0;
     int32_t bc = kNone;
-    int deg = 0;
-#pragma unroll
-    for (int q = 0; q < D; ++q) {
-      if (c[q] >= 0) {
-        ++deg;
-        const double W = (double)w[q];
-        if (W != 0.0) {                                            // OneLevelKernel.cu:303
-          const double g = __dsub_rn(W, __dmul_rn(t[q], kf));      // OneLevelKernel.cu:307-313
-          if (g > 0.0 && better(g, c[q], bg, bc)) { bg = g; bc = c[q]; bw = W; }
-        }
-      }
+    const double W = (double)wv;
+    if (c >= 0 && W != 0.0) {                                       // OneLevelKernel.cu:303
+      const double g = __dsub_rn(W, __dmul_rn(t, kf));              // OneLevelKernel.cu:307-313
+      if (g > 0.0) { bg = g; bc = c; bw = W; }
     }
-    apply_decision_kl(P, i, i, bc, bw, deg + (vi.vid_loop & 1), vi.k, vi.loopw);
+#pragma unroll
+    for (int o = D / 2; o >= 1; o >>= 1) {                          // argmax inside the segment
+      const double g2 = __shfl_xor_sync(full, bg, o);
+      const int32_t c2 = __shfl_xor_sync(full, bc, o);
+      const double w2 = __shfl_xor_sync(full, bw, o);
+      if (better(g2, c2, bg, bc)) { bg = g2; bc = c2; bw = w2; }
+    }
+    const unsigned valid = __ballot_sync(full, c >= 0);
+    if (ok && sl == 0) {
+      const unsigned seg = (D == 32) ? valid : ((valid >> (lane & ~(D - 1))) & ((1u << D) - 1u));
+      const VInfo vi = L.info[j];
+      const int32_t i = vi.vid_loop >> 1;
+      apply_decision_kl(P, i, i, bc, bw, __popc(seg) + (vi.vid_loop & 1), vi.k, vi.loopw);
+    }
   }
 }
 
@@ -785,6 +787,8 @@ constexpr int kTileSlots = 1 << kTileSlotsLog;
 constexpr unsigned long long kEmptyKey = ~0ull;
 static_assert(kTileVtx >= kTileCost / 37 + 1, "tile vertex arrays too small");
 static_assert(kTileCost + kTileMaxDeg + 4 <= (1 << 11) + 8, "tile table load above one half");
+static_assert(kTileCost + kTileMaxDeg + 4 <= 256 * 9, "tile row ids: 9 entries per thread");
+static_assert(kTileVtx < 256, "tile row ids are bytes");
 
 template <typename Acc>
 struct TileSmem {
@@ -802,6 +806,7 @@ struct TileSmem {
   int32_t nseg[kTileVtx];
   int32_t flags[kTileVtx];   // bit0 saw own community, bit1 has self loop
   int32_t nclaimed;
+  uint8_t rowid[kThreads * 9];   // tile vertex of every tile entry
 };
 
 template <typename Acc>
@@ -855,6 +860,18 @@ __global__ void __launch_bounds__(kThreads) move_tile_kernel(MoveArgs P, const i
     if (threadIdx.x < nv) S.rowbeg[threadIdx.x] = pre;
     if (threadIdx.x == 0) S.rowbeg[nv] = ne;
     __syncthreads();
+    {   // row ids: one search per run of 9 entries, then a forward walk
+      const int q0 = threadIdx.x * 9;
+      if (q0 < ne) {
+        int j = tile_find(S.rowbeg, nv, q0);
+        const int q1 = min(q0 + 9, ne);
+        for (int q = q0; q < q1; ++q) {
+          while (S.rowbeg[j + 1] <= q) ++j;
+          S.rowid[q] = (uint8_t)j;
+        }
+      }
+    }
+    __syncthreads();
     for (int q0 = threadIdx.x; q0 < ne; q0 += 4 * kThreads) {
       int jj[4];
       int32_t cc[4];
@@ -864,7 +881,7 @@ __global__ void __launch_bounds__(kThreads) move_tile_kernel(MoveArgs P, const i
         int q = q0 + u * kThreads;
         jj[u] = -1;
         if (q < ne) {
-          int j = tile_find(S.rowbeg, nv, q);
+          int j = S.rowid[q];
           int64_t e = S.beg[j] + (q - S.rowbeg[j]);
           jj[u] = j;
           cc[u] = __ldcs(P.col + e);
@@ -1898,7 +1915,8 @@ static void launch_sp_thread(const LevelGraph& g, MoveArgs P, int bucket, cudaSt
   L.w = g.ell_w + g.ell_base[bucket];
   L.list = g.blist + g.bstart[bucket];
   L.info = g.ell_info + (g.bstart[bucket] - g.bstart[kB4]);
-  int64_t blocks = std::min<int64_t>((L.n + kThreads - 1) / kThreads, (int64_t)sm_count() * 8);
+  const int64_t vper_block = (int64_t)kThreads / D;
+  int64_t blocks = std::min<int64_t>((L.n + vper_block - 1) / vper_block, (int64_t)sm_count() * 16);
   sp_thread_kernel<D><<<(unsigned)std::max<int64_t>(blocks, 1), kThreads, 0, s>>>(P, L);
   LVG_LAUNCH();
 }
