@@ -235,12 +235,14 @@ def run_ours(args, world, rank, local, pg):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     passes_total, move_ms, move_passes = 0, 0.0, 0
+    per_pass = []
     for _ in range(args.steps):
         q, p = lv.one_level(q0)
         passes_total += p
         ms, mp = lv.move_stats()
         move_ms += ms
         move_passes += mp
+        per_pass.append(lv.move_pass_times().tolist())
     e1.record(stream)
     torch.cuda.synchronize()
     launches = kernel_launches() - l0
@@ -259,7 +261,9 @@ def run_ours(args, world, rank, local, pg):
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_kind, "traffic": profiled_traffic(args.workload),
             "kernel": "move kernels of one pass (all degree buckets)", "algorithmic_bytes": b_pass,
-            "move_ms_per_pass": t_move * 1e3}
+            "move_ms_per_pass": t_move * 1e3,
+            "move_ms_by_pass": [round(float(np.median([x[k] for x in per_pass if len(x) > k])), 4)
+                                for k in range(max(len(x) for x in per_pass))]}
     del lv, ds, dd, dw
     torch.cuda.empty_cache()
     # ---------------------------------------------------------------- e2e

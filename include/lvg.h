@@ -164,6 +164,11 @@ lvg_status lvg_move_decide(lvg_ctx* ctx, int32_t* next, int32_t* cand);
  * per-pass breakdown when `ms` is non-NULL (cap entries). */
 lvg_status lvg_last_pass_times(const lvg_ctx* ctx, float* ms, int32_t cap, int32_t* n_passes);
 
+/* Device time of the move kernels of each pass of the last one-level phase
+ * (CUDA events around the move launches; the first pass runs the singleton
+ * kernels).  Fills up to cap values; *n = number of passes. */
+lvg_status lvg_move_pass_times(const lvg_ctx* ctx, float* ms, int32_t cap, int32_t* n);
+
 /* Device time of the move kernels (all degree buckets of a pass, the hot
  * path's dominant work) summed over the passes of the last lvg_one_level /
  * lvg_run, and the number of passes it covers. */

@@ -109,6 +109,7 @@ SIGNATURES = {
     "lvg_move_decide": (i32, [P, P, P]),
     "lvg_last_pass_times": (i32, [P, P, i32, ctypes.POINTER(i32)]),
     "lvg_move_stats": (i32, [P, ctypes.POINTER(dbl), ctypes.POINTER(i64)]),
+    "lvg_move_pass_times": (i32, [P, P, i32, ctypes.POINTER(i32)]),
     "lvg_kernel_launches": (i32, [ctypes.POINTER(i64)]),
     "lvg_memory": (i32, [P, ctypes.POINTER(i64), ctypes.POINTER(i64)]),
     "lvg_batch_run": (i32, [P, P, P, P, P, P, i32, P, P, P, P, P]),

@@ -75,6 +75,7 @@ struct lvg_ctx {
   size_t window_max = 0;
   double move_ms = 0.0;
   int64_t move_passes = 0;
+  std::vector<float> move_pass_ms;  // move kernels of each pass of the last one-level phase
 };
 
 namespace {
@@ -295,8 +296,12 @@ void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int
   c->pass_ms.push_back(elapsed(c->ev0, c->ev1));
   c->move_ms = 0.0;
   c->move_passes = h.passes;
-  for (int p = 0; p < h.passes && 2 * (size_t)p + 1 < c->mev.size(); ++p)
-    c->move_ms += elapsed(c->mev[2 * p], c->mev[2 * p + 1]);
+  c->move_pass_ms.clear();
+  for (int p = 0; p < h.passes && 2 * (size_t)p + 1 < c->mev.size(); ++p) {
+    const float ms = elapsed(c->mev[2 * p], c->mev[2 * p + 1]);
+    c->move_pass_ms.push_back(ms);
+    c->move_ms += ms;
+  }
   if (q_out) *q_out = h.q_ret;
   if (passes_out) *passes_out = h.passes;
   if (status_out) *status_out = h.status;
@@ -766,6 +771,15 @@ lvg_status lvg_last_pass_times(const lvg_ctx* c, float* ms, int32_t cap, int32_t
   int32_t k = (int32_t)c->pass_ms.size();
   if (ms)
     for (int32_t i = 0; i < k && i < cap; ++i) ms[i] = c->pass_ms[i];
+  if (n) *n = k;
+  return LVG_OK;
+}
+
+lvg_status lvg_move_pass_times(const lvg_ctx* c, float* ms, int32_t cap, int32_t* n) {
+  if (!c) return LVG_ERR_INVALID_ARG;
+  const int32_t k = (int32_t)c->move_pass_ms.size();
+  if (ms)
+    for (int32_t i = 0; i < k && i < cap; ++i) ms[i] = c->move_pass_ms[i];
   if (n) *n = k;
   return LVG_OK;
 }

@@ -103,8 +103,8 @@ void finish_impl(const double* p, int64_t n, double* d_out, Arena& a, cudaStream
 
 // ---------------------------------------------------------------------------
 constexpr int kRsThreads = 256;
-constexpr int kRsItems = 8;
-constexpr int kRsTile = kRsThreads * kRsItems;  // 2048 keys
+constexpr int kRsItems = 16;
+constexpr int kRsTile = kRsThreads * kRsItems;  // 4096 keys
 constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kRadix = 256;
 

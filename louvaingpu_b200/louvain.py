@@ -280,6 +280,14 @@ class Louvain:
         self._check(self._L.lvg_last_pass_times(self._h, _p(out), n.value, ctypes.byref(n)))
         return out[:n.value]
 
+    def move_pass_times(self):
+        """Device ms of the move kernels of each pass of the last one-level phase."""
+        n = ctypes.c_int32()
+        self._check(self._L.lvg_move_pass_times(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), np.float32)
+        self._check(self._L.lvg_move_pass_times(self._h, _p(out), n.value, ctypes.byref(n)))
+        return out[:n.value]
+
     def move_stats(self):
         """(device ms of the move kernels, passes) of the last one-level phase(s)."""
         ms, n = ctypes.c_double(), ctypes.c_int64()
