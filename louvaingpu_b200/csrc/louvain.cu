@@ -411,6 +411,27 @@ __device__ __forceinline__ bool table_insert(int32_t* keys, Acc* vals, int logT,
   return false;
 }
 
+// Packed (community << 32 | integer sum) slots, all ones when empty: one
+// 64-bit atomic per entry (the add cannot carry into the key: integral
+// weights keep a sum below 2^30).
+constexpr unsigned long long kPackedEmpty = ~0ull;
+__device__ __forceinline__ bool packed_insert(unsigned long long* t, int logT, int32_t c, uint32_t w) {
+  const uint32_t T = 1u << logT;
+  uint32_t h = hash_c(c, logT);
+  for (uint32_t p = 0; p < T; ++p) {
+    const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(t + h);
+    const uint32_t k = (uint32_t)(cur >> 32);
+    if (k == (uint32_t)c) { atomicAdd(t + h, (unsigned long long)w); return true; }
+    if (cur == kPackedEmpty) {
+      const unsigned long long prev = atomicCAS(t + h, kPackedEmpty, ((unsigned long long)(uint32_t)c << 32) | w);
+      if (prev == kPackedEmpty) return true;
+      if ((uint32_t)(prev >> 32) == (uint32_t)c) { atomicAdd(t + h, (unsigned long long)w); return true; }
+    }
+    h = (h + 1) & (T - 1);
+  }
+  return false;
+}
+
 // Entries [e0 + u*stride) of a row, u < 4: columns and weights first, then
 // the four community gathers, so that each thread keeps several loads in
 // flight; kNone marks entries past `end`.
@@ -992,6 +1013,7 @@ struct HubArgs {
   uint32_t* sawown;
 };
 
+template <bool PACKED>
 __global__ void __launch_bounds__(kThreads) hub_insert_kernel(MoveArgs P, HubArgs H) {
   if (P.ctl->done) return;
   int32_t h = H.chunk_hub[blockIdx.x];
@@ -1001,6 +1023,7 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(MoveArgs P, HubArg
   int64_t end = min(beg + (int64_t)kHubChunk, P.off[i + 1]);
   int32_t* keys = H.keys + H.toff[h];
   double* vals = H.vals + H.toff[h];
+  unsigned long long* packed = reinterpret_cast<unsigned long long*>(vals);
   int logT = H.tlog[h];
   bool sawown = false, overflow = false;
   for (int64_t e0 = beg + threadIdx.x; e0 < end; e0 += kUnroll * kThreads) {
@@ -1011,7 +1034,9 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(MoveArgs P, HubArg
     for (int u = 0; u < kUnroll; ++u) {
       if (c[u] != kNone) {
         sawown |= (c[u] == own);
-        if (!table_insert<double>(keys, vals, logT, c[u], (double)wv[u])) overflow = true;
+        const bool ok = PACKED ? packed_insert(packed, logT, c[u], (uint32_t)wv[u])
+                               : table_insert<double>(keys, vals, logT, c[u], (double)wv[u]);
+        if (!ok) overflow = true;
       }
     }
   }
@@ -1024,6 +1049,7 @@ __global__ void __launch_bounds__(kThreads) hub_insert_kernel(MoveArgs P, HubArg
 // in order and decides.
 constexpr int kHubSeg = 1024;
 
+template <bool PACKED>
 __global__ void __launch_bounds__(kThreads) hub_scan_kernel(MoveArgs P, HubArgs H, const int32_t* seg_hub,
                                                             const int64_t* seg_beg, HubPartial* part) {
   __shared__ double rg[kThreads / 32], rw[kThreads / 32];
@@ -1036,6 +1062,7 @@ __global__ void __launch_bounds__(kThreads) hub_scan_kernel(MoveArgs P, HubArgs 
   int64_t b1 = min(b0 + (int64_t)kHubSeg, T);
   int32_t* keys = H.keys + H.toff[h];
   double* vals = H.vals + H.toff[h];
+  unsigned long long* packed = reinterpret_cast<unsigned long long*>(vals);
   double kf = P.kfrac[i];
   double bg = 0.0, bw = 0.0;
   int32_t bc = kNone;
@@ -1046,8 +1073,14 @@ __global__ void __launch_bounds__(kThreads) hub_scan_kernel(MoveArgs P, HubArgs 
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
       const int64_t sl = s0 + u * kThreads;
-      c[u] = sl < b1 ? keys[sl] : -1;
-      W[u] = c[u] >= 0 ? vals[sl] : 0.0;
+      if (PACKED) {
+        const unsigned long long x = sl < b1 ? packed[sl] : kPackedEmpty;
+        c[u] = x == kPackedEmpty ? -1 : (int32_t)(uint32_t)(x >> 32);
+        W[u] = c[u] >= 0 ? (double)(uint32_t)x : 0.0;
+      } else {
+        c[u] = sl < b1 ? keys[sl] : -1;
+        W[u] = c[u] >= 0 ? vals[sl] : 0.0;
+      }
     }
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) t[u] = (c[u] >= 0 && W[u] != 0.0) ? P.tot[c[u]] : 0.0;
@@ -1060,8 +1093,12 @@ __global__ void __launch_bounds__(kThreads) hub_scan_kernel(MoveArgs P, HubArgs 
           const double g = __dsub_rn(W[u], __dmul_rn(t[u], kf));
           if (g > 0.0 && better(g, c[u], bg, bc)) { bg = g; bc = c[u]; bw = W[u]; }
         }
-        keys[sl] = -1;
-        vals[sl] = 0.0;
+        if (PACKED) {
+          packed[sl] = kPackedEmpty;
+        } else {
+          keys[sl] = -1;
+          vals[sl] = 0.0;
+        }
       }
     }
   }
@@ -1710,7 +1747,8 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
     LVG_CUDA(cudaMemcpyAsync(g.chunk_hub, chub.data(), sizeof(int32_t) * g.nchunk, cudaMemcpyHostToDevice, s));
     LVG_CUDA(cudaMemcpyAsync(g.chunk_beg, cbeg.data(), sizeof(int64_t) * g.nchunk, cudaMemcpyHostToDevice, s));
     LVG_CUDA(cudaMemsetAsync(g.hub_keys, 0xff, sizeof(int32_t) * slots, s));
-    LVG_CUDA(cudaMemsetAsync(g.hub_vals, 0, sizeof(double) * slots, s));
+    // integral weights: hub_vals holds packed (community, sum) slots, empty = all ones
+    LVG_CUDA(cudaMemsetAsync(g.hub_vals, g.int_acc ? 0xff : 0, sizeof(double) * slots, s));
     LVG_CUDA(cudaMemsetAsync(g.hub_sawown, 0, sizeof(uint32_t) * nhub, s));
     LVG_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
   }
@@ -1866,9 +1904,15 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     H.chunk_hub = g.chunk_hub; H.chunk_beg = g.chunk_beg;
     H.toff = g.hub_toff; H.tlog = g.hub_tlog;
     H.keys = g.hub_keys; H.vals = g.hub_vals; H.sawown = g.hub_sawown;
-    hub_insert_kernel<<<(unsigned)g.nchunk, kThreads, 0, sh>>>(P, H);
-    LVG_LAUNCH();
-    hub_scan_kernel<<<(unsigned)g.nseg, kThreads, 0, sh>>>(P, H, g.seg_hub, g.seg_beg, g.hub_part);
+    if (g.int_acc) {
+      hub_insert_kernel<true><<<(unsigned)g.nchunk, kThreads, 0, sh>>>(P, H);
+      LVG_LAUNCH();
+      hub_scan_kernel<true><<<(unsigned)g.nseg, kThreads, 0, sh>>>(P, H, g.seg_hub, g.seg_beg, g.hub_part);
+    } else {
+      hub_insert_kernel<false><<<(unsigned)g.nchunk, kThreads, 0, sh>>>(P, H);
+      LVG_LAUNCH();
+      hub_scan_kernel<false><<<(unsigned)g.nseg, kThreads, 0, sh>>>(P, H, g.seg_hub, g.seg_beg, g.hub_part);
+    }
     LVG_LAUNCH();
     hub_decide_kernel<<<grid_for(nhub, 128), 128, 0, sh>>>(P, H, g.hub_seg0, g.hub_part, nhub);
     LVG_LAUNCH();
