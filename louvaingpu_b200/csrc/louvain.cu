@@ -972,6 +972,164 @@ __global__ void __launch_bounds__(kThreads) move_tile_kernel(MoveArgs P, const i
   if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
 }
 
+struct TilePackedSmem {
+  unsigned long long slot[kTileSlots];
+  uint16_t claimed[kTileSlots];
+  int64_t beg[kTileVtx];
+  double kf[kTileVtx];
+  double bestw[kTileVtx];
+  unsigned long long bestg[kTileVtx];
+  int32_t vid[kTileVtx];
+  int32_t own[kTileVtx];
+  int32_t rowbeg[kTileVtx + 1];
+  int32_t bestc[kTileVtx];
+  int32_t nseg[kTileVtx];
+  int32_t flags[kTileVtx];
+  int32_t nclaimed;
+  uint8_t rowid[kThreads * 9];
+};
+constexpr int kTilePackedMaxComm = 1 << 26;
+
+__device__ __forceinline__ void tile_packed_insert(TilePackedSmem& S, uint32_t key, uint32_t w, bool& overflow) {
+  uint32_t h = (uint32_t)(((unsigned long long)key * 0x9E3779B97F4A7C15ull) >> (64 - kTileSlotsLog));
+  for (int p = 0; p < kTileSlots; ++p) {
+    const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&S.slot[h]);
+    if ((uint32_t)(cur >> 32) == key) { atomicAdd(&S.slot[h], (unsigned long long)w); return; }
+    if (cur == kPackedEmpty) {
+      const unsigned long long prev = atomicCAS(&S.slot[h], kPackedEmpty, ((unsigned long long)key << 32) | w);
+      if (prev == kPackedEmpty) { S.claimed[atomicAdd(&S.nclaimed, 1)] = (uint16_t)h; return; }
+      if ((uint32_t)(prev >> 32) == key) { atomicAdd(&S.slot[h], (unsigned long long)w); return; }
+    }
+    h = (h + 1) & (kTileSlots - 1);
+  }
+  overflow = true;
+}
+
+// The tile kernel with packed slots ((j << 26 | c) << 32 | integer sum, all
+// ones when empty; j < 48, so no key is all ones): one shared atomic per
+// entry and a smaller table.  Integral weights, community ids below 2^26.
+__global__ void __launch_bounds__(kThreads) move_tile_packed_kernel(MoveArgs P, const int32_t* tile_start,
+                                                                    int64_t ntiles) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  TilePackedSmem& S = *reinterpret_cast<TilePackedSmem*>(smem);
+  if (P.ctl->done) return;
+  for (int sl = threadIdx.x; sl < kTileSlots; sl += kThreads) S.slot[sl] = kPackedEmpty;
+  if (threadIdx.x == 0) S.nclaimed = 0;
+  bool overflow = false;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int vb = tile_start[t];
+    const int nv = tile_start[t + 1] - vb;
+    int deg = 0;
+    if (threadIdx.x < nv) {
+      int32_t i = P.list[vb + threadIdx.x];
+      int64_t b = P.off[i];
+      deg = (int)(P.off[i + 1] - b);
+      S.vid[threadIdx.x] = i;
+      S.beg[threadIdx.x] = b;
+      S.own[threadIdx.x] = P.comm[i];
+      S.kf[threadIdx.x] = P.kfrac[i];
+      S.flags[threadIdx.x] = P.has_loop[i] ? 2 : 0;
+      S.bestg[threadIdx.x] = 0ull;
+      S.bestc[threadIdx.x] = kNone;
+      S.nseg[threadIdx.x] = 0;
+    }
+    int ne;
+    int pre = block_exclusive_scan256<int>(deg, &ne);
+    if (threadIdx.x < nv) S.rowbeg[threadIdx.x] = pre;
+    if (threadIdx.x == 0) S.rowbeg[nv] = ne;
+    __syncthreads();
+    {   // row ids: one search per run of 9 entries, then a forward walk
+      const int q0 = threadIdx.x * 9;
+      if (q0 < ne) {
+        int j = tile_find(S.rowbeg, nv, q0);
+        const int q1 = min(q0 + 9, ne);
+        for (int q = q0; q < q1; ++q) {
+          while (S.rowbeg[j + 1] <= q) ++j;
+          S.rowid[q] = (uint8_t)j;
+        }
+      }
+    }
+    __syncthreads();
+    for (int q0 = threadIdx.x; q0 < ne; q0 += 4 * kThreads) {
+      int jj[4];
+      int32_t cc[4];
+      float ww[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        int q = q0 + u * kThreads;
+        jj[u] = -1;
+        if (q < ne) {
+          int j = S.rowid[q];
+          int64_t e = S.beg[j] + (q - S.rowbeg[j]);
+          jj[u] = j;
+          cc[u] = __ldcs(P.col + e);
+          ww[u] = __ldcs(P.cw + e);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (jj[u] >= 0) cc[u] = P.comm[cc[u]];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (jj[u] >= 0) {
+          int j = jj[u];
+          if (cc[u] == S.own[j]) atomicOr(&S.flags[j], 1);
+          tile_packed_insert(S, ((uint32_t)j << 26) | (uint32_t)cc[u], (uint32_t)ww[u], overflow);
+        }
+      }
+    }
+    __syncthreads();
+    const int nc = S.nclaimed;
+    for (int x = threadIdx.x; x < nc; x += kThreads) {       // count, best gain bits
+      int sl = S.claimed[x];
+      const unsigned long long sv = S.slot[sl];
+      const uint32_t key = (uint32_t)(sv >> 32);
+      int j = (int)(key >> 26);
+      int32_t c = (int32_t)(key & ((1u << 26) - 1u));
+      atomicAdd(&S.nseg[j], 1);
+      double W = (double)(uint32_t)sv;
+      if (W != 0.0) {
+        double g = __dsub_rn(W, __dmul_rn(P.tot[c], S.kf[j]));
+        if (g > 0.0) atomicMax(&S.bestg[j], (unsigned long long)__double_as_longlong(g));
+      }
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < nc; x += kThreads) {       // smallest community among the best gains
+      int sl = S.claimed[x];
+      const unsigned long long sv = S.slot[sl];
+      const uint32_t key = (uint32_t)(sv >> 32);
+      int j = (int)(key >> 26);
+      int32_t c = (int32_t)(key & ((1u << 26) - 1u));
+      double W = (double)(uint32_t)sv;
+      if (W != 0.0 && S.bestg[j] != 0ull) {
+        double g = __dsub_rn(W, __dmul_rn(P.tot[c], S.kf[j]));
+        if ((unsigned long long)__double_as_longlong(g) == S.bestg[j]) atomicMin(&S.bestc[j], c);
+      }
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < nc; x += kThreads) {       // weight to the winner; clear the table
+      int sl = S.claimed[x];
+      const unsigned long long sv = S.slot[sl];
+      const uint32_t key = (uint32_t)(sv >> 32);
+      int j = (int)(key >> 26);
+      int32_t c = (int32_t)(key & ((1u << 26) - 1u));
+      if (c == S.bestc[j]) S.bestw[j] = (double)(uint32_t)sv;
+      S.slot[sl] = kPackedEmpty;
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+      int j = threadIdx.x;
+      int f = S.flags[j];
+      int32_t nseg = S.nseg[j] + (((f & 2) && !(f & 1)) ? 1 : 0);
+      int32_t bc = S.bestc[j];
+      apply_decision(P, S.vid[j], S.own[j], bc, bc == kNone ? 0.0 : S.bestw[j], nseg);
+    }
+    if (threadIdx.x == 0) S.nclaimed = 0;
+    __syncthreads();
+  }
+  if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
+}
+
 // Tile boundaries: vertex j of the tile bucket belongs to tile
 // floor(cumcost_j / kTileCost), cost = degree + 4, so a tile holds at most
 // kTileCost / 37 + 1 vertices and kTileCost + kTileMaxDeg + 4 entries.
@@ -1855,6 +2013,8 @@ static void set_move_attributes(int block_log) {
                                 (int)sizeof(TileSmem<int>)));
   LVG_CUDA(cudaFuncSetAttribute(move_tile_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(TileSmem<double>)));
+  LVG_CUDA(cudaFuncSetAttribute(move_tile_packed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TilePackedSmem)));
   size_t smem = ((size_t)1 << block_log) * (sizeof(double) + sizeof(int32_t));
   LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   smem = ((size_t)1 << block_log) * (sizeof(int32_t) + sizeof(int32_t));
@@ -1935,8 +2095,18 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     MoveArgs Q = P;
     Q.list = g.blist + g.bstart[kBTile];
     Q.n = g.nbucket[kBTile];
-    if (g.int_acc) launch_tiles<int>(g, Q, st2);
-    else launch_tiles<double>(g, Q, st2);
+    if (g.int_acc && g.V <= kTilePackedMaxComm) {
+      const size_t smem = sizeof(TilePackedSmem);
+      const int per_sm = std::max(1, std::min(8, (int)((227u * 1024u) / (smem + 1024))));
+      const int64_t grid = std::min<int64_t>(g.ntiles, (int64_t)sm_count() * per_sm);
+      move_tile_packed_kernel<<<(unsigned)std::max<int64_t>(grid, 1), kThreads, smem, st2>>>(Q, g.tile_start,
+                                                                                            g.ntiles);
+      LVG_LAUNCH();
+    } else if (g.int_acc) {
+      launch_tiles<int>(g, Q, st2);
+    } else {
+      launch_tiles<double>(g, Q, st2);
+    }
   }
   launch_thread<32>(g, P, kB32, s);
   launch_thread<16>(g, P, kB16, s);
