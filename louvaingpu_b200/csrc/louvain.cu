@@ -452,7 +452,7 @@ __device__ __forceinline__ void gather4(const MoveArgs& P, int64_t e0, int64_t s
 // Block per vertex (degree up to block_max), table in dynamic shared memory;
 // int32 sums when the weights are integral (exact, half the table bytes).
 template <typename Acc>
-__global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int maxLog) {
+__global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int maxLog, int64_t dlo, int64_t dhi) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double rg[kThreads / 32], rw[kThreads / 32];
   __shared__ int32_t rc[kThreads / 32], rn[kThreads / 32], rs[kThreads / 32];
@@ -466,8 +466,9 @@ __global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int ma
   bool overflow = false;
   for (int64_t item = blockIdx.x; item < P.n; item += gridDim.x) {
     int32_t i = P.list[item];
-    int32_t own = P.comm[i];
     int64_t beg = P.off[i], end = P.off[i + 1];
+    if (end - beg <= dlo || end - beg > dhi) continue;   // another launch takes this degree
+    int32_t own = P.comm[i];
     int logT = min(maxLog, max(5, ceil_log2(2 * (end - beg))));
     int T = 1 << logT;
     bool sawown = false;
@@ -676,6 +677,8 @@ __global__ void __launch_bounds__(kThreads) sp_thread_kernel(MoveArgs P, EllArgs
 // chunk is decided by its warp; longer rows leave a partial per chunk for
 // sp_combine_kernel.
 constexpr int kSpChunk = 512;
+constexpr int kSpUnroll = 4;     // entries per lane in flight
+constexpr bool kBlockSplit = true;
 
 __global__ void __launch_bounds__(kThreads) sp_chunk_kernel(MoveArgs P, const int2* chunks, int64_t nch,
                                                             HubPartial* part) {
@@ -691,20 +694,20 @@ __global__ void __launch_bounds__(kThreads) sp_chunk_kernel(MoveArgs P, const in
     const double kf = P.kfrac[i];
     double bg = 0.0, bw = 0.0;
     int32_t bc = kNone;
-    for (int64_t e0 = beg; e0 < end; e0 += 4 * 32) {
-      int32_t c[4];
-      float w[4];
-      double t[4];
+    for (int64_t e0 = beg; e0 < end; e0 += kSpUnroll * 32) {
+      int32_t c[kSpUnroll];
+      float w[kSpUnroll];
+      double t[kSpUnroll];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kSpUnroll; ++u) {
         const int64_t e = e0 + u * 32 + lane;
         c[u] = e < end ? __ldcs(P.col + e) : kNone;
         w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) t[u] = c[u] != kNone ? P.tot[c[u]] : 0.0;
+      for (int u = 0; u < kSpUnroll; ++u) t[u] = c[u] != kNone ? P.tot[c[u]] : 0.0;
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kSpUnroll; ++u) {
         const double W = (double)w[u];
         if (c[u] != kNone && W != 0.0) {
           const double g = __dsub_rn(W, __dmul_rn(t[u], kf));
@@ -2083,11 +2086,19 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     Q.n = g.nbucket[kBBlock];
     int lg = g.block_log;
     if (g.int_acc) {
+      // two launches when the table is large: degrees up to 2^(lg-2) get half
+      // the table, so twice the blocks fit on an SM
+      int64_t split = kBlockSplit && lg >= 12 ? ((int64_t)1 << (lg - 2)) : 0;
+      if (split > 0) {
+        size_t smem = ((size_t)1 << (lg - 1)) * (sizeof(int32_t) + sizeof(int32_t));
+        move_block_kernel<int><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg - 1, 0, split);
+        LVG_LAUNCH();
+      }
       size_t smem = ((size_t)1 << lg) * (sizeof(int32_t) + sizeof(int32_t));
-      move_block_kernel<int><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg);
+      move_block_kernel<int><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg, split, INT64_MAX);
     } else {
       size_t smem = ((size_t)1 << lg) * (sizeof(double) + sizeof(int32_t));
-      move_block_kernel<double><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg);
+      move_block_kernel<double><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg, 0, INT64_MAX);
     }
     LVG_LAUNCH();
   }
