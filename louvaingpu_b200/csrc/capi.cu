@@ -65,7 +65,6 @@ struct lvg_ctx {
   std::vector<float> pass_ms;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t pev[6] = {};        // phase timing: build, renumber, induce (start, end)
-  float build_ms = 0.0f;          // build of the current level
   SideStreams side{};
   bool have_side = false;
   std::vector<cudaEvent_t> mev;   // move-phase events, two per pass
@@ -158,9 +157,7 @@ void prepare_level(lvg_ctx* c) {
   build_level(c->g, c->tune, c->arena, c->stream);
   alloc_state(c->g, c->st, c->arena);
   init_state(c->g, c->st, 0.0, c->cfg.pass_min_gain, c->cfg.max_passes, c->arena, c->stream);
-  LVG_CUDA(cudaEventRecord(c->pev[1], c->stream));
-  LVG_CUDA(cudaEventSynchronize(c->pev[1]));
-  c->build_ms = elapsed(c->pev[0], c->pev[1]);
+  LVG_CUDA(cudaEventRecord(c->pev[1], c->stream));   // read once the stream has synchronised
   c->have_state = true;
   c->renumbered = false;
 }
@@ -256,8 +253,10 @@ void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int
   cudaStream_t s = c->stream;
   init_state(c->g, c->st, lower, c->cfg.pass_min_gain, c->cfg.max_passes, c->arena, s);
   L2Window l2(c, c->st);
+  // The first pass runs the singleton kernels and a level usually stops at
+  // its second pass, so the hashing pass is captured only when a third pass
+  // is launched.
   const bool use_graphs = c->cfg.use_graphs != 0;
-  if (use_graphs) ensure_graphs(c);
   PassCtl h;
   const int chunk = c->cfg.passes_per_sync > 0 ? c->cfg.passes_per_sync : 4;
   c->pass_ms.clear();
@@ -272,11 +271,13 @@ void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int
         c->mev.push_back(ev);
       }
       LVG_CUDA(cudaEventRecord(c->mev[e], s));
+      const bool graph = use_graphs && launched >= 2;
+      if (graph) ensure_graphs(c);
       if (launched == 0) launch_moves_singleton(c->g, c->st, s, &c->side);   // state is singletons
-      else if (use_graphs) LVG_CUDA(cudaGraphLaunch(c->g_moves, s));
+      else if (graph) LVG_CUDA(cudaGraphLaunch(c->g_moves, s));
       else launch_moves(c->g, c->st, s, &c->side);
       LVG_CUDA(cudaEventRecord(c->mev[e + 1], s));
-      if (use_graphs) LVG_CUDA(cudaGraphLaunch(c->g_commit, s));
+      if (graph) LVG_CUDA(cudaGraphLaunch(c->g_commit, s));
       else launch_commit(c->g, c->st, s);
       ++launched;
     }
@@ -323,7 +324,6 @@ int32_t renumber_level(lvg_ctx* c) {
   int32_t C = renumber(c->g, c->st.comm, part, c->arena, c->stream);
   compose(c->composed, part, c->V0, c->stream);    // partitionAtLevel (LouvainCPP.cpp:82-106)
   LVG_CUDA(cudaEventRecord(c->pev[3], c->stream));
-  LVG_CUDA(cudaEventSynchronize(c->pev[3]));
   c->d_part_cur = part;
   c->C_cur = C;
   c->renumbered = true;
@@ -335,8 +335,7 @@ int32_t renumber_level(lvg_ctx* c) {
   r.info.n_entries = c->g.E;
   r.info.nnz = c->g.nnz;
   r.info.n_comms = C;
-  r.info.ms_build = c->build_ms;
-  r.info.ms_renumber = elapsed(c->pev[2], c->pev[3]);
+  r.info.ms_build = elapsed(c->pev[0], c->pev[1]);   // complete: renumber synchronised the stream
   c->levels.push_back(r);
   return C;
 }
@@ -360,7 +359,10 @@ void induce_level(lvg_ctx* c) {
   }
   LVG_CUDA(cudaEventRecord(c->pev[5], c->stream));
   sync(c);
-  if (!c->levels.empty()) c->levels.back().info.ms_induce = elapsed(c->pev[4], c->pev[5]);
+  if (!c->levels.empty()) {
+    c->levels.back().info.ms_renumber = elapsed(c->pev[2], c->pev[3]);
+    c->levels.back().info.ms_induce = elapsed(c->pev[4], c->pev[5]);
+  }
   c->arena.hi = c->run_hi;
   int32_t C = c->C_cur;
   c->g = LevelGraph();
@@ -406,7 +408,7 @@ lvg_status lvg_config_default(lvg_config* cfg) {
   cfg->arena_bytes = 0;
   cfg->tile_max_degree = 512;
   cfg->block_max_degree = 4096;
-  cfg->passes_per_sync = 4;
+  cfg->passes_per_sync = 2;   // a level of this method stops at its second pass
   cfg->use_graphs = 1;
   cfg->l2_persist = 1;
   return LVG_OK;
@@ -611,6 +613,8 @@ lvg_status lvg_run(lvg_ctx* c, lvg_result* res) {
       res->q_final = modularity_fp64(c->src0, c->dst0, c->w0, c->E0, std::max(c->C_cur, 1), c->composed,
                                      c->arena, c->stream);
     }
+    sync(c);
+    if (!c->levels.empty()) c->levels.back().info.ms_renumber = elapsed(c->pev[2], c->pev[3]);
   });
   if (s == LVG_OK && run_status != 0) return fail(c, (lvg_status)run_status, "cap reached before convergence");
   return s;

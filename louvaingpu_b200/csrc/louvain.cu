@@ -436,8 +436,8 @@ __device__ __forceinline__ bool packed_insert(unsigned long long* t, int logT, i
 // the four community gathers, so that each thread keeps several loads in
 // flight; kNone marks entries past `end`.
 constexpr int kUnroll = 4;
-__device__ __forceinline__ void gather4(const MoveArgs& P, int64_t e0, int64_t stride, int64_t end, int32_t (&c)[4],
-                                        float (&w)[4]) {
+__device__ __forceinline__ void gather4(const MoveArgs& P, int64_t e0, int64_t stride, int64_t end,
+                                        int32_t (&c)[kUnroll], float (&w)[kUnroll]) {
   int32_t col[kUnroll];
 #pragma unroll
   for (int u = 0; u < kUnroll; ++u) {
@@ -804,6 +804,7 @@ __global__ void ell_fill_kernel(const int32_t* list, const int64_t* off, const i
 // largest gain bits (positive doubles order like their bit patterns), then the
 // smallest community among equal gains.
 constexpr int kTileMaxDeg = 512;
+constexpr int kTileUnroll = 4;   // tile entries per thread in flight
 constexpr int kTileCost = 1536;
 constexpr int kTileVtx = 48;          // >= kTileCost / (33 + 4) + 1
 constexpr int kTileSlotsLog = 12;     // 4096 slots for <= kTileCost + kTileMaxDeg + 4 entries
@@ -896,12 +897,12 @@ __global__ void __launch_bounds__(kThreads) move_tile_kernel(MoveArgs P, const i
       }
     }
     __syncthreads();
-    for (int q0 = threadIdx.x; q0 < ne; q0 += 4 * kThreads) {
-      int jj[4];
-      int32_t cc[4];
-      float ww[4];
+    for (int q0 = threadIdx.x; q0 < ne; q0 += kTileUnroll * kThreads) {
+      int jj[kTileUnroll];
+      int32_t cc[kTileUnroll];
+      float ww[kTileUnroll];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kTileUnroll; ++u) {
         int q = q0 + u * kThreads;
         jj[u] = -1;
         if (q < ne) {
@@ -913,10 +914,10 @@ __global__ void __launch_bounds__(kThreads) move_tile_kernel(MoveArgs P, const i
         }
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < kTileUnroll; ++u)
         if (jj[u] >= 0) cc[u] = P.comm[cc[u]];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kTileUnroll; ++u) {
         if (jj[u] >= 0) {
           int j = jj[u];
           if (cc[u] == S.own[j]) atomicOr(&S.flags[j], 1);
@@ -1053,12 +1054,12 @@ __global__ void __launch_bounds__(kThreads) move_tile_packed_kernel(MoveArgs P, 
       }
     }
     __syncthreads();
-    for (int q0 = threadIdx.x; q0 < ne; q0 += 4 * kThreads) {
-      int jj[4];
-      int32_t cc[4];
-      float ww[4];
+    for (int q0 = threadIdx.x; q0 < ne; q0 += kTileUnroll * kThreads) {
+      int jj[kTileUnroll];
+      int32_t cc[kTileUnroll];
+      float ww[kTileUnroll];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kTileUnroll; ++u) {
         int q = q0 + u * kThreads;
         jj[u] = -1;
         if (q < ne) {
@@ -1070,10 +1071,10 @@ __global__ void __launch_bounds__(kThreads) move_tile_packed_kernel(MoveArgs P, 
         }
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < kTileUnroll; ++u)
         if (jj[u] >= 0) cc[u] = P.comm[cc[u]];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kTileUnroll; ++u) {
         if (jj[u] >= 0) {
           int j = jj[u];
           if (cc[u] == S.own[j]) atomicOr(&S.flags[j], 1);
