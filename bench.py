@@ -45,8 +45,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--graphs", type=int, default=8192, help="batched workload: number of graphs")
-    ap.add_argument("--batch-entries", type=float, default=2.5e8,
+    ap.add_argument("--batch-entries", type=float, default=1.25e8,
                     help="batched/serving workloads: entries per packed sub-batch")
+    ap.add_argument("--batch-workers", type=int, default=4,
+                    help="batched workload: contexts running sub-batches at the same time")
     ap.add_argument("--requests", type=int, default=5000, help="serving workload: requests")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving workload: Poisson arrivals per second")
     ap.add_argument("--pool", type=int, default=2048, help="serving workload: distinct small graphs")
@@ -381,11 +383,36 @@ def run_batched(args, world, rank, local, pg):
     G = sum(d.n_graphs for d in dgs)
     E = sum(d.n_entries for d in dgs)
     V = sum(d.n_vertices for d in dgs)
-    lv = Louvain(device=local)
-    lv.set_stream(stream.cuda_stream)
+    # workers: contexts (own streams) that take the sub-batches in turn, so
+    # one batch's host checks and small kernels overlap another's work
+    nw = max(1, min(args.batch_workers, len(dgs)))
+    ctxs = [Louvain(device=local) for _ in range(nw)]
+    if nw == 1:
+        ctxs[0].set_stream(stream.cuda_stream)
+    lv = ctxs[0]
 
     def batched_step():
-        return [lv.run_batch_device(d.src, d.dst, d.w, d.entry_off, d.vertex_off) for d in dgs]
+        if nw == 1:
+            return [lv.run_batch_device(d.src, d.dst, d.w, d.entry_off, d.vertex_off) for d in dgs]
+        import threading
+        out = [None] * len(dgs)
+        errs = []
+
+        def work(k):
+            try:
+                for b in range(k, len(dgs), nw):
+                    d = dgs[b]
+                    out[b] = ctxs[k].run_batch_device(d.src, d.dst, d.w, d.entry_off, d.vertex_off)
+            except Exception as e:   # reported after the join
+                errs.append(e)
+        ts = [threading.Thread(target=work, args=(k,)) for k in range(nw)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        if errs:
+            raise errs[0]
+        return out
 
     clocks = Clocks(local)
     clocks.start()
@@ -446,7 +473,7 @@ def run_batched(args, world, rank, local, pg):
     torch.cuda.synchronize()
     t_e2e = f0.elapsed_time(f1)
     e2e = d0.n_graphs * args.steps * world / (t_e2e / 1e3)
-    del lv
+    del lv, ctxs
     if rank != 0:
         return
     cpu = None
@@ -467,7 +494,7 @@ def run_batched(args, world, rank, local, pg):
         "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
         "config": {"workload": "batched SBMs", "graphs": G, "entries": E, "vertices": V,
                    "n_range": [64, 200000], "blocks": [4, 400], "avg_degree": [8, 32], "intra_fraction": 0.7,
-                   "weights": "integer 1..4", "sub_batches": len(dgs), "seed": 3,
+                   "weights": "integer 1..4", "sub_batches": len(dgs), "batch_workers": nw, "seed": 3,
                    "inputs": "device-resident packed lists (device generator)",
                    "l2": "inputs larger than L2"},
         "plain": {"value": plain, "unit": "graphs/s", "ms_per_sweep": t_plain,
