@@ -1519,28 +1519,6 @@ __global__ void run_sum_kernel(const uint64_t* keys, const float* vals, int64_t 
 // Ain (2w for entries inside one community).  Few communities: block-private
 // shared-memory sums flushed once per block; many: global atomics.
 constexpr int kNmSmemMax = 4096;
-__global__ void __launch_bounds__(kThreads) nm_accum_smem_kernel(const int32_t* src, const int32_t* dst,
-                                                                 const float* w, int64_t E, const int32_t* part,
-                                                                 int32_t C, double* Kc, double* Ain) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  double* sK = reinterpret_cast<double*>(smem);
-  double* sA = sK + C;
-  for (int c = threadIdx.x; c < 2 * C; c += kThreads) sK[c] = 0.0;
-  __syncthreads();
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
-    double x = (double)w[e];
-    int32_t a = part[src[e]], b = part[dst[e]];
-    atomicAdd(&sK[a], x);
-    atomicAdd(&sK[b], x);
-    if (a == b) atomicAdd(&sA[a], 2.0 * x);
-  }
-  __syncthreads();
-  for (int c = threadIdx.x; c < C; c += kThreads) {
-    if (sK[c] != 0.0) atomicAdd(&Kc[c], sK[c]);
-    if (sA[c] != 0.0) atomicAdd(&Ain[c], sA[c]);
-  }
-}
-
 // Lanes of a warp holding the same key add their values before one atomic:
 // large communities (the last levels have few) would otherwise serialise on a
 // handful of addresses.  Every lane gets its group's sum; the lowest lane of
@@ -1555,6 +1533,31 @@ __device__ __forceinline__ void warp_group_add(double* arr, int32_t key, double 
     if ((peers >> l) & 1u) sum += v;
   }
   if (key >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&arr[key], sum);
+}
+
+__global__ void __launch_bounds__(kThreads) nm_accum_smem_kernel(const int32_t* src, const int32_t* dst,
+                                                                 const float* w, int64_t E, const int32_t* part,
+                                                                 int32_t C, double* Kc, double* Ain) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* sK = reinterpret_cast<double*>(smem);
+  double* sA = sK + C;
+  for (int c = threadIdx.x; c < 2 * C; c += kThreads) sK[c] = 0.0;
+  __syncthreads();
+  // few communities: lanes with the same community add first (warp-uniform loop)
+  for (int64_t e0 = blockIdx.x * (int64_t)blockDim.x; e0 < E; e0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = e0 + threadIdx.x;
+    const bool ok = e < E;
+    const double x = ok ? (double)w[e] : 0.0;
+    const int32_t a = ok ? part[src[e]] : -1, b = ok ? part[dst[e]] : -1;
+    warp_group_add(sK, a, x);
+    warp_group_add(sK, b, x);
+    warp_group_add(sA, (ok && a == b) ? a : -1, 2.0 * x);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += kThreads) {
+    if (sK[c] != 0.0) atomicAdd(&Kc[c], sK[c]);
+    if (sA[c] != 0.0) atomicAdd(&Ain[c], sA[c]);
+  }
 }
 
 // Kc, Ain of modularity_fp64 for many communities: grid-stride over whole

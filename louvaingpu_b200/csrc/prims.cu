@@ -1,11 +1,12 @@
 // Device-wide primitives: scans, fixed-tree sums, stable LSD radix sort.
 //
 // Radix sort (replaces thrust::sort_by_key on zip keys, NeighbourCompute.cu:82,
-// InducedGraphKernel.cu:91): 8-bit digits, reduce-then-scan.  Per digit pass a
-// histogram kernel counts digits per 2048-key tile, an exclusive scan over the
-// digit-major [256][tiles] table yields every tile's global digit offsets, and
-// a scatter kernel ranks the tile's keys stably in shared memory (warp
-// __match_any_sync multisplit) and writes them to their global positions.
+// InducedGraphKernel.cu:91): stable LSD, 8-bit digits.  One upfront pass over
+// the keys counts every digit position; then one kernel per digit: a
+// 4096-key tile (taken in launch order from a counter) ranks its keys stably
+// in shared memory (warp __match_any_sync multisplit), learns the counts of
+// its digits in all earlier tiles by decoupled look-back (bounded spin, error
+// flag), and writes its keys out digit run by digit run.
 #include <mutex>
 
 #include "prims.cuh"
