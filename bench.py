@@ -162,6 +162,35 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def phase_roofline(levels, peak):
+    """Algorithmic bytes and achieved GB/s of the level phases of one run:
+    build 2*(8+4) B per doubled-list entry read and written + 8 B per vertex;
+    coarsening 12 B per entry read + 16 B per entry per radix pass + 12 B per
+    coarse entry written; renumbering 12 B per vertex."""
+    def bits(x):
+        b = 0
+        while (1 << b) < x:
+            b += 1
+        return b
+    tot = {"build": 0.0, "induce": 0.0, "renumber": 0.0}
+    ms = {"build": 0.0, "induce": 0.0, "renumber": 0.0}
+    for l, x in enumerate(levels):
+        tot["build"] += 24.0 * 2 * x.n_entries + 8.0 * x.n_vertices
+        ms["build"] += x.ms_build
+        tot["renumber"] += 12.0 * x.n_vertices
+        ms["renumber"] += x.ms_renumber
+        if l + 1 < len(levels):
+            passes = (2 * max(1, bits(x.n_comms)) + 7) // 8
+            tot["induce"] += 12.0 * x.n_entries + 16.0 * x.n_entries * passes + 12.0 * levels[l + 1].n_entries
+            ms["induce"] += x.ms_induce
+    out = {}
+    for k in tot:
+        gbs = tot[k] / (ms[k] * 1e-3) / 1e9 if ms[k] > 0 else 0.0
+        out[k] = {"algorithmic_bytes": tot[k], "ms": round(ms[k], 3), "achieved_gbs": round(gbs, 1),
+                  "frac": round(gbs / peak, 4)}
+    return out
+
+
 def cpu_baseline(n, s, d, w, level_min, threads):
     from oracle import oracle as O
     r = O.Run(n, s, d, w, level_min_gain=level_min, n_threads=threads)
@@ -313,6 +342,7 @@ def run_ours(args, world, rank, local, pg):
     phases = {k: round(sum(getattr(x, "ms_" + k) for x in levels), 3) for k in ("build", "passes", "renumber", "induce")}
     phases.update(host_load_ms=round((h1 - h0) * 1e3, 3), host_run_ms=round((h2 - h1) * 1e3, 3),
                   host_partition_ms=round((h3 - h2) * 1e3, 3))
+    phase_roof = phase_roofline(levels, measured_peak()[0])
     del lv2
     if rank != 0:
         return
@@ -329,6 +359,11 @@ def run_ours(args, world, rank, local, pg):
             v, secs = cpu_baseline(n, s, d, w, level_min, threads)
             sample = f"one whole dendrogram run of the workload ({secs:.1f} s)"
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        from louvaingpu_b200 import graphgen
+        sn, ss_, sd_, sw_ = graphgen.sbm_10k(seed=0)
+        v1, secs1 = cpu_baseline(sn, ss_, sd_, sw_, 1e-6, 1)
+        cpu["single_thread"] = {"value": v1, "unit": UNIT, "cores": 1,
+                                "sample": f"one whole run of the SBM 10k config, one thread ({secs1:.2f} s)"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -340,7 +375,7 @@ def run_ours(args, world, rank, local, pg):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 12 * E, "d2h_bytes_per_step": 4 * n,
                 "ms_per_run": t2 / args.steps, "q_final": qf, "levels": len(levels),
-                "phases_ms": phases},
+                "phases_ms": phases, "phase_roofline": phase_roof},
         "clocks": clk,
         "gpu_launches": launches,
     }

@@ -143,6 +143,17 @@ def test_full_run_bit_exact(Louvain, oracle, gen, case):
         run_equal(lv, res, orun, n, s, d, w, oracle)
 
 
+@pytest.mark.parametrize("name", ["k4k4", "ring_k5", "star", "path"])
+def test_hand_graphs_bit_exact(Louvain, oracle, name):
+    from conftest import hand_graph
+    n, s, d, w = hand_graph(name)
+    orun = oracle.Run(n, s, d, w)
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        res = lv.run()
+        run_equal(lv, res, orun, n, s, d, w, oracle)
+
+
 def test_sbm_10k_config(Louvain, oracle, gen):
     """SBM n=10,000 config: level gain threshold 1e-6, bit-exact dendrogram."""
     n, s, d, w = gen.sbm_10k(seed=0)

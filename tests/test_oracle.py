@@ -165,3 +165,24 @@ def test_sbm_golden_regression(oracle, gen):
     assert [lv.q for lv in r.levels] == g["q_level"]
     assert int(np.bincount(r.final).max()) == g["largest_community"]
     assert oracle.modularity_fp64(n, s, d, w, r.final) == g["final_modularity_fp64"]
+
+
+def test_hand_graph_known_answers(oracle):
+    """Two K4 joined by one edge: in pass 1 (m = 26) vertex 0's best gains
+    tie between 1 and 2 (1 - 9/52), the tie goes to 1 and the singleton-pair
+    rule keeps 0; 1, 2, 3 join 0; 4's best is 5 and it stays; 6, 7 join 5 and
+    5 stays.  In pass 2 vertex 4 has W = 3 to {5,6,7} (gain 3 - 9*4/52 > 0)
+    and W = 1 to {0..3} (gain 1 - 13*4/52 = 0), so it joins 5: two communities,
+    the K4s.  Star: every leaf's only candidate is the centre (gain 1/2), the
+    centre's tie over the leaves goes to leaf 1 and the singleton-pair rule
+    keeps it, so all join community 0.  Ring of 8 K5: the cliques."""
+    from conftest import hand_graph
+    r = oracle.Run(*hand_graph("k4k4"))
+    assert r.final.tolist() == [0, 0, 0, 0, 1, 1, 1, 1]
+    assert r.levels[0].passes == 2
+    r = oracle.Run(*hand_graph("star"))
+    assert r.final.tolist() == [0] * 10
+    r = oracle.Run(*hand_graph("ring_k5"))
+    assert r.final.tolist() == [i // 5 for i in range(40)]
+    r = oracle.Run(*hand_graph("path"))
+    assert len(r.levels) >= 1 and r.final.max() < 12
