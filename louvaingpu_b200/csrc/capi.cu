@@ -119,7 +119,7 @@ size_t arena_estimate(int64_t V, int64_t E, bool copy_list) {
   b += 16 * (size_t)E + 80 * (size_t)V;     // CSR (<= 2E entries) + per-vertex + state
   b += 88 * (size_t)E + 24 * (size_t)V;     // build scratch: 2 x 2E x 12 B sort, head/pos, wsum
   b += 16 * (size_t)E;                      // hub tables (degree-bounded) and per-level partitions
-  b += 32 * (size_t)V + (size_t)E / 4;      // first-pass chunk lists and partials
+  b += 36 * (size_t)V + (size_t)E / 4;      // first-pass chunk lists, partials, int32 degrees
   b += (size_t)64 << 20;
   return b;
 }

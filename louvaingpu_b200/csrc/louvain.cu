@@ -331,6 +331,7 @@ struct MoveArgs {
   double* din;
   int32_t* dsize;
   PassCtl* ctl;
+  const int32_t* k32;    // degrees as int32 (integral weights), else nullptr: the singleton tot
   const int32_t* gid;    // batched runs: graph of each vertex (nullptr for one graph)
   const int32_t* gdone;  // batched runs: 1 once a graph's level loop has stopped
 };
@@ -648,7 +649,7 @@ __global__ void __launch_bounds__(kThreads) sp_thread_kernel(MoveArgs P, EllArgs
     const int32_t c = ok ? __ldcs(L.col + j * D + sl) : -1;
     const float wv = ok ? __ldcs(L.w + j * D + sl) : 0.0f;
     const double kf = ok ? L.info[j].kfrac : 0.0;
-    const double t = c >= 0 ? P.tot[c] : 0.0;
+    const double t = c < 0 ? 0.0 : (P.k32 ? (double)P.k32[c] : P.tot[c]);   // singleton tot = k
     double bg = 0.0, bw = 0.0;
     int32_t bc = kNone;
     const double W = (double)wv;
@@ -705,7 +706,8 @@ __global__ void __launch_bounds__(kThreads) sp_chunk_kernel(MoveArgs P, const in
         w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
       }
 #pragma unroll
-      for (int u = 0; u < kSpUnroll; ++u) t[u] = c[u] != kNone ? P.tot[c[u]] : 0.0;
+      for (int u = 0; u < kSpUnroll; ++u)
+        t[u] = c[u] == kNone ? 0.0 : (P.k32 ? (double)P.k32[c[u]] : P.tot[c[u]]);   // singleton tot = k
 #pragma unroll
       for (int u = 0; u < kSpUnroll; ++u) {
         const double W = (double)w[u];
@@ -760,6 +762,11 @@ __global__ void sp_fill_kernel(const int32_t* list, int64_t n, const int64_t* of
 }
 
 // k/2m; in a batched run m is the vertex's own graph's (gm[vgid[i]]).
+__global__ void k32_kernel(int32_t V, const double* k, int32_t* k32) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x)
+    k32[i] = (int32_t)k[i];   // integral and below 2^30 when called
+}
+
 __global__ void kfrac_kernel(int32_t V, const double* k, double m, const double* gm, const int32_t* vgid,
                              double* kfrac) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
@@ -1632,6 +1639,7 @@ MoveArgs move_args(const LevelGraph& g, CommState& st) {
   P.next = st.next; P.cand = st.cand;
   P.dtot = st.dtot; P.din = st.din; P.dsize = st.dsize;
   P.ctl = st.ctl;
+  P.k32 = g.k32;
   P.gid = st.gid;
   P.gdone = st.gdone;
   return P;
@@ -1852,6 +1860,13 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
     LVG_CUDA(cudaMemcpyAsync(&h, notint, sizeof h, cudaMemcpyDeviceToHost, s));
     LVG_CUDA(cudaStreamSynchronize(s));
     g.int_acc = h == 0;
+  }
+  // the first pass gathers a neighbour's singleton total k as int32 when exact
+  g.k32 = nullptr;
+  if (g.int_acc && V > 0) {
+    g.k32 = a.lo_n<int32_t>(V);
+    k32_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, g.k, g.k32);
+    LVG_LAUNCH();
   }
   // hub tables
   g.nchunk = 0;

@@ -63,6 +63,7 @@ struct LevelGraph {
   int32_t* tile_start = nullptr;  // [ntiles+1] first bucket index of each tile
   int64_t ntiles = 0;
   bool int_acc = false;           // integral weights, degrees < 2^30: exact int32 sums
+  int32_t* k32 = nullptr;         // k as int32 when int_acc (the first pass's gathered totals)
   // hub tables
   int64_t hub_slots = 0;
   int64_t* hub_toff = nullptr;    // [nhub] table offset
