@@ -358,11 +358,14 @@ __device__ __forceinline__ void warp_best(double& bg, int32_t& bc, double& bw) {
 // (OneLevelKernel.cu:407-410), remove/insert into the delta buffers
 // (OneLevelKernel.cu:52-78, 412-421) and the isolated-merge candidate
 // (OneLevelKernel.cu:142-169).
+// SINGLETON: the state is the level's initial one (every community a single
+// vertex), so both sizes are 1 without reading them.
+template <bool SINGLETON = false>
 __device__ __forceinline__ void apply_decision_kl(const MoveArgs& P, int32_t i, int32_t own, int32_t bc, double bw,
                                                   int32_t nseg, double ki, float loopw) {
   if (P.gdone && P.gdone[P.gid[i]]) return;   // that graph's pass loop has stopped
   int32_t raw = bc == kNone ? own : bc;
-  int32_t so = P.size[own], sb = P.size[raw];
+  int32_t so = SINGLETON ? 1 : P.size[own], sb = SINGLETON ? 1 : P.size[raw];
   int32_t best = raw;
   if (so == 1 && sb == 1 && raw > own) best = own;
   P.next[i] = best;
@@ -378,11 +381,12 @@ __device__ __forceinline__ void apply_decision_kl(const MoveArgs& P, int32_t i, 
   }
 }
 
+template <bool SINGLETON = false>
 __device__ __forceinline__ void apply_decision(const MoveArgs& P, int32_t i, int32_t own, int32_t bc, double bw,
                                                int32_t nseg) {
   if (P.gdone && P.gdone[P.gid[i]]) return;   // that graph's pass loop has stopped
   int32_t raw = bc == kNone ? own : bc;
-  int32_t so = P.size[own], sb = P.size[raw];
+  int32_t so = SINGLETON ? 1 : P.size[own], sb = SINGLETON ? 1 : P.size[raw];
   int32_t best = raw;
   if (so == 1 && sb == 1 && raw > own) best = own;
   P.next[i] = best;
@@ -669,7 +673,7 @@ __global__ void __launch_bounds__(kThreads) sp_thread_kernel(MoveArgs P, EllArgs
       const unsigned seg = (D == 32) ? valid : ((valid >> (lane & ~(D - 1))) & ((1u << D) - 1u));
       const VInfo vi = L.info[j];
       const int32_t i = vi.vid_loop >> 1;
-      apply_decision_kl(P, i, i, bc, bw, __popc(seg) + (vi.vid_loop & 1), vi.k, vi.loopw);
+      apply_decision_kl<true>(P, i, i, bc, bw, __popc(seg) + (vi.vid_loop & 1), vi.k, vi.loopw);
     }
   }
 }
@@ -719,7 +723,7 @@ __global__ void __launch_bounds__(kThreads) sp_chunk_kernel(MoveArgs P, const in
     }
     warp_best(bg, bc, bw);
     if (lane == 0) {
-      if (deg <= kSpChunk) apply_decision(P, i, i, bc, bw, (int32_t)deg + (P.has_loop[i] ? 1 : 0));
+      if (deg <= kSpChunk) apply_decision<true>(P, i, i, bc, bw, (int32_t)deg + (P.has_loop[i] ? 1 : 0));
       else part[q] = HubPartial{bg, bw, bc, 0};
     }
   }
@@ -737,7 +741,7 @@ __global__ void sp_combine_kernel(MoveArgs P, const int2* multi, int64_t nmulti,
       const HubPartial h = part[first + k];
       if (better(h.g, h.c, g, c)) { g = h.g; c = h.c; w = h.w; }
     }
-    apply_decision(P, i, i, c, w, (int32_t)deg + (P.has_loop[i] ? 1 : 0));
+    apply_decision<true>(P, i, i, c, w, (int32_t)deg + (P.has_loop[i] ? 1 : 0));
   }
 }
 
