@@ -197,6 +197,24 @@ def cpu_baseline(n, s, d, w, level_min, threads):
     return r.pass_entries / r.seconds, r.seconds
 
 
+def max_over_ranks(values, pg):
+    """Element-wise max over the ranks (device times: the slowest rank sets
+    the job's time).  NCCL reduces on the GPU, gloo on the host."""
+    if not pg:
+        return list(values)
+    import torch
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def whole_job_rate(units_per_rank, world, t_max_ms):
+    """Units every rank processed (equal per rank: replicas / weak scaling)
+    divided by the slowest rank's time."""
+    return units_per_rank * world / (t_max_ms / 1e3)
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -279,11 +297,9 @@ def run_ours(args, world, rank, local, pg):
     launches = kernel_launches() - l0
     t_ms = e0.elapsed_time(e1)
     if pg:
-        tt = torch.tensor([t_ms], device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t_ms = float(tt.item())
+        t_ms = max_over_ranks([t_ms], pg)[0]
     entries = nnz * passes_total
-    value = entries * world / (t_ms / 1e3)
+    value = whole_job_rate(entries, world, t_ms)
     # roofline of the move kernels: B_pass = 12 nnz + 24 V bytes per pass
     peak, peak_kind = measured_peak()
     b_pass = 12.0 * nnz + 24.0 * V
@@ -324,9 +340,7 @@ def run_ours(args, world, rank, local, pg):
     torch.cuda.synchronize()
     t2 = f0.elapsed_time(f1)
     if pg:
-        tt = torch.tensor([t2], device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t2 = float(tt.item())
+        t2 = max_over_ranks([t2], pg)[0]
     clk = clocks.stop()
     e2e_value = pe * world / (t2 / 1e3)
     # one more run, timed by part on the host (not part of the timed steps)
@@ -489,9 +503,7 @@ def run_batched(args, world, rank, local, pg):
     clk = clocks.stop()
     del pl
     if pg:
-        tt = torch.tensor([t_ms, t_plain], device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t_ms, t_plain = float(tt[0].item()), float(tt[1].item())
+        t_ms, t_plain = max_over_ranks([t_ms, t_plain], pg)
     value = G * args.steps * world / (t_ms / 1e3)
     plain = G * world / (t_plain / 1e3)
     # e2e: the host-buffer entry point on the first sub-batch, from pinned memory
