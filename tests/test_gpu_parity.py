@@ -154,6 +154,24 @@ def test_hand_graphs_bit_exact(Louvain, oracle, name):
         run_equal(lv, res, orun, n, s, d, w, oracle)
 
 
+@pytest.mark.parametrize("case", ["weighted", "hub"])
+def test_fractional_weights_within_tolerance(Louvain, oracle, gen, case):
+    """Non-integral weights take the f64 accumulators (tile, block, hub
+    tables); sums may round in another order than the oracle's, so the
+    check is the north-star tolerance on the final modularity."""
+    n, s, d, w = make_case(gen, case)
+    w = (w * 0.37 + 0.05).astype(np.float32)
+    orun = oracle.Run(n, s, d, w)
+    q_oracle = oracle.modularity_fp64(n, s, d, w, orun.final)
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        res = lv.run()
+        part = lv.partition()
+        assert part.min() >= 0 and part.max() < n
+        assert res.q_final == pytest.approx(oracle.modularity_fp64(n, s, d, w, part), abs=1e-9)
+        assert abs(res.q_final - q_oracle) <= 1e-3
+
+
 def test_sbm_10k_config(Louvain, oracle, gen):
     """SBM n=10,000 config: level gain threshold 1e-6, bit-exact dendrogram."""
     n, s, d, w = gen.sbm_10k(seed=0)
