@@ -291,6 +291,67 @@ lvg_status lvg_modularity_fp64_noalloc(const int32_t* d_src, const int32_t* d_ds
 /* Bytes of device memory the context holds (arena capacity) and its peak use. */
 lvg_status lvg_memory(const lvg_ctx* ctx, int64_t* capacity, int64_t* peak);
 
+/* ------------------------------------------------------------ autotuner ----
+ * The move kernels split a pass's vertices into degree classes: rows up to 32
+ * entries (thread/lane kernels), up to tile_max_degree (shared-memory tiles),
+ * up to block_max_degree (one block and one shared table per vertex) and
+ * above (global hub tables).  Which split is fastest depends on the graph's
+ * degree distribution and on the GPU.  The reference has fixed launch shapes
+ * (<<<N,32>>> per vertex, OneLevelKernel.cu:248-386, and serial chunks for
+ * hubs) and no tuner; these entry points have no counterpart in it.
+ *
+ * The thresholds change which kernel handles a vertex, never a decision: every
+ * kernel computes the same FP64 gains with the same tie-break, so any pair
+ * gives the same passes, partitions and Q (the tuner checks this on the graph
+ * it measures and fails with LVG_ERR_STATE if a candidate disagrees). */
+typedef struct {
+  int32_t tile_max_degree;
+  int32_t block_max_degree;
+  float move_ms;    /* median device time of the move kernels of the hashing
+                       passes (every pass after the first) of one level-0
+                       one-level phase; < 0: candidate did not fit the arena */
+  float build_ms;   /* device time of the level-0 build with these thresholds */
+} lvg_tune_point;
+
+typedef struct {
+  const int32_t* tile_max_degrees;   /* candidates, each in [32, 512] (NULL: 64, 128, 256, 512) */
+  int32_t n_tile;
+  const int32_t* block_max_degrees;  /* candidates, each in [32, 8192] (NULL: 1024, 2048, 4096, 8192) */
+  int32_t n_block;
+  int32_t reps;                      /* timed one-level phases per candidate (<= 0: 3), after one untimed */
+  int32_t use_cache;                 /* 1: reuse the pair tuned earlier in this process for a graph of the
+                                        same shape class on the same device, without measuring */
+} lvg_tune_space;
+
+/* Measure every (tile, block) pair with tile <= block on the loaded level-0
+ * graph and keep the fastest: rebuild level 0 with the pair, run one untimed
+ * and `reps` timed level-0 one-level phases, and take the median move time of
+ * the hashing passes.  Pairs within 2 % of the fastest defer to the context's
+ * configured pair when it is among them (lvg_tune_pick).  The chosen pair is
+ * then used by every level built afterwards (this graph's later levels,
+ * lvg_run, batched runs of this context) and the context is left at level 0,
+ * rebuilt, as after a load.  Shape class = (device, floor(log2 V),
+ * floor(log2 nnz), floor(log2 max degree), integral weights); the process-wide
+ * cache keeps the pair of each class.  points (nullable, cap entries) receives
+ * every measured pair in order, *n_points their number (0 on a cache hit);
+ * best (nullable) the chosen one.  Costs one level-0 build and reps+1
+ * one-level phases per pair. */
+lvg_status lvg_autotune(lvg_ctx* ctx, const lvg_tune_space* space, lvg_tune_point* points, int32_t cap,
+                        int32_t* n_points, lvg_tune_point* best);
+
+/* The degree thresholds the context builds levels with. */
+lvg_status lvg_get_thresholds(const lvg_ctx* ctx, int32_t* tile_max_degree, int32_t* block_max_degree);
+
+/* The tuner's choice among measured points (host only, no device call): the
+ * smallest move_ms >= 0; a point equal to (pref_tile, pref_block) wins when
+ * within 2 % of it; among equal times the earlier point.  *best_index = -1
+ * when no point has move_ms >= 0. */
+lvg_status lvg_tune_pick(const lvg_tune_point* points, int32_t n, int32_t pref_tile, int32_t pref_block,
+                         int32_t* best_index);
+
+/* Forget every cached pair. */
+lvg_status lvg_tune_cache_clear(void);
+
 #ifdef __cplusplus
 }
 #endif

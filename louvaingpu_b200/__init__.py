@@ -4,8 +4,8 @@ The compute runs in liblvg.so (hand-written CUDA for sm_100a, C ABI in
 include/lvg.h); this package is the Python side of that ABI.
 """
 from .louvain import (BatchResult, Louvain, LevelInfo, RunResult, count_partitions, kernel_launches,  # noqa: F401
-                      pack_graphs)
+                      pack_graphs, tune_pick)
 from ._lib import LvgError  # noqa: F401
 
 __all__ = ["Louvain", "LevelInfo", "RunResult", "BatchResult", "pack_graphs", "count_partitions", "kernel_launches",
-           "LvgError"]
+           "tune_pick", "LvgError"]

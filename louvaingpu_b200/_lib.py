@@ -80,6 +80,26 @@ class LvgServeResult(ctypes.Structure):
     ]
 
 
+class LvgTunePoint(ctypes.Structure):
+    _fields_ = [
+        ("tile_max_degree", ctypes.c_int32),
+        ("block_max_degree", ctypes.c_int32),
+        ("move_ms", ctypes.c_float),
+        ("build_ms", ctypes.c_float),
+    ]
+
+
+class LvgTuneSpace(ctypes.Structure):
+    _fields_ = [
+        ("tile_max_degrees", ctypes.POINTER(ctypes.c_int32)),
+        ("n_tile", ctypes.c_int32),
+        ("block_max_degrees", ctypes.POINTER(ctypes.c_int32)),
+        ("n_block", ctypes.c_int32),
+        ("reps", ctypes.c_int32),
+        ("use_cache", ctypes.c_int32),
+    ]
+
+
 # Every entry point declared in include/lvg.h, with its ctypes signature.
 P = ctypes.c_void_p
 i32, i64, dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
@@ -126,6 +146,11 @@ SIGNATURES = {
     "lvg_server_last_error": (ctypes.c_char_p, [P]),
     "lvg_server_destroy": (i32, [P]),
     "lvg_modularity_fp64_noalloc": (i32, [P, P, P, i64, P, i32, P, ctypes.POINTER(dbl)]),
+    "lvg_autotune": (i32, [P, ctypes.POINTER(LvgTuneSpace), ctypes.POINTER(LvgTunePoint), i32,
+                           ctypes.POINTER(i32), ctypes.POINTER(LvgTunePoint)]),
+    "lvg_get_thresholds": (i32, [P, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
+    "lvg_tune_pick": (i32, [ctypes.POINTER(LvgTunePoint), i32, i32, i32, ctypes.POINTER(i32)]),
+    "lvg_tune_cache_clear": (i32, []),
 }
 
 # Device generators declared in include/lvg_gen.h (same library).

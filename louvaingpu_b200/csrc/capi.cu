@@ -12,7 +12,10 @@
 #include <cmath>
 #include <numeric>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "louvain.cuh"
@@ -809,6 +812,172 @@ lvg_status lvg_memory(const lvg_ctx* c, int64_t* capacity, int64_t* peak) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Autotuner of the degree-class thresholds (no counterpart in the reference,
+// whose launch shapes are fixed: <<<N,32>>> per vertex, OneLevelKernel.cu:248-386).
+namespace {
+
+using ShapeKey = std::tuple<int, int, int, int, int>;   // device, log2 V, log2 nnz, log2 max degree, integral
+std::mutex g_tune_mu;
+std::map<ShapeKey, std::pair<int32_t, int32_t>> g_tune_cache;
+
+int floor_log2(int64_t x) {
+  int l = -1;
+  for (; x > 0; x >>= 1) ++l;
+  return l;
+}
+
+ShapeKey shape_key(lvg_ctx* c) {
+  const int64_t dmax = max_degree(c->g, c->arena, c->stream);
+  return ShapeKey(c->device, floor_log2(c->g.V), floor_log2(c->g.nnz), floor_log2(dmax), c->g.int_acc ? 1 : 0);
+}
+
+void set_tuning(lvg_ctx* c, int32_t tile, int32_t block) {
+  c->tune.warp_max = tile;
+  c->tune.block_max = block;
+  c->cfg.tile_max_degree = tile;
+  c->cfg.block_max_degree = block;
+}
+
+}  // namespace
+
+extern "C" lvg_status lvg_tune_pick(const lvg_tune_point* p, int32_t n, int32_t pref_tile, int32_t pref_block,
+                                    int32_t* best_index) {
+  if (!best_index || n < 0 || (n > 0 && !p)) return LVG_ERR_INVALID_ARG;
+  int32_t b = -1;
+  for (int32_t i = 0; i < n; ++i)
+    if (p[i].move_ms >= 0.0f && (b < 0 || p[i].move_ms < p[b].move_ms)) b = i;
+  if (b >= 0) {
+    for (int32_t i = 0; i < n; ++i) {
+      if (p[i].tile_max_degree == pref_tile && p[i].block_max_degree == pref_block && p[i].move_ms >= 0.0f &&
+          (double)p[i].move_ms <= 1.02 * (double)p[b].move_ms) {
+        b = i;
+        break;
+      }
+    }
+  }
+  *best_index = b;
+  return LVG_OK;
+}
+
+extern "C" lvg_status lvg_tune_cache_clear(void) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune_cache.clear();
+  return LVG_OK;
+}
+
+extern "C" lvg_status lvg_get_thresholds(const lvg_ctx* c, int32_t* tile_max_degree, int32_t* block_max_degree) {
+  if (!c) return LVG_ERR_INVALID_ARG;
+  if (tile_max_degree) *tile_max_degree = c->tune.warp_max;
+  if (block_max_degree) *block_max_degree = c->tune.block_max;
+  return LVG_OK;
+}
+
+extern "C" lvg_status lvg_autotune(lvg_ctx* c, const lvg_tune_space* sp, lvg_tune_point* points, int32_t cap,
+                                   int32_t* n_points, lvg_tune_point* best) {
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded, LVG_ERR_STATE, "no graph loaded");
+    require(cap >= 0 && (cap == 0 || points), LVG_ERR_INVALID_ARG, "bad points buffer");
+    static const int32_t kTiles[] = {64, 128, 256, 512};
+    static const int32_t kBlocks[] = {1024, 2048, 4096, 8192};
+    const int32_t* tl = sp && sp->tile_max_degrees ? sp->tile_max_degrees : kTiles;
+    const int32_t nt = sp && sp->tile_max_degrees ? sp->n_tile : 4;
+    const int32_t* bl = sp && sp->block_max_degrees ? sp->block_max_degrees : kBlocks;
+    const int32_t nb = sp && sp->block_max_degrees ? sp->n_block : 4;
+    require(nt > 0 && nb > 0, LVG_ERR_INVALID_ARG, "empty candidate list");
+    for (int32_t i = 0; i < nt; ++i)
+      require(tl[i] >= 32 && tl[i] <= 512, LVG_ERR_INVALID_ARG, "tile_max_degree candidates must be in [32, 512]");
+    for (int32_t i = 0; i < nb; ++i)
+      require(bl[i] >= 32 && bl[i] <= 8192, LVG_ERR_INVALID_ARG, "block_max_degree candidates must be in [32, 8192]");
+    const int reps = sp && sp->reps > 0 ? sp->reps : 3;
+    std::vector<std::pair<int32_t, int32_t>> cands;
+    for (int32_t i = 0; i < nt; ++i)
+      for (int32_t j = 0; j < nb; ++j)
+        if (bl[j] >= tl[i] && std::find(cands.begin(), cands.end(), std::make_pair(tl[i], bl[j])) == cands.end())
+          cands.emplace_back(tl[i], bl[j]);
+    require(!cands.empty(), LVG_ERR_INVALID_ARG, "no candidate pair has tile_max_degree <= block_max_degree");
+    if (n_points) *n_points = 0;
+    const int32_t pref_tile = c->tune.warp_max, pref_block = c->tune.block_max;
+    if (c->level != 0 || c->renumbered || !c->levels.empty()) reset_to_level0(c);
+    const ShapeKey key = shape_key(c);
+    if (sp && sp->use_cache) {
+      std::pair<int32_t, int32_t> hit(0, 0);
+      {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) hit = it->second;
+      }
+      if (hit.first > 0) {
+        set_tuning(c, hit.first, hit.second);
+        reset_to_level0(c);
+        if (best) *best = lvg_tune_point{hit.first, hit.second, -1.0f, -1.0f};
+        return;
+      }
+    }
+    std::vector<lvg_tune_point> pts;
+    std::vector<int32_t> labels, ref_labels;
+    double ref_q = 0.0;
+    int32_t ref_passes = -1;
+    for (const auto& cand : cands) {
+      lvg_tune_point pt{cand.first, cand.second, -1.0f, -1.0f};
+      set_tuning(c, cand.first, cand.second);
+      try {
+        reset_to_level0(c);
+      } catch (const Error& e) {
+        if (e.status != LVG_ERR_OOM) throw;
+        pts.push_back(pt);   // this pair's hub tables do not fit the context's arena
+        continue;
+      }
+      const double q0 = read_q(c);   // synchronises: the build events are complete
+      pt.build_ms = elapsed(c->pev[0], c->pev[1]);
+      std::vector<float> ms;
+      for (int r = 0; r <= reps; ++r) {
+        double q = 0.0;
+        int32_t passes = 0, status = 0;
+        one_level(c, q0, &q, &passes, &status, nullptr);
+        if (r == 0) {
+          // the thresholds route vertices to kernels; the decisions must not move
+          labels.resize((size_t)c->g.V);
+          if (c->g.V > 0)
+            LVG_CUDA(cudaMemcpyAsync(labels.data(), c->st.comm, sizeof(int32_t) * c->g.V, cudaMemcpyDeviceToHost,
+                                     c->stream));
+          sync(c);
+          if (ref_passes < 0) {
+            ref_q = q;
+            ref_passes = passes;
+            ref_labels = labels;
+          } else {
+            require(q == ref_q && passes == ref_passes && labels == ref_labels, LVG_ERR_STATE,
+                    "autotune: two threshold pairs gave different level-0 results");
+          }
+          continue;
+        }
+        float h = 0.0f;
+        for (size_t p = 1; p < c->move_pass_ms.size(); ++p) h += c->move_pass_ms[p];
+        ms.push_back(h);
+      }
+      std::sort(ms.begin(), ms.end());
+      pt.move_ms = ms[ms.size() / 2];
+      pts.push_back(pt);
+    }
+    int32_t bi = -1;
+    lvg_tune_pick(pts.data(), (int32_t)pts.size(), pref_tile, pref_block, &bi);
+    const int32_t tile = bi >= 0 ? pts[bi].tile_max_degree : pref_tile;
+    const int32_t block = bi >= 0 ? pts[bi].block_max_degree : pref_block;
+    set_tuning(c, tile, block);
+    reset_to_level0(c);
+    if (bi >= 0) {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      g_tune_cache[key] = std::make_pair(tile, block);
+    }
+    const int32_t n = (int32_t)pts.size();
+    for (int32_t i = 0; i < std::min(n, cap); ++i) points[i] = pts[i];
+    if (n_points) *n_points = n;
+    if (best) *best = bi >= 0 ? pts[bi] : lvg_tune_point{tile, block, -1.0f, -1.0f};
+  });
+}
 
 // ============================================================================
 // Batched runs (no counterpart in the reference, which runs one graph per

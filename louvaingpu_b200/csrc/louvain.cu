@@ -2855,4 +2855,26 @@ void batch_modularity(const int32_t* src, const int32_t* dst, const float* w, in
   LVG_LAUNCH();
 }
 
+// ------------------------------------------------------------ degree statistics
+__global__ void max_degree_kernel(const int64_t* off, int32_t V, unsigned long long* out) {
+  unsigned long long m = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, (unsigned long long)(off[i + 1] - off[i]));
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+int64_t max_degree(const LevelGraph& g, Arena& a, cudaStream_t s) {
+  if (g.V <= 0) return 0;
+  HiScope hs(a);
+  unsigned long long* d = a.hi_n<unsigned long long>(1);
+  LVG_CUDA(cudaMemsetAsync(d, 0, sizeof *d, s));
+  max_degree_kernel<<<sm_grid(g.V, kThreads), kThreads, 0, s>>>(g.off, g.V, d);
+  LVG_LAUNCH();
+  unsigned long long h = 0;
+  LVG_CUDA(cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  return (int64_t)h;
+}
+
 }  // namespace lvg

@@ -235,6 +235,9 @@ void batch_modularity(const int32_t* src, const int32_t* dst, const float* w, in
                       const int32_t* local0, const BatchPlan& cp, const int32_t* cg, int32_t Ctot, int32_t G,
                       double* q, Arena& a, cudaStream_t s);
 
+// Largest row of the level CSR (synchronises).
+int64_t max_degree(const LevelGraph& g, Arena& a, cudaStream_t s);
+
 // x[i] = i for i < n.
 void iota(int32_t* x, int64_t n, cudaStream_t s);
 // part_out[i] = part_level[composed[i]] for i < n.

@@ -294,6 +294,41 @@ class Louvain:
         self._check(self._L.lvg_move_stats(self._h, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
 
+    # ------------------------------------------------------------------ autotuner
+    def autotune(self, tile_max_degrees=None, block_max_degrees=None, reps=3, use_cache=False):
+        """Time every (tile, block) degree-threshold pair on the loaded
+        level-0 graph and keep the fastest (lvg_autotune).  Returns (best,
+        points): best = (tile, block, move_ms, build_ms), points = every
+        measured pair in that form (empty on a cache hit).  Results of the
+        run do not depend on the pair."""
+        sp = _lib.LvgTuneSpace()
+        keep = []
+        if tile_max_degrees is not None:
+            t = np.ascontiguousarray(tile_max_degrees, np.int32)
+            keep.append(t)
+            sp.tile_max_degrees = t.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+            sp.n_tile = len(t)
+        if block_max_degrees is not None:
+            b = np.ascontiguousarray(block_max_degrees, np.int32)
+            keep.append(b)
+            sp.block_max_degrees = b.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+            sp.n_block = len(b)
+        sp.reps = int(reps)
+        sp.use_cache = 1 if use_cache else 0
+        cap = 64
+        pts = (_lib.LvgTunePoint * cap)()
+        n = ctypes.c_int32()
+        best = _lib.LvgTunePoint()
+        self._check(self._L.lvg_autotune(self._h, ctypes.byref(sp), pts, cap, ctypes.byref(n), ctypes.byref(best)))
+        row = lambda p: (p.tile_max_degree, p.block_max_degree, p.move_ms, p.build_ms)
+        return row(best), [row(pts[i]) for i in range(min(n.value, cap))]
+
+    def thresholds(self):
+        """(tile_max_degree, block_max_degree) the context builds levels with."""
+        t, b = ctypes.c_int32(), ctypes.c_int32()
+        self._check(self._L.lvg_get_thresholds(self._h, ctypes.byref(t), ctypes.byref(b)))
+        return t.value, b.value
+
     def memory(self):
         cap, peak = ctypes.c_int64(), ctypes.c_int64()
         self._check(self._L.lvg_memory(self._h, ctypes.byref(cap), ctypes.byref(peak)))
@@ -305,6 +340,20 @@ def kernel_launches():
     n = ctypes.c_int64()
     _lib.check(None, _lib.load().lvg_kernel_launches(ctypes.byref(n)))
     return n.value
+
+
+def tune_pick(points, pref=(512, 4096)):
+    """Index of the point the autotuner keeps among (tile, block, move_ms,
+    build_ms) rows (lvg_tune_pick; host only): the fastest, or the preferred
+    pair when within 2 % of it; -1 when no point was measured."""
+    n = len(points)
+    arr = (_lib.LvgTunePoint * max(n, 1))()
+    for i, p in enumerate(points):
+        arr[i].tile_max_degree, arr[i].block_max_degree = int(p[0]), int(p[1])
+        arr[i].move_ms, arr[i].build_ms = float(p[2]), float(p[3]) if len(p) > 3 else 0.0
+    b = ctypes.c_int32()
+    _lib.check(None, _lib.load().lvg_tune_pick(arr, n, int(pref[0]), int(pref[1]), ctypes.byref(b)))
+    return b.value
 
 
 def count_partitions(part):
