@@ -901,6 +901,10 @@ extern "C" lvg_status lvg_autotune(lvg_ctx* c, const lvg_tune_space* sp, lvg_tun
     if (n_points) *n_points = 0;
     const int32_t pref_tile = c->tune.warp_max, pref_block = c->tune.block_max;
     if (c->level != 0 || c->renumbered || !c->levels.empty()) reset_to_level0(c);
+    if (c->E0 == 0 || c->g.nnz == 0) {   // no move pass to time (lvg_run runs none either)
+      if (best) *best = lvg_tune_point{pref_tile, pref_block, -1.0f, -1.0f};
+      return;
+    }
     const ShapeKey key = shape_key(c);
     if (sp && sp->use_cache) {
       std::pair<int32_t, int32_t> hit(0, 0);

@@ -86,3 +86,13 @@ def test_autotuned_batched_run_equals_default(Louvain, gen):
     np.testing.assert_array_equal(r0.partition, r1.partition)
     np.testing.assert_array_equal(r0.q_final, r1.q_final)
     np.testing.assert_array_equal(r0.n_levels, r1.n_levels)
+
+
+def test_autotune_empty_graph_keeps_configured_pair(Louvain):
+    with Louvain(tile_max_degree=256, block_max_degree=2048) as lv:
+        lv.load_edges([], [], [], 7)
+        best, pts = lv.autotune()
+        assert pts == [] and (best[0], best[1]) == (256, 2048)
+        assert lv.thresholds() == (256, 2048)
+        lv.run()
+        assert lv.partition().tolist() == list(range(7))
