@@ -303,7 +303,8 @@ lvg_status lvg_memory(const lvg_ctx* ctx, int64_t* capacity, int64_t* peak);
  * The thresholds change which kernel handles a vertex, never a decision: every
  * kernel computes the same FP64 gains with the same tie-break, so any pair
  * gives the same passes, partitions and Q (the tuner checks this on the graph
- * it measures and fails with LVG_ERR_STATE if a candidate disagrees). */
+ * it measures and fails with LVG_ERR_STATE if a candidate disagrees; on any
+ * failure the context is left rebuilt at level 0 with the pair it had). */
 typedef struct {
   int32_t tile_max_degree;
   int32_t block_max_degree;

@@ -924,47 +924,57 @@ extern "C" lvg_status lvg_autotune(lvg_ctx* c, const lvg_tune_space* sp, lvg_tun
     std::vector<int32_t> labels, ref_labels;
     double ref_q = 0.0;
     int32_t ref_passes = -1;
-    for (const auto& cand : cands) {
-      lvg_tune_point pt{cand.first, cand.second, -1.0f, -1.0f};
-      set_tuning(c, cand.first, cand.second);
-      try {
-        reset_to_level0(c);
-      } catch (const Error& e) {
-        if (e.status != LVG_ERR_OOM) throw;
-        pts.push_back(pt);   // this pair's hub tables do not fit the context's arena
-        continue;
-      }
-      const double q0 = read_q(c);   // synchronises: the build events are complete
-      pt.build_ms = elapsed(c->pev[0], c->pev[1]);
-      std::vector<float> ms;
-      for (int r = 0; r <= reps; ++r) {
-        double q = 0.0;
-        int32_t passes = 0, status = 0;
-        one_level(c, q0, &q, &passes, &status, nullptr);
-        if (r == 0) {
-          // the thresholds route vertices to kernels; the decisions must not move
-          labels.resize((size_t)c->g.V);
-          if (c->g.V > 0)
-            LVG_CUDA(cudaMemcpyAsync(labels.data(), c->st.comm, sizeof(int32_t) * c->g.V, cudaMemcpyDeviceToHost,
-                                     c->stream));
-          sync(c);
-          if (ref_passes < 0) {
-            ref_q = q;
-            ref_passes = passes;
-            ref_labels = labels;
-          } else {
-            require(q == ref_q && passes == ref_passes && labels == ref_labels, LVG_ERR_STATE,
-                    "autotune: two threshold pairs gave different level-0 results");
-          }
+    try {
+      for (const auto& cand : cands) {
+        lvg_tune_point pt{cand.first, cand.second, -1.0f, -1.0f};
+        set_tuning(c, cand.first, cand.second);
+        try {
+          reset_to_level0(c);
+        } catch (const Error& e) {
+          if (e.status != LVG_ERR_OOM) throw;
+          pts.push_back(pt);   // this pair's hub tables do not fit the context's arena
           continue;
         }
-        float h = 0.0f;
-        for (size_t p = 1; p < c->move_pass_ms.size(); ++p) h += c->move_pass_ms[p];
-        ms.push_back(h);
+        const double q0 = read_q(c);   // synchronises: the build events are complete
+        pt.build_ms = elapsed(c->pev[0], c->pev[1]);
+        std::vector<float> ms;
+        for (int r = 0; r <= reps; ++r) {
+          double q = 0.0;
+          int32_t passes = 0, status = 0;
+          one_level(c, q0, &q, &passes, &status, nullptr);
+          if (r == 0) {
+            // the thresholds route vertices to kernels; the decisions must not move
+            labels.resize((size_t)c->g.V);
+            if (c->g.V > 0)
+              LVG_CUDA(cudaMemcpyAsync(labels.data(), c->st.comm, sizeof(int32_t) * c->g.V, cudaMemcpyDeviceToHost,
+                                       c->stream));
+            sync(c);
+            if (ref_passes < 0) {
+              ref_q = q;
+              ref_passes = passes;
+              ref_labels = labels;
+            } else {
+              require(q == ref_q && passes == ref_passes && labels == ref_labels, LVG_ERR_STATE,
+                      "autotune: two threshold pairs gave different level-0 results");
+            }
+            continue;
+          }
+          float h = 0.0f;
+          for (size_t p = 1; p < c->move_pass_ms.size(); ++p) h += c->move_pass_ms[p];
+          ms.push_back(h);
+        }
+        std::sort(ms.begin(), ms.end());
+        pt.move_ms = ms[ms.size() / 2];
+        pts.push_back(pt);
       }
-      std::sort(ms.begin(), ms.end());
-      pt.move_ms = ms[ms.size() / 2];
-      pts.push_back(pt);
+    } catch (...) {
+      // leave the context built with the pair it had before the call
+      set_tuning(c, pref_tile, pref_block);
+      try {
+        reset_to_level0(c);
+      } catch (...) {
+      }
+      throw;
     }
     int32_t bi = -1;
     lvg_tune_pick(pts.data(), (int32_t)pts.size(), pref_tile, pref_block, &bi);
