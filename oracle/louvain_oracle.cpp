@@ -28,6 +28,59 @@
 namespace {
 
 double tree_sum(const double* x, int64_t n);
+template <typename T>
+double tree_sum_of(const T* x, int64_t n);
+
+// One entry of a source-grouped list: neighbour (or coarse target) and weight.
+struct Ent {
+  int32_t c;
+  float w;
+};
+inline bool ent_less(const Ent& x, const Ent& y) { return x.c < y.c; }
+
+// Stable counting sort of items 0..n-1 by key(i) in [0, K): bucket k receives
+// its items in index order at positions [off[k], off[k+1]), put(pos, i) writes
+// one.  Threads count and place contiguous index ranges; a thread's items of a
+// bucket go after those of every lower-ranked thread, so the order is the
+// same as one thread's.
+template <typename KeyF, typename PutF>
+void stable_scatter(int64_t n, int32_t K, KeyF key, PutF put, std::vector<int64_t>& off) {
+  off.assign((size_t)K + 1, 0);
+  int want = n < (1 << 16) ? 1 : std::min(omp_get_max_threads(), 32);
+  std::unique_ptr<int64_t[]> cnt;
+  int nth = 1;
+#pragma omp parallel num_threads(want)
+  {
+#pragma omp single
+    {
+      nth = omp_get_num_threads();
+      cnt.reset(new int64_t[(size_t)nth * (size_t)K + 1]);
+    }
+    const int t = omp_get_thread_num();
+    const int64_t lo = n * t / nth, hi = n * (t + 1) / nth;
+    int64_t* c = cnt.get() + (size_t)t * (size_t)K;
+    std::fill(c, c + K, (int64_t)0);
+    for (int64_t i = lo; i < hi; ++i) c[key(i)]++;
+#pragma omp barrier
+#pragma omp for schedule(static)
+    for (int32_t k = 0; k < K; ++k) {
+      int64_t run = 0;
+      for (int tt = 0; tt < nth; ++tt) {
+        int64_t& x = cnt[(size_t)tt * (size_t)K + k];
+        const int64_t v = x;
+        x = run;
+        run += v;
+      }
+      off[(size_t)k + 1] = run;
+    }
+#pragma omp single
+    for (int32_t k = 0; k < K; ++k) off[(size_t)k + 1] += off[k];
+    for (int64_t i = lo; i < hi; ++i) {
+      const int32_t k = key(i);
+      put(off[k] + c[k]++, i);
+    }
+  }
+}
 
 struct Csr {
   int32_t V = 0;
@@ -49,24 +102,23 @@ struct Csr {
 // weight of every distinct non-loop neighbour.
 Csr* build_csr(int32_t V, int64_t E, const int32_t* src, const int32_t* dst, const float* w) {
   if (V < 0 || E < 0) return nullptr;
+  bool bad = false;
+#pragma omp parallel for schedule(static) reduction(|| : bad)
   for (int64_t e = 0; e < E; ++e) {
-    if (src[e] < 0 || src[e] >= V || dst[e] < 0 || dst[e] >= V) return nullptr;
-    if (!(w[e] >= 0.0f) || std::isinf(w[e])) return nullptr;
+    if (src[e] < 0 || src[e] >= V || dst[e] < 0 || dst[e] >= V) bad = true;
+    if (!(w[e] >= 0.0f) || std::isinf(w[e])) bad = true;
   }
+  if (bad) return nullptr;
   auto* g = new Csr();
   g->V = V;
-  {  // m = sum of weights (NeighbourCompute.cu:46) on the fixed tree
-    std::vector<double> wd(w, w + E);
-    g->m = tree_sum(wd.data(), E);
-  }
-  // stable counting sort of D by source
-  std::vector<int64_t> roff(V + 1, 0);
-  for (int64_t e = 0; e < E; ++e) { roff[src[e] + 1]++; roff[dst[e] + 1]++; }
-  for (int32_t i = 0; i < V; ++i) roff[i + 1] += roff[i];
-  std::vector<int64_t> cur(roff.begin(), roff.end() - 1);
-  std::vector<std::pair<int32_t, float>> D(2 * E);
-  for (int64_t e = 0; e < E; ++e) D[cur[src[e]]++] = {dst[e], w[e]};
-  for (int64_t e = 0; e < E; ++e) D[cur[dst[e]]++] = {src[e], w[e]};
+  g->m = tree_sum_of(w, E);   // m = sum of weights (NeighbourCompute.cu:46) on the fixed tree
+  // stable counting sort of D by source: D-order index d < E is input entry d,
+  // d >= E the reversed copy of entry d - E
+  std::vector<int64_t> roff;
+  std::unique_ptr<Ent[]> D(new Ent[2 * E]);   // uninitialised: the scattering threads touch it first
+  stable_scatter(
+      2 * E, V, [&](int64_t d) { return d < E ? src[d] : dst[d - E]; },
+      [&](int64_t pos, int64_t d) { D[pos] = d < E ? Ent{dst[d], w[d]} : Ent{src[d - E], w[d - E]}; }, roff);
   g->k.assign(V, 0.0);
   g->kf32.assign(V, 0.0f);
   g->loopw.assign(V, 0.0f);
@@ -75,20 +127,19 @@ Csr* build_csr(int32_t V, int64_t E, const int32_t* src, const int32_t* dst, con
   std::vector<int64_t> cnt(V + 1, 0);
 #pragma omp parallel for schedule(dynamic, 256)
   for (int32_t i = 0; i < V; ++i) {
-    auto b = D.begin() + roff[i], e = D.begin() + roff[i + 1];
-    std::stable_sort(b, e, [](const std::pair<int32_t, float>& x, const std::pair<int32_t, float>& y) {
-      return x.first < y.first;
-    });
+    Ent* b = D.get() + roff[i];
+    Ent* e = D.get() + roff[i + 1];
+    std::stable_sort(b, e, ent_less);
     double kd = 0.0;
     float kf = 0.0f;
     int64_t distinct = 0;
-    for (auto it = b; it != e; ++it) {
-      float v = it->second == 0.0f ? 1.0f : it->second;   // InitKernel.cu:165-167
-      if (it->first == i) v *= 2.0f;                         // InitKernel.cu:169-170
+    for (Ent* it = b; it != e; ++it) {
+      float v = it->w == 0.0f ? 1.0f : it->w;   // InitKernel.cu:165-167
+      if (it->c == i) v *= 2.0f;                 // InitKernel.cu:169-170
       kd += (double)v;
       kf += v;
-      if (it->first == i) { g->loopw[i] = it->second; g->has_loop[i] = 1; }
-      else if (it == b || (it - 1)->first != it->first) distinct++;
+      if (it->c == i) { g->loopw[i] = it->w; g->has_loop[i] = 1; }
+      else if (it == b || (it - 1)->c != it->c) distinct++;
     }
     g->k[i] = kd;
     g->kf32[i] = kf;
@@ -105,10 +156,10 @@ Csr* build_csr(int32_t V, int64_t E, const int32_t* src, const int32_t* dst, con
     int64_t o = g->off[i];
     int64_t p = roff[i], q = roff[i + 1];
     while (p < q) {
-      int32_t j = D[p].first;
+      int32_t j = D[p].c;
       double s = 0.0;
       int64_t r = p;
-      while (r < q && D[r].first == j) s += (double)D[r++].second;
+      while (r < q && D[r].c == j) s += (double)D[r++].w;
       if (j != i) { g->col[o] = j; g->w[o] = (float)s; ++o; }
       p = r;
     }
@@ -129,13 +180,14 @@ double tree32(const double* v, int n) {
     for (int l = 0; l < o; ++l) s[l] = s[l] + s[l + o];
   return s[0];
 }
-double group_sum(const double* x, int64_t n) {
+template <typename T>
+double group_sum(const T* x, int64_t n) {  // values are widened to double as read
   double ts[256];
   for (int t = 0; t < 256; ++t) {
     double s = 0.0;
     for (int j = 0; j < 8; ++j) {
       int64_t idx = (int64_t)j * 256 + t;
-      if (idx < n) s = s + x[idx];
+      if (idx < n) s = s + (double)x[idx];
     }
     ts[t] = s;
   }
@@ -143,18 +195,23 @@ double group_sum(const double* x, int64_t n) {
   for (int wi = 0; wi < 8; ++wi) ws[wi] = tree32(ts + wi * 32, 32);
   return tree32(ws, 8);
 }
-double tree_sum(const double* x, int64_t n) {
+template <typename T>
+double tree_sum_of(const T* x, int64_t n) {
   if (n <= 0) return 0.0;
-  std::vector<double> cur(x, x + n), nxt;
-  do {
+  const int64_t nb0 = (n + 2047) / 2048;
+  std::vector<double> cur(nb0), nxt;
+#pragma omp parallel for schedule(static) if (nb0 >= 64)
+  for (int64_t b = 0; b < nb0; ++b) cur[b] = group_sum(x + b * 2048, std::min<int64_t>(2048, n - b * 2048));
+  while (cur.size() > 1) {
     int64_t nn = (int64_t)cur.size();
     int64_t nb = (nn + 2047) / 2048;
     nxt.assign(nb, 0.0);
     for (int64_t b = 0; b < nb; ++b) nxt[b] = group_sum(cur.data() + b * 2048, std::min<int64_t>(2048, nn - b * 2048));
     cur.swap(nxt);
-  } while (cur.size() > 1);
+  }
   return cur[0];
 }
+double tree_sum(const double* x, int64_t n) { return tree_sum_of(x, n); }
 
 double q_terms_fp64(const double* tot, const double* in, int32_t n, double m) {
   // OneLevelKernel.cu:427-451 in FP64: in/m - (tot/2m)^2, zero when m == 0.
@@ -381,26 +438,39 @@ void induce(int64_t E, const int32_t* src, const int32_t* dst, const float* w, c
             int32_t C, Edges& out) {
   // InducedGraphKernel.cu:28-113: map both endpoints, weight 0 -> 1, sort by
   // (cu, cv) and sum the weights of equal keys (FP64 sum, rounded once).
-  std::vector<int64_t> cnt((size_t)C + 1, 0);
-  for (int64_t e = 0; e < E; ++e) cnt[part[src[e]] + 1]++;
-  for (int32_t c = 0; c < C; ++c) cnt[c + 1] += cnt[c];
-  std::vector<int64_t> cur(cnt.begin(), cnt.end() - 1);
-  std::vector<std::pair<int32_t, float>> R(E);
-  for (int64_t e = 0; e < E; ++e) {
-    float x = w[e] == 0.0f ? 1.0f : w[e];
-    R[cur[part[src[e]]]++] = {part[dst[e]], x};
-  }
-  out.s.clear(); out.t.clear(); out.w.clear();
+  // Entries grouped by cu in input order, then each group sorted stably by
+  // cv; groups are independent, so they sort and sum in parallel and write
+  // their distinct keys at offsets from a scan of the per-group counts.
+  std::vector<int64_t> cnt;
+  std::unique_ptr<Ent[]> R(new Ent[E]);
+  stable_scatter(
+      E, C, [&](int64_t e) { return part[src[e]]; },
+      [&](int64_t pos, int64_t e) { R[pos] = Ent{part[dst[e]], w[e] == 0.0f ? 1.0f : w[e]}; }, cnt);
+  std::vector<int64_t> dcnt((size_t)C + 1, 0);
+#pragma omp parallel for schedule(dynamic, 64)
   for (int32_t a = 0; a < C; ++a) {
-    auto b = R.begin() + cnt[a], e = R.begin() + cnt[a + 1];
-    std::stable_sort(b, e, [](const std::pair<int32_t, float>& x, const std::pair<int32_t, float>& y) {
-      return x.first < y.first;
-    });
-    for (auto it = b; it != e;) {
-      int32_t v = it->first;
+    Ent* b = R.get() + cnt[a];
+    Ent* e = R.get() + cnt[a + 1];
+    std::stable_sort(b, e, ent_less);
+    int64_t d = 0;
+    for (Ent* it = b; it != e; ++it)
+      if (it == b || (it - 1)->c != it->c) ++d;
+    dcnt[(size_t)a + 1] = d;
+  }
+  for (int32_t a = 0; a < C; ++a) dcnt[(size_t)a + 1] += dcnt[a];
+  const int64_t n_out = dcnt[C];
+  out.s.assign(n_out, 0); out.t.assign(n_out, 0); out.w.assign(n_out, 0.0f);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int32_t a = 0; a < C; ++a) {
+    int64_t o = dcnt[a];
+    const Ent* b = R.get() + cnt[a];
+    const Ent* e = R.get() + cnt[a + 1];
+    for (const Ent* it = b; it != e;) {
+      int32_t v = it->c;
       double s = 0.0;
-      while (it != e && it->first == v) { s += (double)it->second; ++it; }
-      out.s.push_back(a); out.t.push_back(v); out.w.push_back((float)s);
+      while (it != e && it->c == v) { s += (double)it->w; ++it; }
+      out.s[o] = a; out.t[o] = v; out.w[o] = (float)s;
+      ++o;
     }
   }
 }
