@@ -38,6 +38,22 @@ struct Ent {
 };
 inline bool ent_less(const Ent& x, const Ent& y) { return x.c < y.c; }
 
+// Stable sort by c.  Short runs take an insertion sort in place (no buffer
+// allocation per run); a stable sort's result is unique, so both give the
+// same order.
+inline void stable_sort_ents(Ent* b, Ent* e) {
+  if (e - b > 48) {
+    std::stable_sort(b, e, ent_less);
+    return;
+  }
+  for (Ent* i = b + 1; i < e; ++i) {
+    Ent x = *i;
+    Ent* j = i;
+    for (; j > b && x.c < (j - 1)->c; --j) *j = *(j - 1);
+    *j = x;
+  }
+}
+
 // Stable counting sort of items 0..n-1 by key(i) in [0, K): bucket k receives
 // its items in index order at positions [off[k], off[k+1]), put(pos, i) writes
 // one.  Threads count and place contiguous index ranges; a thread's items of a
@@ -129,7 +145,7 @@ Csr* build_csr(int32_t V, int64_t E, const int32_t* src, const int32_t* dst, con
   for (int32_t i = 0; i < V; ++i) {
     Ent* b = D.get() + roff[i];
     Ent* e = D.get() + roff[i + 1];
-    std::stable_sort(b, e, ent_less);
+    stable_sort_ents(b, e);
     double kd = 0.0;
     float kf = 0.0f;
     int64_t distinct = 0;
@@ -451,7 +467,7 @@ void induce(int64_t E, const int32_t* src, const int32_t* dst, const float* w, c
   for (int32_t a = 0; a < C; ++a) {
     Ent* b = R.get() + cnt[a];
     Ent* e = R.get() + cnt[a + 1];
-    std::stable_sort(b, e, ent_less);
+    stable_sort_ents(b, e);
     int64_t d = 0;
     for (Ent* it = b; it != e; ++it)
       if (it == b || (it - 1)->c != it->c) ++d;
