@@ -186,3 +186,33 @@ def test_hand_graph_known_answers(oracle):
     assert r.final.tolist() == [i // 5 for i in range(40)]
     r = oracle.Run(*hand_graph("path"))
     assert len(r.levels) >= 1 and r.final.max() < 12
+
+
+def test_results_do_not_depend_on_thread_count(oracle):
+    """The CSR build and the coarsening sort per thread; a shuffled list with
+    repeated (src, dst) entries and fractional weights of wide range makes
+    the summation order visible, so every output is compared bit for bit."""
+    rng = np.random.default_rng(12)
+    n, m = 3000, 150000
+    s = rng.integers(0, n, m).astype(np.int32)
+    d = rng.integers(0, n, m).astype(np.int32)
+    w = (rng.random(m) * 3.7 + 1e-3).astype(np.float32)
+    w[::7] *= 1e5
+    runs = {}
+    for th in (1, 3, 8):
+        runs[th] = oracle.Run(n, s, d, w, n_threads=th)
+    part = rng.integers(0, 400, n).astype(np.int32)
+    ind = oracle.induce(n, s, d, w, part)
+    for th in (3, 8):
+        a, b = runs[1], runs[th]
+        assert len(a.levels) == len(b.levels)
+        for la, lb in zip(a.levels, b.levels):
+            assert (la.nnz, la.n_comms, la.passes) == (lb.nnz, lb.n_comms, lb.passes)
+            assert la.q.hex() == lb.q.hex() and la.q_start.hex() == lb.q_start.hex()
+            np.testing.assert_array_equal(la.labels, lb.labels)
+        np.testing.assert_array_equal(a.final, b.final)
+    # `ind` ran on the thread count the last Run set (8); now one thread
+    oracle.Run(n, s[:10], d[:10], w[:10], n_threads=1)
+    ind8, ind1 = ind, oracle.induce(n, s, d, w, part)
+    for x, y in zip(ind1, ind8):
+        assert x.tobytes() == y.tobytes()
