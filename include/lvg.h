@@ -260,6 +260,7 @@ lvg_status lvg_server_drain(lvg_server* srv, int64_t timeout_ms);
 /* Counters: submitted, completed, batched runs, device bytes reserved. */
 lvg_status lvg_server_stats(lvg_server* srv, int64_t* submitted, int64_t* completed, int64_t* batches,
                             int64_t* reserved_bytes);
+/* Last error message of the server (a copy, valid until this thread's next call). */
 const char* lvg_server_last_error(const lvg_server* srv);
 /* Stops the workers after the queue is empty and frees every slot. */
 lvg_status lvg_server_destroy(lvg_server* srv);

@@ -329,7 +329,15 @@ lvg_status lvg_server_stats(lvg_server* S, int64_t* submitted, int64_t* complete
   return LVG_OK;
 }
 
-const char* lvg_server_last_error(const lvg_server* S) { return S ? S->err.c_str() : "null server"; }
+// Workers write the message under the lock; the caller gets a copy that stays
+// valid until its own thread's next call.
+const char* lvg_server_last_error(const lvg_server* S) {
+  if (!S) return "null server";
+  static thread_local std::string copy;
+  std::lock_guard<std::mutex> lk(const_cast<lvg_server*>(S)->mu);
+  copy = S->err;
+  return copy.c_str();
+}
 
 lvg_status lvg_server_destroy(lvg_server* S) {
   if (!S) return LVG_ERR_INVALID_ARG;
