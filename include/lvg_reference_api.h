@@ -278,12 +278,13 @@ inline Partition partitionAtLevel(std::vector<Partition>& dendogram, int level) 
   return out;
 }
 
-/* getPartitions (LouvainCPP.cpp:108-114).  The reference evaluates
- * `level || dendogram.size() - 1`, a bool, so it always returns level 1 when
- * there are two or more levels; reference_quirk = true keeps that behaviour,
- * false returns the requested level (the last level for level < 0). */
+/* getPartitions (LouvainCPP.cpp:108-114).  The reference rejects a level
+ * outside [0, size-1], then evaluates `level || dendogram.size() - 1`, a
+ * bool, so it always returns level 1 when there are two or more levels;
+ * reference_quirk = true keeps both behaviours, false returns the requested
+ * level (the last level for level < 0). */
 inline Partition getPartitions(std::vector<Partition>& dendogram, int level = 0, bool reference_quirk = true) {
-  if (level >= (int)dendogram.size())
+  if (level >= (int)dendogram.size() || (reference_quirk && level < 0))
     throw Error(LVG_ERR_INVALID_ARG, "Invalid argument: level is not between 1 and len(dendogram) - 1 included.");
   if (reference_quirk) return partitionAtLevel(dendogram, (level != 0 || dendogram.size() - 1 != 0) ? 1 : 0);
   return partitionAtLevel(dendogram, level < 0 ? (int)dendogram.size() - 1 : level);
@@ -296,7 +297,9 @@ inline int countPartitions(const Partition& p) {
   return 1 + mx;
 }
 
-/* loadNodes (LouvainCPP.cpp:660-701): "count id id id ..." */
+/* loadNodes (LouvainCPP.cpp:660-701): "count id id id ...".  Every value is
+ * read; the reference's read-then-test-eof loop also drops the last value of a
+ * file that does not end in whitespace, which this loader does not copy. */
 inline std::vector<int> loadNodes(const std::string& path = "nodes.txt") {
   std::ifstream f(path);
   if (!f) throw Error(LVG_ERR_INVALID_ARG, "cannot open " + path);
@@ -309,7 +312,8 @@ inline std::vector<int> loadNodes(const std::string& path = "nodes.txt") {
   return ids;
 }
 
-/* loadEdges (LouvainCPP.cpp:703-737): "count src tgt w src tgt w ..." */
+/* loadEdges (LouvainCPP.cpp:703-737): "count src tgt w src tgt w ...", read
+ * the same way as loadNodes. */
 inline std::vector<Edge> loadEdges(const std::string& path = "edges.txt") {
   std::ifstream f(path);
   if (!f) throw Error(LVG_ERR_INVALID_ARG, "cannot open " + path);

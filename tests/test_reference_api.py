@@ -59,6 +59,22 @@ def test_loaders_and_shim_header_self_contained(tmp_path):
     subprocess.check_call([cxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(f)])
 
 
+def test_shim_host_logic_known_answers(tmp_path):
+    """partitionAtLevel / getPartitions / countPartitions and the loaders of
+    the shim on hand-worked dendrograms and files (no device call)."""
+    from louvaingpu_b200 import build
+    build.build_lvg()
+    exe = str(tmp_path / "shim_host_check")
+    libdir = os.path.join(ROOT, "louvaingpu_b200")
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    subprocess.check_call([cxx, "-std=c++17", "-O1", "-Wall", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "cpp", "shim_host_check.cpp"), "-L", libdir, "-llvg",
+                           f"-Wl,-rpath,{libdir}", "-o", exe])
+    r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip() == "ok"
+
+
 @pytest.mark.gpu
 def test_reference_driver_run_and_steps(tmp_path, oracle, gen):
     n, s, d, w = gen.sbm(1500, 15, 0.06, 0.003, 1, 3, seed=9)
