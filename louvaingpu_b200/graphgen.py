@@ -86,13 +86,20 @@ def rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, w_lo=1, w_hi=16, seed=2)
 def batched_sbm_params(count, seed=3, n_lo=64, n_hi=200000):
     """Per-graph SBM parameters of the batched shape: n log-uniform in
     [n_lo, n_hi], 4-400 blocks, average degree uniform in [8, 32], 70% intra
-    edges, integer weights 1..4."""
+    edges, integer weights 1..4.
+
+    The block count drawn in [4, 400] is capped so that a block holds at least
+    0.7 d + 1 vertices: then 70 % of the degree fits inside the block
+    (p_in <= 1).  Graphs too small for 4 such blocks (n < 4 (0.7 d + 1), at
+    most 94 vertices) keep 4 blocks and take p_in = 1, below the target."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
         n = int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
-        blocks = int(min(rng.integers(4, 401), max(1, n // 4)))
+        drawn = int(rng.integers(4, 401))
         d = float(rng.uniform(8, 32))
+        cap = int(n // (0.7 * d + 1.0))
+        blocks = max(min(4, max(1, n // 4)), min(drawn, cap))
         s = n / blocks
         p_in = min(1.0, 0.7 * d / max(s - 1, 1))
         p_out = min(1.0, 0.3 * d / max(n - s, 1))
