@@ -301,3 +301,28 @@ def test_pass_cap_reports_not_converged(Louvain, gen):
         with pytest.raises(LvgError) as e:
             lv.run()
         assert e.value.status == 4
+
+
+@pytest.mark.parametrize("name", ["lfr_seed1.json", "rmat16_seed2.json"])
+def test_committed_workload_fixtures(Louvain, gen, name):
+    """The CUDA path reproduces the committed fixtures of the LFR n=2^20 and
+    R-MAT 16 graphs (tests/golden/make_workload_goldens.py): level sizes,
+    passes, community counts and per-level Q bit for bit, the final partition
+    by its hash, and the final FP64 Q within the tolerance of the other tests."""
+    import hashlib
+    with open(os.path.join(GOLDEN, name)) as f:
+        g = json.load(f)
+    n, s, d, w = gen.lfr() if name.startswith("lfr") else gen.rmat(16)
+    assert (n, len(s)) == (g["n_vertices"], g["n_entries"])
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        res = lv.run()
+        assert res.n_levels == len(g["levels"])
+        for l, x in enumerate(g["levels"]):
+            li = lv.level_info(l)
+            assert (li.n_vertices, li.nnz, li.passes, li.n_comms) == \
+                   (x["n_vertices"], x["nnz"], x["passes"], x["n_comms"]), f"level {l}"
+            assert li.q_start.hex() == x["q_start"] and li.q_level.hex() == x["q_level"], f"level {l}"
+        part = np.ascontiguousarray(lv.partition(), np.int32)
+        assert hashlib.sha256(part.tobytes()).hexdigest() == g["final_partition_sha256"]
+        assert res.q_final == pytest.approx(float.fromhex(g["final_modularity_fp64"]), abs=1e-9)

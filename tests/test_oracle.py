@@ -216,3 +216,28 @@ def test_results_do_not_depend_on_thread_count(oracle):
     ind8, ind1 = ind, oracle.induce(n, s, d, w, part)
     for x, y in zip(ind1, ind8):
         assert x.tobytes() == y.tobytes()
+
+
+def _golden_sha(*arrays):
+    import hashlib
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+@pytest.mark.parametrize("name,make", [("lfr_seed1.json", "lfr"), ("rmat16_seed2.json", "rmat16")])
+def test_workload_golden_regression(oracle, gen, name, make):
+    """The generators and the oracle reproduce the committed fixtures of the
+    LFR n=2^20 and R-MAT 16 graphs bit for bit (make_workload_goldens.py)."""
+    g = load_golden(name)
+    n, s, d, w = gen.lfr() if make == "lfr" else gen.rmat(16)
+    assert (n, len(s)) == (g["n_vertices"], g["n_entries"])
+    assert _golden_sha(s, d, w) == g["input_sha256"]
+    r = oracle.Run(n, s, d, w)
+    assert len(r.levels) == len(g["levels"])
+    for lv, x in zip(r.levels, g["levels"]):
+        assert (lv.n_vertices, lv.nnz, lv.passes, lv.n_comms) == (x["n_vertices"], x["nnz"], x["passes"], x["n_comms"])
+        assert lv.q_start.hex() == x["q_start"] and lv.q.hex() == x["q_level"]
+    assert _golden_sha(r.final.astype(np.int32)) == g["final_partition_sha256"]
+    assert oracle.modularity_fp64(n, s, d, w, r.final).hex() == g["final_modularity_fp64"]
