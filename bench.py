@@ -1,18 +1,28 @@
 """Benchmark of the Louvain hot path: edges/s per Louvain pass.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload lfr|sbm10k|rmat<scale>|batched|serving]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rmat25|lfr|sbm10k|rmat<scale>|batched|serving]
                     [--impl ours|reference] [--graphs G]
 
-Workload (default): the LFR-style graph n = 2^20 (power-law degrees, exponent
-2.5 on [5, 5000]; community sizes exponent 1.5 on [50, 50000]; mu = 0.3; unit
-weights; seed 1) -- synthetic, seeded, generated on the host.
+Workload (default): the R-MAT graph of scale 25 (33,554,432 vertices, edge
+factor 16, (a,b,c,d) = (0.57, 0.19, 0.19, 0.05), self loops dropped,
+duplicates merged by summing weights, integer weights 1..16, seed 2;
+1,047,217,118 symmetric entries) -- synthetic, seeded; generated on the
+device for the GPU arm and by the same generator on the host for the
+reference arm (the two are equal entry for entry).
 
-One step (value) = the level-0 one-level phase (all move passes from the
-singleton state, ΔQ test, commit and isolated-vertex merge) on the
-device-resident CSR.  value = CSR entries x passes / step time.
-e2e = one whole dendrogram run through the C ABI from pinned host buffers:
-H2D of the edge list, CSR build, every level, final FP64 modularity and D2H of
-the partition; e2e value = sum over levels of CSR entries x passes / run time.
+One step (value) = the move passes of the level-0 one-level phase: both
+passes (the singleton pass and the hashing pass), the ΔQ test, commit and
+isolated-vertex merge on the device-resident CSR.  value = CSR entries x
+passes / step time.  e2e = one whole dendrogram run through the C ABI from
+pinned host buffers: H2D of the edge list, CSR build, every level, final FP64
+modularity and D2H of the partition; e2e value = sum over levels of CSR
+entries x passes / run time.
+
+--impl reference times the oracle (the CPU restatement of the reference's
+method) on the same graph and the same two passes, on all host cores: each
+step decides a bounded sample of the vertices (every 8th vertex, a different
+eighth per step) from the singleton state and from the state after a full
+first pass; value = sampled CSR entries x 2 / decision time.
 
 With --gpus N each rank runs an independent replica (the path does not shard
 within one graph); value is the sum over ranks of entries processed divided by
@@ -33,7 +43,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "edges/s per Louvain pass"
 DEVICE_GEN_SCALE = 20     # R-MAT graphs this large are generated on the device
-CPU_SAMPLE_RMAT_SCALE = 20  # the CPU baseline of larger R-MAT graphs runs on this scale
 UNIT = "edges/s"
 
 
@@ -42,7 +51,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="lfr")
+    ap.add_argument("--workload", default="rmat25")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
@@ -60,7 +69,10 @@ def parse():
     return ap.parse_args()
 
 
-def make_graph(workload):
+def make_graph(workload, host=False):
+    """(n, src, dst, w, config description, level gain threshold) of a plain
+    workload; R-MAT graphs of scale >= DEVICE_GEN_SCALE are generated on the
+    device unless `host` (the reference arm, which runs no device code)."""
     from louvaingpu_b200 import graphgen
     if workload == "lfr":
         n, s, d, w = graphgen.lfr()
@@ -74,7 +86,7 @@ def make_graph(workload):
         return n, s, d, w, desc, 1e-6
     if workload.startswith("rmat"):
         scale = int(workload[4:])
-        if scale >= DEVICE_GEN_SCALE:
+        if scale >= DEVICE_GEN_SCALE and not host:
             # generated on the device (equal to the host generator), copied back once
             dg = graphgen.rmat_device(scale)
             n = dg.n_vertices
@@ -198,10 +210,49 @@ def phase_roofline(levels, peak):
     return out
 
 
-def cpu_baseline(n, s, d, w, level_min, threads):
-    from oracle import oracle as O
-    r = O.Run(n, s, d, w, level_min_gain=level_min, n_threads=threads)
-    return r.pass_entries / r.seconds, r.seconds
+SAMPLE_STRIDE = 8        # CPU legs: every 8th vertex per step
+STEP = "move passes of the level-0 one-level phase (singleton pass + hashing pass)"
+
+
+class CpuPassSample:
+    """The two level-0 move passes run by the oracle (the CPU restatement of
+    the reference's method, OneLevelKernel.cu:248-422) on the workload graph,
+    over a bounded sample per step: the vertices i with i % 8 == step % 8
+    (every eighth vertex, a different eighth each step), decided from the
+    singleton state (pass 1) and from the state after a full first pass
+    (pass 2), as the one-level phase runs them.  The full first pass that
+    sets up pass 2 runs once, untimed."""
+
+    def __init__(self, n, s, d, w, threads):
+        from oracle import oracle as O
+        self.threads = threads
+        self.c = O.Csr(n, s, d, w, arrays=False)
+        V = self.c.V
+        self.deg = np.diff(self.c.off)
+        self.state0 = (np.arange(V, dtype=np.int32), self.c.k, np.ones(V, np.int32))
+        nxt = self.c.decide(*self.state0, n_threads=threads)[0]
+        tot = np.bincount(nxt, weights=self.c.k, minlength=V)   # integral weights: exact in any order
+        self.state1 = (nxt, tot, np.bincount(nxt, minlength=V).astype(np.int32))
+
+    def step(self, k):
+        """(entries decided, seconds) of one step: both passes over sample k."""
+        verts = np.arange(k % SAMPLE_STRIDE, self.c.V, SAMPLE_STRIDE, dtype=np.int32)
+        t1, _ = self.c.decide_subset(*self.state0, verts, n_threads=self.threads)
+        t2, _ = self.c.decide_subset(*self.state1, verts, n_threads=self.threads)
+        return 2 * int(self.deg[verts].sum()), t1 + t2
+
+    def sample_text(self, steps):
+        return (f"{steps} steps, each both level-0 move passes of the oracle over every {SAMPLE_STRIDE}th vertex "
+                f"of the workload graph (a different eighth per step), decision time only")
+
+
+def plain_config(desc, E, nnz, V, gpus):
+    """config of the plain workloads, the same in both arms."""
+    mb = (12.0 * nnz + 24.0 * V) / 1e6
+    l2 = ("inputs larger than L2 (move pass touches %.0f MB)" % mb if mb > 126.0 else
+          "inputs fit in L2 (move pass touches %.1f MB; no flush between steps)" % mb)
+    return dict(desc, n_entries=E, csr_entries=nnz, parallelism="replicas" if gpus > 1 else "single", step=STEP,
+                l2=l2)
 
 
 def max_over_ranks(values, pg):
@@ -236,31 +287,33 @@ def dist_setup(args):
 
 
 def run_reference(args, world, rank, pg):
-    """Reference arm: the CPU restatement of the reference's method on all host cores."""
+    """Reference arm: the CPU restatement of the reference's method (the
+    reference has no CPU Louvain and its GPU code cannot be built here) on all
+    host cores, on the same graph and the same two level-0 passes as the GPU
+    arm, over a bounded vertex sample per step (CpuPassSample)."""
     if rank != 0:
         return
-    n, s, d, w, desc, level_min = make_graph(args.workload)
+    n, s, d, w, desc, level_min = make_graph(args.workload, host=True)
+    E = len(s)
     threads = os.cpu_count() or 1
-    from oracle import oracle as O
-    for _ in range(args.warmup):
-        O.Run(n, s, d, w, level_min_gain=level_min, n_threads=threads)
-    # each step is timed inside the library (the whole dendrogram run), as the
-    # cpu_baseline leg does; the binding's copies of every level's results are
-    # not part of the method
+    cs = CpuPassSample(n, s, d, w, threads)
+    del s, d, w
+    for k in range(args.warmup):
+        cs.step(k)
     entries, t = 0, 0.0
-    for _ in range(args.steps):
-        r = O.Run(n, s, d, w, level_min_gain=level_min, n_threads=threads)
-        entries += r.pass_entries
-        t += r.seconds
+    for k in range(args.steps):
+        e, secs = cs.step(args.warmup + k)
+        entries += e
+        t += secs
     v = entries / t
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-        "config": dict(desc, parallelism="replicas", step="whole dendrogram run"),
+        "config": plain_config(desc, E, cs.c.nnz, cs.c.V, args.gpus),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} whole runs of the workload (CPU restatement of the reference "
-                                   f"method; the reference's own GPU code cannot be built here)"},
+                         "sample": cs.sample_text(args.steps) + " (CPU restatement of the reference method; the "
+                                   "reference's own GPU code cannot be built here)"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -329,12 +382,16 @@ def run_ours(args, world, rank, local, pg):
     b_pass = 12.0 * nnz + 24.0 * V
     t_move = move_ms / max(move_passes, 1) / 1e3
     achieved = b_pass / t_move / 1e9 if t_move > 0 else 0.0
+    by_pass = [float(np.median([x[k] for x in per_pass if len(x) > k])) for k in range(max(len(x) for x in per_pass))]
+    names = ["singleton (table-free) kernels", "hashing kernels"]
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_kind, "traffic": profiled_traffic(args.workload),
-            "kernel": "move kernels of one pass (all degree buckets)", "algorithmic_bytes": b_pass,
-            "move_ms_per_pass": t_move * 1e3,
-            "move_ms_by_pass": [round(float(np.median([x[k] for x in per_pass if len(x) > k])), 4)
-                                for k in range(max(len(x) for x in per_pass))]}
+            "kernel": "move kernels of one pass (all degree classes), mean over the step's passes",
+            "algorithmic_bytes": b_pass, "move_ms_per_pass": t_move * 1e3,
+            "passes": [{"pass": k + 1, "kernels": names[min(k, 1)], "ms": round(ms, 4),
+                        "achieved": round(b_pass / (ms * 1e-3) / 1e9, 1) if ms > 0 else 0.0,
+                        "frac": round(b_pass / (ms * 1e-3) / 1e9 / peak, 4) if ms > 0 else 0.0}
+                       for k, ms in enumerate(by_pass)]}
     del lv, ds, dd, dw
     torch.cuda.empty_cache()
     # ---------------------------------------------------------------- e2e
@@ -388,29 +445,18 @@ def run_ours(args, world, rank, local, pg):
     cpu = None
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        if args.workload.startswith("rmat") and int(args.workload[4:]) > CPU_SAMPLE_RMAT_SCALE:
-            from louvaingpu_b200 import graphgen
-            del s, d, w, hs, hd, hw
-            cn, cs, cd, cw = graphgen.rmat(CPU_SAMPLE_RMAT_SCALE)
-            v, secs = cpu_baseline(cn, cs, cd, cw, level_min, threads)
-            sample = f"one whole dendrogram run of R-MAT scale {CPU_SAMPLE_RMAT_SCALE} (same generator; {secs:.1f} s)"
-        else:
-            v, secs = cpu_baseline(n, s, d, w, level_min, threads)
-            sample = f"one whole dendrogram run of the workload ({secs:.1f} s)"
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
-        from louvaingpu_b200 import graphgen
-        sn, ss_, sd_, sw_ = graphgen.sbm_10k(seed=0)
-        v1, secs1 = cpu_baseline(sn, ss_, sd_, sw_, 1e-6, 1)
-        cpu["single_thread"] = {"value": v1, "unit": UNIT, "cores": 1,
-                                "sample": f"one whole run of the SBM 10k config, one thread ({secs1:.2f} s)"}
+        del hs, hd, hw
+        cs = CpuPassSample(n, s, d, w, threads)
+        e, secs = cs.step(0)
+        cpu = {"value": e / secs, "unit": UNIT, "cores": threads, "kind": "port", "sample": cs.sample_text(1)}
+        del cs
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-        "config": dict(desc, n_entries=E, csr_entries=nnz, parallelism="replicas" if world > 1 else "single",
-                       step="level-0 one-level phase", passes_per_step=passes_total // args.steps,
-                       thresholds=tune,
-                       l2="inputs larger than L2 (move pass touches %.0f MB)" % (b_pass / 1e6)),
+        "config": plain_config(desc, E, nnz, V, args.gpus),
+        "passes_per_step": passes_total // args.steps,
+        "tuning": tune,
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 12 * E, "d2h_bytes_per_step": 4 * n,

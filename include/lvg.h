@@ -150,6 +150,13 @@ lvg_status lvg_get_csr(const lvg_ctx* ctx, int32_t* n_vertices, int64_t* nnz, do
                        int64_t* off, int32_t* col, float* w, double* k, float* loopw,
                        uint8_t* has_loop);
 
+/* Copy the current level's input list to host buffers (any may be NULL):
+ * src/dst/w of n_entries entries.  After lvg_induce this is the coarse list
+ * inducedGraphCUDA writes (InducedGraphKernel.cu:84-113): one entry per
+ * distinct (community of src, community of dst) key in ascending key order,
+ * weight = sum over the level's entries of (w == 0 ? 1 : w). */
+lvg_status lvg_get_level_edges(const lvg_ctx* ctx, int64_t* n_entries, int32_t* src, int32_t* dst, float* w);
+
 /* Set the committed community state of the current level from host arrays
  * (communities as vertex indices) and recompute its totals; used to drive
  * single passes from a known state. */
@@ -267,27 +274,44 @@ lvg_status lvg_server_destroy(lvg_server* srv);
 
 /* Largest community count lvg_modularity_fp64_noalloc accepts. */
 #define LVG_NOALLOC_MAX_COMMS (1 << 18)
+/* Size of its fixed device array: 3 * 2^18 + 2^18/2048 + 3 = 786,563 doubles
+ * (Kc, Ain and the per-community terms, the tree partials, 2W, Q and a flag). */
+#define LVG_NOALLOC_SCRATCH_BYTES 6292504
 
 /* FP64 Newman modularity of a partition, like lvg_modularity_fp64, for
- * callers that cannot allocate device memory at call time: code running while
- * a stream is captured into a CUDA graph (cudaMalloc/cudaFree are not allowed
- * there), serving loops whose HBM is all held by their own pool, and paths
- * that cannot take the device-wide synchronisation of cudaMalloc/cudaFree.
+ * callers that cannot allocate device memory when they need the value: a
+ * serving process whose caching allocator already holds all free HBM in its
+ * own pool (a cudaMalloc would fail, or force that pool to give memory back),
+ * and latency-bound loops running beside work on other streams, which cannot
+ * take the device-wide synchronisation of cudaMalloc/cudaFree.
  * No counterpart in the reference.
- * Inputs are device pointers: the edge list (n_entries entries) and the
- * community of each vertex, values in [0, n_comms); the result goes to the
- * host double *q.  The call allocates nothing: its scratch is a fixed device
- * array of 3 * LVG_NOALLOC_MAX_COMMS doubles (6 MiB) that every GPU which
- * loads the library holds until the process exits.  n_comms above
- * LVG_NOALLOC_MAX_COMMS returns LVG_ERR_CAPACITY.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress), so make it
- * before any stream capture.  All calls share the array: calls that overlap on
- * the GPU (other streams, other host threads) race and must be serialised by
- * the caller.  The call synchronises `stream` (a cudaStream_t, NULL for the
- * legacy default stream) to return the value. */
+ * Inputs are device pointers: the edge list (n_entries entries, ids that index
+ * d_part) and the community of each vertex, values in [0, n_comms).  An id
+ * outside that range is left out of the sums and the call returns
+ * LVG_ERR_INVALID_ARG.  The result goes to the host double *q.  The call
+ * allocates nothing: its scratch is a fixed device array of
+ * LVG_NOALLOC_SCRATCH_BYTES bytes that every GPU which loads the library holds
+ * until the process exits.  n_comms above LVG_NOALLOC_MAX_COMMS returns
+ * LVG_ERR_CAPACITY.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make it before any stream capture.  All
+ * calls share the array and each call clears what it sums into: calls that
+ * overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller.  The call synchronises `stream` (a cudaStream_t,
+ * NULL for the legacy default stream) before it returns the value. */
 lvg_status lvg_modularity_fp64_noalloc(const int32_t* d_src, const int32_t* d_dst, const float* d_w,
                                        int64_t n_entries, const int32_t* d_part, int32_t n_comms,
                                        void* stream, double* q);
+
+/* Test hook of the failure paths (no counterpart in the reference, whose
+ * sorts are Thrust's and wait on nothing).  The radix sort of the CSR build
+ * and the coarsening finds each tile's offsets by decoupled look-back: a tile
+ * waits for the counts its predecessors publish, for at most spin_limit polls
+ * (default 1 << 22), then sets an error flag and goes on, and the sort returns
+ * LVG_ERR_CUDA ("radix sort look-back did not complete") instead of hanging.
+ * hold_tile >= 0 makes that tile of every later sort never publish, so the
+ * waits of the tiles after it run out; hold_tile = -1 and the default limit
+ * restore normal operation.  Process-wide; for tests only. */
+lvg_status lvg_debug_radix_hold(int32_t spin_limit, int64_t hold_tile);
 
 /* Bytes of device memory the context holds (arena capacity) and its peak use. */
 lvg_status lvg_memory(const lvg_ctx* ctx, int64_t* capacity, int64_t* peak);

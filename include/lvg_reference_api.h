@@ -17,6 +17,9 @@
 #define LVG_REFERENCE_API_H
 
 #include <algorithm>
+#include <cerrno>
+#include <cstdint>
+#include <cstdlib>
 #include <fstream>
 #include <map>
 #include <numeric>
@@ -297,32 +300,70 @@ inline int countPartitions(const Partition& p) {
   return 1 + mx;
 }
 
-/* loadNodes (LouvainCPP.cpp:660-701): "count id id id ...".  Every value is
- * read; the reference's read-then-test-eof loop also drops the last value of a
- * file that does not end in whitespace, which this loader does not copy. */
-inline std::vector<int> loadNodes(const std::string& path = "nodes.txt") {
+/* Whitespace-separated tokens of a text file after its leading count.  The
+ * reference parses them with atoi/atof (a corrupt token becomes 0) and writes
+ * past its count-sized array when the file holds more values than the count
+ * (LouvainCPP.cpp:660-737); here a token that is not entirely a number, a
+ * count that is not a non-negative integer, or a value count that differs
+ * from `count * per_record` throws Error. */
+namespace detail {
+inline std::vector<std::string> counted_tokens(const std::string& path, size_t per_record, long long& count) {
   std::ifstream f(path);
   if (!f) throw Error(LVG_ERR_INVALID_ARG, "cannot open " + path);
+  std::string tok;
+  if (!(f >> tok)) throw Error(LVG_ERR_INVALID_ARG, path + ": empty file (no count)");
+  char* end = nullptr;
+  errno = 0;
+  count = std::strtoll(tok.c_str(), &end, 10);
+  if (errno || *end != '\0' || count < 0) throw Error(LVG_ERR_INVALID_ARG, path + ": bad count '" + tok + "'");
+  std::vector<std::string> out;
+  out.reserve((size_t)count * per_record);
+  while (f >> tok) {
+    if (out.size() == (size_t)count * per_record)
+      throw Error(LVG_ERR_INVALID_ARG, path + ": more values than the count " + std::to_string(count) + " gives");
+    out.push_back(tok);
+  }
+  if (out.size() != (size_t)count * per_record)
+    throw Error(LVG_ERR_INVALID_ARG, path + ": truncated: " + std::to_string(out.size()) + " values, " +
+                                         std::to_string((size_t)count * per_record) + " expected");
+  return out;
+}
+inline int to_int(const std::string& path, const std::string& t) {
+  char* end = nullptr;
+  errno = 0;
+  long v = std::strtol(t.c_str(), &end, 10);
+  if (errno || *end != '\0' || t.empty() || v < INT32_MIN || v > INT32_MAX)
+    throw Error(LVG_ERR_INVALID_ARG, path + ": not an integer id: '" + t + "'");
+  return (int)v;
+}
+inline float to_float(const std::string& path, const std::string& t) {
+  char* end = nullptr;
+  errno = 0;
+  float v = std::strtof(t.c_str(), &end);
+  if (errno || *end != '\0' || t.empty()) throw Error(LVG_ERR_INVALID_ARG, path + ": not a weight: '" + t + "'");
+  return v;
+}
+}  // namespace detail
+
+/* loadNodes (LouvainCPP.cpp:660-701): "count id id id ...". */
+inline std::vector<int> loadNodes(const std::string& path = "nodes.txt") {
   long long count = 0;
-  f >> count;
-  std::vector<int> ids;
-  ids.reserve(count > 0 ? (size_t)count : 0);
-  int x;
-  while (f >> x) ids.push_back(x);
+  std::vector<std::string> tok = detail::counted_tokens(path, 1, count);
+  std::vector<int> ids(tok.size());
+  for (size_t i = 0; i < tok.size(); ++i) ids[i] = detail::to_int(path, tok[i]);
   return ids;
 }
 
-/* loadEdges (LouvainCPP.cpp:703-737): "count src tgt w src tgt w ...", read
- * the same way as loadNodes. */
+/* loadEdges (LouvainCPP.cpp:703-737): "count src tgt w src tgt w ...". */
 inline std::vector<Edge> loadEdges(const std::string& path = "edges.txt") {
-  std::ifstream f(path);
-  if (!f) throw Error(LVG_ERR_INVALID_ARG, "cannot open " + path);
   long long count = 0;
-  f >> count;
-  std::vector<Edge> edges;
-  edges.reserve(count > 0 ? (size_t)count : 0);
-  Edge e;
-  while (f >> e.source >> e.target >> e.weight) edges.push_back(e);
+  std::vector<std::string> tok = detail::counted_tokens(path, 3, count);
+  std::vector<Edge> edges((size_t)count);
+  for (size_t i = 0; i < edges.size(); ++i) {
+    edges[i].source = detail::to_int(path, tok[3 * i]);
+    edges[i].target = detail::to_int(path, tok[3 * i + 1]);
+    edges[i].weight = detail::to_float(path, tok[3 * i + 2]);
+  }
   return edges;
 }
 

@@ -125,6 +125,8 @@ SIGNATURES = {
     "lvg_count_partitions": (i32, [P, i64, ctypes.POINTER(i32)]),
     "lvg_modularity_fp64": (i32, [P, P, ctypes.POINTER(dbl)]),
     "lvg_get_csr": (i32, [P, ctypes.POINTER(i32), ctypes.POINTER(i64), ctypes.POINTER(dbl), P, P, P, P, P, P]),
+    "lvg_get_level_edges": (i32, [P, ctypes.POINTER(i64), P, P, P]),
+    "lvg_debug_radix_hold": (i32, [i32, i64]),
     "lvg_set_communities": (i32, [P, P]),
     "lvg_move_decide": (i32, [P, P, P]),
     "lvg_last_pass_times": (i32, [P, P, i32, ctypes.POINTER(i32)]),

@@ -736,6 +736,21 @@ lvg_status lvg_get_csr(const lvg_ctx* cc, int32_t* n_vertices, int64_t* nnz, dou
   });
 }
 
+lvg_status lvg_get_level_edges(const lvg_ctx* cc, int64_t* n_entries, int32_t* src, int32_t* dst, float* w) {
+  lvg_ctx* c = const_cast<lvg_ctx*>(cc);
+  return guarded(c, [&] {
+    check_ctx(c);
+    require(c->loaded && c->have_state, LVG_ERR_STATE, "no graph loaded");
+    const LevelGraph& g = c->g;
+    if (n_entries) *n_entries = g.E;
+    cudaStream_t s = c->stream;
+    if (src && g.E) LVG_CUDA(cudaMemcpyAsync(src, g.src, sizeof(int32_t) * g.E, cudaMemcpyDeviceToHost, s));
+    if (dst && g.E) LVG_CUDA(cudaMemcpyAsync(dst, g.dst, sizeof(int32_t) * g.E, cudaMemcpyDeviceToHost, s));
+    if (w && g.E) LVG_CUDA(cudaMemcpyAsync(w, g.w, sizeof(float) * g.E, cudaMemcpyDeviceToHost, s));
+    sync(c);
+  });
+}
+
 lvg_status lvg_set_communities(lvg_ctx* c, const int32_t* comm) {
   return guarded(c, [&] {
     check_ctx(c);

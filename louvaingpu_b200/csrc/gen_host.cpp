@@ -46,34 +46,86 @@ struct lvggen_graph {
 
 namespace {
 
-// Undirected edges (u < v) -> merged, symmetric, sorted list.
+template <typename T>
+inline T fetch_add(T* x, T v) { return __atomic_fetch_add(x, v, __ATOMIC_RELAXED); }
+
+// Undirected edges (u < v; u < 0 marks a dropped entry) -> merged, symmetric
+// list sorted by (src, dst), built in parallel.  Row i holds its partners
+// below i (edges (u, i)) and then those above i (edges (i, v)), each part in
+// increasing partner order; duplicate edges are merged (weights summed, or the
+// first kept).  The list is unique: parts are sorted by partner, and equal
+// (u, v) weights are integers, whose sums are exact in any order.
 void finish(lvggen_graph* g, std::vector<UEdge>& ue, bool sum_dups) {
-  std::sort(ue.begin(), ue.end(), [](const UEdge& a, const UEdge& b) {
-    return a.u != b.u ? a.u < b.u : a.v < b.v;
-  });
-  std::vector<UEdge> m;
-  m.reserve(ue.size());
-  for (const UEdge& e : ue) {
-    if (!m.empty() && m.back().u == e.u && m.back().v == e.v) {
-      if (sum_dups) m.back().w += e.w;
-    } else {
-      m.push_back(e);
+  const int32_t n = g->n;
+  const int64_t M = (int64_t)ue.size();
+  // 1. bucket by the smaller endpoint
+  std::vector<int64_t> off((size_t)n + 1, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t e = 0; e < M; ++e)
+    if (ue[e].u >= 0) fetch_add<int64_t>(&off[(size_t)ue[e].u + 1], 1);
+  for (int32_t i = 0; i < n; ++i) off[i + 1] += off[i];
+  std::vector<UEdge> b((size_t)off[n]);
+  {
+    std::vector<int64_t> cur(off.begin(), off.end() - 1);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < M; ++e)
+      if (ue[e].u >= 0) b[(size_t)fetch_add<int64_t>(&cur[ue[e].u], 1)] = ue[e];
+  }
+  std::vector<UEdge>().swap(ue);
+  // 2. each bucket sorted by partner, duplicates merged in place
+  std::vector<int64_t> mcnt(n, 0), tcnt(n, 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int32_t u = 0; u < n; ++u) {
+    UEdge* lo = b.data() + off[u];
+    UEdge* hi = b.data() + off[u + 1];
+    std::sort(lo, hi, [](const UEdge& x, const UEdge& y) { return x.v != y.v ? x.v < y.v : x.w < y.w; });
+    int64_t k = 0;
+    for (UEdge* it = lo; it != hi; ++it) {
+      if (k > 0 && lo[k - 1].v == it->v) {
+        if (sum_dups) lo[k - 1].w += it->w;
+      } else {
+        lo[k++] = *it;
+      }
+    }
+    mcnt[u] = k;
+    for (int64_t j = 0; j < k; ++j) fetch_add<int64_t>(&tcnt[lo[j].v], 1);
+  }
+  // 3. rows of the symmetric list
+  std::vector<int64_t> row((size_t)n + 1, 0);
+  for (int32_t i = 0; i < n; ++i) row[i + 1] = row[i] + tcnt[i] + mcnt[i];
+  const int64_t E = row[n];
+  g->src.resize(E); g->dst.resize(E); g->w.resize(E);
+  {
+    std::vector<int64_t> cur(row.begin(), row.end() - 1);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int32_t u = 0; u < n; ++u) {
+      const UEdge* lo = b.data() + off[u];
+      for (int64_t j = 0; j < mcnt[u]; ++j) {   // (u, v) seen from v: partner u below v
+        const int64_t p = fetch_add<int64_t>(&cur[lo[j].v], 1);
+        g->src[p] = lo[j].v; g->dst[p] = u; g->w[p] = lo[j].w;
+      }
+      const int64_t q = row[u] + tcnt[u];       // partners above u, already in order
+      for (int64_t j = 0; j < mcnt[u]; ++j) {
+        g->src[q + j] = u; g->dst[q + j] = lo[j].v; g->w[q + j] = lo[j].w;
+      }
     }
   }
-  // both directions, sorted by (src, dst): counting sort by src
-  const int32_t n = g->n;
-  std::vector<int64_t> cnt((size_t)n + 1, 0);
-  for (const UEdge& e : m) { cnt[e.u + 1]++; cnt[e.v + 1]++; }
-  for (int32_t i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
-  const int64_t E = cnt[n];
-  g->src.resize(E); g->dst.resize(E); g->w.resize(E);
-  std::vector<int64_t> cur(cnt.begin(), cnt.end() - 1);
-  for (const UEdge& e : m) {
-    int64_t p = cur[e.u]++; g->src[p] = e.u; g->dst[p] = e.v; g->w[p] = e.w;
-    int64_t q = cur[e.v]++; g->src[q] = e.v; g->dst[q] = e.u; g->w[q] = e.w;
+  // 4. the lower part of every row in partner order (partners are distinct)
+#pragma omp parallel
+  {
+    std::vector<std::pair<int32_t, float>> tmp;
+#pragma omp for schedule(dynamic, 1024)
+    for (int32_t i = 0; i < n; ++i) {
+      const int64_t lo = row[i], k = tcnt[i];
+      if (k < 2) continue;
+      tmp.resize(k);
+      for (int64_t j = 0; j < k; ++j) tmp[j] = {g->dst[lo + j], g->w[lo + j]};
+      std::sort(tmp.begin(), tmp.end(), [](const std::pair<int32_t, float>& x, const std::pair<int32_t, float>& y) {
+        return x.first < y.first;
+      });
+      for (int64_t j = 0; j < k; ++j) { g->dst[lo + j] = tmp[j].first; g->w[lo + j] = tmp[j].second; }
+    }
   }
-  // rows come out sorted: edges (u, i), u < i, precede edges (i, v), v > i,
-  // and each group is visited in increasing partner order.
 }
 
 float int_weight(uint64_t r, int32_t lo, int32_t hi) {
@@ -216,9 +268,9 @@ lvggen_graph* lvggen_rmat(int32_t scale, int32_t edge_factor, double a, double b
   g->n = (int32_t)1 << scale;
   g->truth.assign(g->n, -1);
   const int64_t M = (int64_t)edge_factor << scale;
-  std::vector<UEdge> ue;
-  ue.reserve(M);
+  std::vector<UEdge> ue((size_t)M);
   const double ab = a + b, abc = a + b + c;
+#pragma omp parallel for schedule(static)
   for (int64_t e = 0; e < M; ++e) {
     uint32_t u = 0, v = 0;
     for (int l = 0; l < scale; ++l) {
@@ -228,9 +280,9 @@ lvggen_graph* lvggen_rmat(int32_t scale, int32_t edge_factor, double a, double b
       u = (u << 1) | bu;
       v = (v << 1) | bv;
     }
-    if (u == v) continue;
+    if (u == v) { ue[e] = {-1, -1, 0.0f}; continue; }   // self loop: dropped
     float w = int_weight(rng_at(seed, 3, (uint64_t)e), w_lo, w_hi);
-    ue.push_back({(int32_t)std::min(u, v), (int32_t)std::max(u, v), w});
+    ue[e] = {(int32_t)std::min(u, v), (int32_t)std::max(u, v), w};
   }
   finish(g, ue, true);
   return g;

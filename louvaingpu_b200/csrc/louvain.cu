@@ -1546,9 +1546,25 @@ __device__ __forceinline__ void warp_group_add(double* arr, int32_t key, double 
   if (key >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&arr[key], sum);
 }
 
+// Community ids of an entry's endpoints as accumulation keys: -1 (no part in
+// the sums) for a lane past the end, and for an id outside [0, C), which also
+// sets *bad when the caller passes a flag (callers that validated the ids on
+// the host pass none).
+__device__ __forceinline__ void nm_keys(const int32_t* part, const int32_t* src, const int32_t* dst, int64_t e,
+                                        bool ok, int32_t C, uint32_t* bad, int32_t& a, int32_t& b) {
+  a = ok ? part[src[e]] : -1;
+  b = ok ? part[dst[e]] : -1;
+  const bool oob = ok && ((uint32_t)a >= (uint32_t)C || (uint32_t)b >= (uint32_t)C);
+  if (oob) {
+    if (bad) atomicOr(bad, 1u);
+    a = (uint32_t)a < (uint32_t)C ? a : -1;
+    b = (uint32_t)b < (uint32_t)C ? b : -1;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) nm_accum_smem_kernel(const int32_t* src, const int32_t* dst,
                                                                  const float* w, int64_t E, const int32_t* part,
-                                                                 int32_t C, double* Kc, double* Ain) {
+                                                                 int32_t C, double* Kc, double* Ain, uint32_t* bad) {
   extern __shared__ __align__(16) unsigned char smem[];
   double* sK = reinterpret_cast<double*>(smem);
   double* sA = sK + C;
@@ -1559,10 +1575,11 @@ __global__ void __launch_bounds__(kThreads) nm_accum_smem_kernel(const int32_t* 
     const int64_t e = e0 + threadIdx.x;
     const bool ok = e < E;
     const double x = ok ? (double)w[e] : 0.0;
-    const int32_t a = ok ? part[src[e]] : -1, b = ok ? part[dst[e]] : -1;
+    int32_t a, b;
+    nm_keys(part, src, dst, e, ok, C, bad, a, b);
     warp_group_add(sK, a, x);
     warp_group_add(sK, b, x);
-    warp_group_add(sA, (ok && a == b) ? a : -1, 2.0 * x);
+    warp_group_add(sA, (a >= 0 && a == b) ? a : -1, 2.0 * x);
   }
   __syncthreads();
   for (int c = threadIdx.x; c < C; c += kThreads) {
@@ -1574,27 +1591,17 @@ __global__ void __launch_bounds__(kThreads) nm_accum_smem_kernel(const int32_t* 
 // Kc, Ain of modularity_fp64 for many communities: grid-stride over whole
 // warps, warp-aggregated atomics.
 __global__ void nm_accum_agg_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
-                                    const int32_t* part, double* Kc, double* Ain) {
+                                    const int32_t* part, int32_t C, double* Kc, double* Ain, uint32_t* bad) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t e0 = blockIdx.x * (int64_t)blockDim.x; e0 < E; e0 += stride) {
     const int64_t e = e0 + threadIdx.x;
     const bool ok = e < E;
     const double x = ok ? (double)w[e] : 0.0;
-    const int32_t a = ok ? part[src[e]] : -1, b = ok ? part[dst[e]] : -1;
+    int32_t a, b;
+    nm_keys(part, src, dst, e, ok, C, bad, a, b);
     warp_group_add(Kc, a, x);
     warp_group_add(Kc, b, x);
-    warp_group_add(Ain, (ok && a == b) ? a : -1, 2.0 * x);
-  }
-}
-
-__global__ void nm_accum_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
-                                const int32_t* part, double* Kc, double* Ain) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
-    double x = (double)w[e];
-    int32_t a = part[src[e]], b = part[dst[e]];
-    atomicAdd(&Kc[a], x);
-    atomicAdd(&Kc[b], x);
-    if (a == b) atomicAdd(&Ain[a], 2.0 * x);
+    warp_group_add(Ain, (a >= 0 && a == b) ? a : -1, 2.0 * x);
   }
 }
 
@@ -2321,6 +2328,38 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
   return cnt;
 }
 
+// Raises the dynamic shared memory limit of nm_accum_smem_kernel on the
+// current device to at least `smem` bytes.  The limit only ever grows, under
+// one lock shared by every caller, so a launch never finds it lowered by a
+// smaller request made in between.
+static void nm_smem_attr(size_t smem) {
+  if (smem <= 48 * 1024) return;
+  constexpr int kDevs = 64;
+  static std::mutex mu;
+  static size_t attr[kDevs] = {};
+  int dev = 0;
+  LVG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < kDevs && smem <= attr[dev]) return;
+  LVG_CUDA(cudaFuncSetAttribute(nm_accum_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (dev >= 0 && dev < kDevs) attr[dev] = smem;
+}
+
+// Kc and Ain of every community: shared-memory sums when they fit, else
+// warp-aggregated global atomics.
+static void nm_accum(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
+                     const int32_t* part, double* Kc, double* Ain, uint32_t* bad, cudaStream_t s) {
+  if (E <= 0) return;
+  if (C <= kNmSmemMax) {
+    const size_t smem = sizeof(double) * 2 * (size_t)C;
+    nm_smem_attr(smem);
+    nm_accum_smem_kernel<<<sm_grid(E, kThreads), kThreads, smem, s>>>(src, dst, w, E, part, C, Kc, Ain, bad);
+  } else {
+    nm_accum_agg_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, C, Kc, Ain, bad);
+  }
+  LVG_LAUNCH();
+}
+
 double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
                        const int32_t* part, Arena& a, cudaStream_t s) {
   HiScope hs(a);
@@ -2330,23 +2369,7 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
   double* twoW = a.hi_n<double>(2);
   LVG_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * std::max(C, 1), s));
   LVG_CUDA(cudaMemsetAsync(Ain, 0, sizeof(double) * std::max(C, 1), s));
-  if (E > 0 && C <= kNmSmemMax) {
-    size_t smem = sizeof(double) * 2 * (size_t)C;
-    static std::mutex mu;
-    static size_t attr = 0;
-    {
-      std::lock_guard<std::mutex> lock(mu);
-      if (smem > 48 * 1024 && smem > attr) {
-        LVG_CUDA(cudaFuncSetAttribute(nm_accum_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = smem;
-      }
-    }
-    nm_accum_smem_kernel<<<sm_grid(E, kThreads), kThreads, smem, s>>>(src, dst, w, E, part, C, Kc, Ain);
-    LVG_LAUNCH();
-  } else if (E > 0) {
-    nm_accum_agg_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
-    LVG_LAUNCH();
-  }
+  nm_accum(src, dst, w, E, C, part, Kc, Ain, nullptr, s);   // ids checked on the host
   tree_sum_f64(Kc, C, twoW, a, s);
   nm_term_kernel<<<sm_grid(C, kThreads), kThreads, 0, s>>>(Kc, Ain, C, twoW, t);
   LVG_LAUNCH();
@@ -2359,21 +2382,13 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
 
 // The modularity kernels of modularity_fp64 with every scratch array given by
 // the caller (used by the allocation-free entry point).  C <= 2048 * 2048.
+// Community ids outside [0, C) take no part in the sums and set *bad.
 void modularity_fp64_scratch(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
                              const int32_t* part, double* Kc, double* Ain, double* t, double* partials,
-                             double* twoW_q, cudaStream_t s) {
+                             double* twoW_q, uint32_t* bad, cudaStream_t s) {
   LVG_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * C, s));
   LVG_CUDA(cudaMemsetAsync(Ain, 0, sizeof(double) * C, s));
-  if (E > 0 && C <= kNmSmemMax) {
-    size_t smem = sizeof(double) * 2 * (size_t)C;
-    if (smem > 48 * 1024)
-      LVG_CUDA(cudaFuncSetAttribute(nm_accum_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    nm_accum_smem_kernel<<<sm_grid(E, kThreads), kThreads, smem, s>>>(src, dst, w, E, part, C, Kc, Ain);
-    LVG_LAUNCH();
-  } else if (E > 0) {
-    nm_accum_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
-    LVG_LAUNCH();
-  }
+  nm_accum(src, dst, w, E, C, part, Kc, Ain, bad, s);
   // the fixed tree of tree_sum_f64, partials from the caller
   auto tree = [&](const double* x, double* out) {
     int64_t nb = ((int64_t)C + kGroup - 1) / kGroup;

@@ -166,9 +166,11 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
 
 // The same modularity with caller-provided scratch: Kc, Ain, t of C doubles,
 // partials of ceil(C/2048) doubles; twoW_q[0] = 2W, twoW_q[1] = Q (device).
+// Community ids outside [0, C) are left out of the sums and set *bad (device
+// flag, nullable).
 void modularity_fp64_scratch(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
                              const int32_t* part, double* Kc, double* Ain, double* t, double* partials,
-                             double* twoW_q, cudaStream_t s);
+                             double* twoW_q, uint32_t* bad, cudaStream_t s);
 
 // ---------------------------------------------------------------- batched runs
 // Per-graph pass control of a batched run (device arrays of the level's graphs).

@@ -1,13 +1,13 @@
 // Allocation-free FP64 modularity.
 //
 // Some callers cannot allocate device memory at the moment they need a
-// modularity value: code that runs while a stream is being captured into a
-// CUDA graph (cudaMalloc and cudaFree are not allowed there), serving loops
-// that have handed all free HBM to their own pool and must not grow it, and
-// latency-bound paths that cannot take the device-wide synchronisation a
-// cudaMalloc or cudaFree implies.  lvg_modularity_fp64_noalloc serves them:
-// its scratch is the file-scope array below, allocated once when the module is
-// loaded on a device and kept until the process exits.
+// modularity value: a serving process whose caching allocator has already
+// reserved all free HBM for its own pool (a cudaMalloc would fail or force
+// that pool to shrink), and latency-bound loops that run beside work on other
+// streams and cannot take the device-wide synchronisation that cudaMalloc and
+// cudaFree imply.  lvg_modularity_fp64_noalloc serves them: its scratch is the
+// file-scope array below, allocated once when the module is loaded on a device
+// and kept until the process exits.
 #include <cstring>
 #include <mutex>
 
@@ -17,8 +17,9 @@ namespace {
 
 constexpr int64_t kMaxComms = LVG_NOALLOC_MAX_COMMS;
 constexpr int64_t kPartials = (kMaxComms + lvg::kGroup - 1) / lvg::kGroup;
-// Kc | Ain | t (kMaxComms each) | tree partials | 2W, Q
-constexpr int64_t kScratch = 3 * kMaxComms + kPartials + 2;
+// Kc | Ain | t (kMaxComms each) | tree partials | 2W, Q | bad-id flag
+constexpr int64_t kScratch = 3 * kMaxComms + kPartials + 3;
+static_assert(kScratch * sizeof(double) == LVG_NOALLOC_SCRATCH_BYTES, "header states the array size");
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratch];
 
@@ -56,12 +57,17 @@ extern "C" lvg_status lvg_modularity_fp64_noalloc(const int32_t* d_src, const in
   double* Ain = base + kMaxComms;
   double* t = base + 2 * kMaxComms;
   double* partials = base + 3 * kMaxComms;
-  double* out = partials + kPartials;
+  double* out = partials + kPartials;                       // 2W, Q
+  uint32_t* bad = reinterpret_cast<uint32_t*>(out + 2);     // set by a community id outside [0, n_comms)
   try {
-    lvg::modularity_fp64_scratch(d_src, d_dst, d_w, n_entries, n_comms, d_part, Kc, Ain, t, partials, out, s);
-    double h[2];
+    LVG_CUDA(cudaMemsetAsync(bad, 0, sizeof(double), s));
+    lvg::modularity_fp64_scratch(d_src, d_dst, d_w, n_entries, n_comms, d_part, Kc, Ain, t, partials, out, bad, s);
+    double h[3];
     LVG_CUDA(cudaMemcpyAsync(h, out, sizeof h, cudaMemcpyDeviceToHost, s));
     LVG_CUDA(cudaStreamSynchronize(s));
+    uint32_t flag = 0;
+    std::memcpy(&flag, &h[2], sizeof flag);
+    if (flag) return LVG_ERR_INVALID_ARG;
     *q = h[1];
   } catch (const lvg::Error& e) {
     return e.status;

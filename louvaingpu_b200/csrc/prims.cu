@@ -7,6 +7,7 @@
 // in shared memory (warp __match_any_sync multisplit), learns the counts of
 // its digits in all earlier tiles by decoupled look-back (bounded spin, error
 // flag), and writes its keys out digit run by digit run.
+#include <atomic>
 #include <mutex>
 
 #include "prims.cuh"
@@ -153,6 +154,10 @@ struct RsSmem {
 // tile's count, 2p+2: count of every tile up to this one, for pass p; codes of
 // earlier passes read as "not yet"), count in bits 0..31.
 constexpr int kRsSpinLimit = 1 << 22;
+// Test hook (lvg_debug_radix_hold): a smaller spin limit and one tile that
+// never publishes, so that the bounded wait of its successors runs out.
+std::atomic<int> g_rs_spin_limit{kRsSpinLimit};
+std::atomic<int64_t> g_rs_hold_tile{-1};
 
 __device__ __forceinline__ void rs_publish(unsigned long long* w, unsigned code, uint32_t count) {
   atomicExch(w, ((unsigned long long)code << 56) | count);
@@ -166,7 +171,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_onesweep_kernel(const uint64_t*
                                                                  uint64_t* kout, float* vout, int64_t n,
                                                                  int shift, int pass, const uint32_t* gstart,
                                                                  unsigned long long* look, uint32_t* counter,
-                                                                 uint32_t* err) {
+                                                                 uint32_t* err, int spin_limit, int64_t hold) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RsSmem& S = *reinterpret_cast<RsSmem*>(smem_raw);
   const unsigned full = 0xffffffffu;
@@ -213,11 +218,12 @@ __global__ void __launch_bounds__(kRsThreads) rs_onesweep_kernel(const uint64_t*
   }
   const unsigned agg = 2u * (unsigned)pass + 1u, inc = agg + 1u;
   unsigned long long* mine = look + tile * kRadix + d;
+  const bool publish = tile != hold;   // hold: a test makes this tile's successors wait out their limit
   uint32_t excl = 0;
   if (tile == 0) {
-    rs_publish(mine, inc, cnt);
+    if (publish) rs_publish(mine, inc, cnt);
   } else {
-    rs_publish(mine, agg, cnt);
+    if (publish) rs_publish(mine, agg, cnt);
     int64_t j = tile - 1;
     int spins = 0;
     while (j >= 0) {
@@ -225,9 +231,9 @@ __global__ void __launch_bounds__(kRsThreads) rs_onesweep_kernel(const uint64_t*
       const unsigned code = (unsigned)(x >> 56);
       if (code == inc) { excl += (uint32_t)x; break; }
       if (code == agg) { excl += (uint32_t)x; --j; continue; }
-      if (++spins > kRsSpinLimit) { atomicOr(err, 1u); break; }   // bounded wait: report, never hang
+      if (++spins > spin_limit) { atomicOr(err, 1u); break; }   // bounded wait: report, never hang
     }
-    rs_publish(mine, inc, excl + cnt);
+    if (publish) rs_publish(mine, inc, excl + cnt);
   }
   uint32_t tot;
   const uint32_t start = block_exclusive_scan<uint32_t>(cnt, &tot);
@@ -321,7 +327,8 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
   float* Vv[2] = {v0, v1};
   for (int p = 0; p < npass; ++p) {
     rs_onesweep_kernel<<<(unsigned)ntiles, kRsThreads, sizeof(RsSmem), s>>>(
-        K[cur], Vv[cur], K[cur ^ 1], Vv[cur ^ 1], n, 8 * p, p, ghist + p * kRadix, look, counters + p, err);
+        K[cur], Vv[cur], K[cur ^ 1], Vv[cur ^ 1], n, 8 * p, p, ghist + p * kRadix, look, counters + p, err,
+        g_rs_spin_limit.load(), g_rs_hold_tile.load());
     LVG_LAUNCH();
     cur ^= 1;
   }
@@ -333,3 +340,10 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
 }
 
 }  // namespace lvg
+
+extern "C" lvg_status lvg_debug_radix_hold(int32_t spin_limit, int64_t hold_tile) {
+  if (spin_limit < 1) return LVG_ERR_INVALID_ARG;
+  lvg::g_rs_spin_limit.store(spin_limit);
+  lvg::g_rs_hold_tile.store(hold_tile);
+  return LVG_OK;
+}

@@ -262,6 +262,16 @@ class Louvain:
                                         _p(col), _p(w), _p(k), _p(loopw), _p(hl)))
         return dict(V=V, nnz=nnz, m=m, off=off, col=col, w=w, k=k, loopw=loopw, has_loop=hl)
 
+    def level_edges(self):
+        """The current level's input list (src, dst, w); after induce() the
+        coarse list of inducedGraphCUDA (InducedGraphKernel.cu:84-113)."""
+        n = ctypes.c_int64()
+        self._check(self._L.lvg_get_level_edges(self._h, ctypes.byref(n), None, None, None))
+        src, dst = np.zeros(n.value, np.int32), np.zeros(n.value, np.int32)
+        w = np.zeros(n.value, np.float32)
+        self._check(self._L.lvg_get_level_edges(self._h, ctypes.byref(n), _p(src), _p(dst), _p(w)))
+        return src, dst, w
+
     def set_communities(self, comm):
         comm = np.ascontiguousarray(comm, np.int32)
         self._check(self._L.lvg_set_communities(self._h, _p(comm)))

@@ -537,6 +537,32 @@ void orc_move_decide(const orc_csr* h, const int32_t* comm, const double* tot, c
   }
 }
 
+// orc_move_decide for the listed vertices only (a bounded sample of one
+// decision pass): outputs are written at the listed positions.  Returns the
+// seconds of the decisions alone (the per-thread scratch is set up first, as
+// a whole run sets it up once per level).
+double orc_move_decide_subset(const orc_csr* h, const int32_t* comm, const double* tot, const int32_t* size,
+                            const int32_t* verts, int64_t n_verts, int32_t* next, int32_t* cand, int32_t* nseg,
+                            int n_threads) {
+  const Csr& g = h->g;
+  int nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+  std::vector<std::unique_ptr<Scratch<double>>> scr(nt);
+#pragma omp parallel num_threads(nt)
+  scr[omp_get_thread_num()].reset(new Scratch<double>(g.V));   // first touch by the thread that uses it
+  const double twom = 2.0 * g.m;
+  const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 512)
+  for (int64_t j = 0; j < n_verts; ++j) {
+    const int32_t i = verts[j];
+    double kf = g.m > 0.0 ? g.k[i] / twom : 0.0;
+    auto d = decide<false>(g, i, comm, tot, size, kf, 0.0f, *scr[omp_get_thread_num()]);
+    if (next) next[i] = d.next;
+    if (cand) cand[i] = d.cand;
+    if (nseg) nseg[i] = d.nseg;
+  }
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
 double orc_tree_sum(const double* x, int64_t n) { return tree_sum(x, n); }
 
 double orc_q_totals(const double* tot, const double* in, int32_t n, double m) {

@@ -49,6 +49,13 @@ void orc_move_decide(const orc_csr*, const int32_t* comm, const double* tot,
                      const int32_t* size, int32_t* next, int32_t* cand, int32_t* nseg,
                      int n_threads);
 
+/* orc_move_decide restricted to the n_verts vertices listed in verts (a
+ * bounded sample of one pass); outputs are written at those positions.
+ * Returns the seconds the decisions took (scratch set-up excluded). */
+double orc_move_decide_subset(const orc_csr*, const int32_t* comm, const double* tot,
+                            const int32_t* size, const int32_t* verts, int64_t n_verts,
+                            int32_t* next, int32_t* cand, int32_t* nseg, int n_threads);
+
 /* Deterministic fixed-tree FP64 sum used for Q on both sides. */
 double orc_tree_sum(const double* x, int64_t n);
 

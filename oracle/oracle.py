@@ -52,6 +52,8 @@ def lib():
         L.orc_csr_m.argtypes = [P]
         L.orc_csr_get.argtypes = [P, P, P, P, P, P, P]
         L.orc_move_decide.argtypes = [P, P, P, P, P, P, P, ctypes.c_int]
+        L.orc_move_decide_subset.restype = dbl
+        L.orc_move_decide_subset.argtypes = [P, P, P, P, P, i64, P, P, P, ctypes.c_int]
         L.orc_tree_sum.restype = dbl
         L.orc_tree_sum.argtypes = [P, i64]
         L.orc_q_totals.restype = dbl
@@ -95,7 +97,9 @@ def _edges(src, dst, w):
 class Csr:
     """Level CSR (NeighbourCompute.cu:42-117 + InitKernel.cu:154-243)."""
 
-    def __init__(self, n_vertices, src, dst, w):
+    def __init__(self, n_vertices, src, dst, w, arrays=True):
+        """arrays=False copies out only off and k (large graphs: the
+        entry arrays stay inside the library)."""
         s, d, ww = _edges(src, dst, w)
         self.V = int(n_vertices)
         self.h = lib().orc_csr_build(self.V, len(s), _p(s), _p(d), _p(ww))
@@ -104,13 +108,16 @@ class Csr:
         self.nnz = lib().orc_csr_nnz(self.h)
         self.m = lib().orc_csr_m(self.h)
         self.off = np.zeros(self.V + 1, np.int64)
-        self.col = np.zeros(self.nnz, np.int32)
-        self.w = np.zeros(self.nnz, np.float32)
         self.k = np.zeros(self.V, np.float64)
-        self.loopw = np.zeros(self.V, np.float32)
-        self.has_loop = np.zeros(self.V, np.uint8)
-        lib().orc_csr_get(self.h, _p(self.off), _p(self.col), _p(self.w), _p(self.k),
-                          _p(self.loopw), _p(self.has_loop))
+        if arrays:
+            self.col = np.zeros(self.nnz, np.int32)
+            self.w = np.zeros(self.nnz, np.float32)
+            self.loopw = np.zeros(self.V, np.float32)
+            self.has_loop = np.zeros(self.V, np.uint8)
+            lib().orc_csr_get(self.h, _p(self.off), _p(self.col), _p(self.w), _p(self.k),
+                              _p(self.loopw), _p(self.has_loop))
+        else:
+            lib().orc_csr_get(self.h, _p(self.off), None, None, _p(self.k), None, None)
 
     def decide(self, comm, tot, size, n_threads=0):
         comm = np.ascontiguousarray(comm, np.int32)
@@ -121,6 +128,19 @@ class Csr:
         nseg = np.zeros(self.V, np.int32)
         lib().orc_move_decide(self.h, _p(comm), _p(tot), _p(size), _p(nxt), _p(cand), _p(nseg), n_threads)
         return nxt, cand, nseg
+
+    def decide_subset(self, comm, tot, size, verts, n_threads=0):
+        """decide() for the listed vertices only; returns the seconds the
+        decisions took (timed inside the library, scratch set-up excluded)
+        and next[] (entries of unlisted vertices are 0)."""
+        comm = np.ascontiguousarray(comm, np.int32)
+        tot = np.ascontiguousarray(tot, np.float64)
+        size = np.ascontiguousarray(size, np.int32)
+        verts = np.ascontiguousarray(verts, np.int32)
+        nxt = np.zeros(self.V, np.int32)
+        secs = lib().orc_move_decide_subset(self.h, _p(comm), _p(tot), _p(size), _p(verts), len(verts), _p(nxt),
+                                            None, None, n_threads)
+        return secs, nxt
 
     def __del__(self):
         if getattr(self, "h", None):

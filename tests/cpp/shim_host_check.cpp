@@ -94,6 +94,26 @@ int main(int argc, char** argv) {
   threw = false;
   try { lvg_ref::loadNodes(dir + "/absent.txt"); } catch (const lvg_ref::Error&) { threw = true; }
   expect(threw, "loadNodes on a missing file");
+  // truncated and corrupt files are errors, not short or garbage lists
+  // (the reference reads them with atoi/atof and writes past its arrays)
+  const char* bad_nodes[] = {"", "4\n1000 -3\n77\n", "3\n1 2 3 4\n", "x\n1 2\n", "-2\n", "2\n1 2x\n",
+                             "2\n1 99999999999\n"};
+  for (const char* text : bad_nodes) {
+    { std::ofstream f(dir + "/bad_nodes.txt"); f << text; }
+    threw = false;
+    try { lvg_ref::loadNodes(dir + "/bad_nodes.txt"); } catch (const lvg_ref::Error&) { threw = true; }
+    expect(threw, (std::string("loadNodes rejects: ") + text).c_str());
+  }
+  const char* bad_edges[] = {"2\n1 2 1.0\n", "2\n1 2 1.0\n3 4\n", "1\n1 2 1.0 5\n", "1\n1 2 heavy\n",
+                             "1\n1 two 1.0\n", "1\n1.5 2 1.0\n", "1 1 2\n"};
+  for (const char* text : bad_edges) {
+    { std::ofstream f(dir + "/bad_edges.txt"); f << text; }
+    threw = false;
+    try { lvg_ref::loadEdges(dir + "/bad_edges.txt"); } catch (const lvg_ref::Error&) { threw = true; }
+    expect(threw, (std::string("loadEdges rejects: ") + text).c_str());
+  }
+  { std::ofstream f(dir + "/empty_edges.txt"); f << "0\n"; }
+  expect(lvg_ref::loadEdges(dir + "/empty_edges.txt").empty(), "loadEdges of count 0");
   std::printf(failures ? "%d FAILED\n" : "ok\n", failures);
   return failures ? 1 : 0;
 }

@@ -326,3 +326,41 @@ def test_committed_workload_fixtures(Louvain, gen, name):
         part = np.ascontiguousarray(lv.partition(), np.int32)
         assert hashlib.sha256(part.tobytes()).hexdigest() == g["final_partition_sha256"]
         assert res.q_final == pytest.approx(float.fromhex(g["final_modularity_fp64"]), abs=1e-9)
+
+
+def coarsening_partitions(oracle, gen, case, n, s, d, w):
+    """Partitions (community ids as vertex indices) to coarsen under: the
+    oracle's level-0 labels, or the planted communities for the LFR graph,
+    and random labels over a seventh of the ids."""
+    rng = np.random.default_rng(23)
+    if case == "lfr":
+        _, _, _, _, truth = gen.lfr(with_truth=True)
+        first = truth.astype(np.int32)
+    else:
+        first = oracle.Run(n, s, d, w, max_levels=1).levels[0].labels
+    return [first, rng.integers(0, max(1, n // 7), n).astype(np.int32)]
+
+
+@pytest.mark.parametrize("case", ["weighted", "loops_zeros_isolated", "odd_sizes", "hub", "lfr"])
+def test_coarsening_bit_exact(Louvain, oracle, gen, case):
+    """renumber + induce from a given partition: the vertex map
+    (RenumberKernel.cu:121-133), the coarse list -- one entry per distinct
+    (cu, cv) key in key order, weight 0 counted as 1 (InducedGraphKernel.cu:28-48)
+    and equal keys summed (:84-101) -- and the CSR built from it equal the
+    oracle's entry for entry."""
+    n, s, d, w = gen.lfr() if case == "lfr" else make_case(gen, case)
+    with Louvain() as lv:
+        for comm in coarsening_partitions(oracle, gen, case, n, s, d, w):
+            lv.load_edges(s, d, w, n)
+            lv.set_communities(comm)
+            part, C = lv.renumber()
+            exp_part, exp_C = oracle.renumber(comm)
+            assert C == exp_C
+            np.testing.assert_array_equal(part, exp_part)
+            lv.induce()
+            es, ed, ew = lv.level_edges()
+            os_, od, ow = oracle.induce(n, s, d, w, exp_part)
+            np.testing.assert_array_equal(es, os_)
+            np.testing.assert_array_equal(ed, od)
+            np.testing.assert_array_equal(ew, ow)
+            csr_equal(lv, oracle.Csr(C, os_, od, ow))
