@@ -62,6 +62,7 @@ struct lvg_ctx {
   CommState st;
   bool have_state = false;
   bool renumbered = false;
+  bool pristine = false;         // level 0 as loaded: no pass, state change or renumbering since
   int32_t* d_part_cur = nullptr;
   int32_t C_cur = 0;
   std::vector<LevelRec> levels;
@@ -186,6 +187,7 @@ void load_common(lvg_ctx* c, const int32_t* d_src, const int32_t* d_dst, const f
   c->g.w = d_w;
   prepare_level(c);
   c->loaded = true;
+  c->pristine = true;
 }
 
 void reset_to_level0(lvg_ctx* c) {
@@ -205,6 +207,7 @@ void reset_to_level0(lvg_ctx* c) {
   c->g.dst = c->dst0;
   c->g.w = c->w0;
   prepare_level(c);
+  c->pristine = true;
 }
 
 double read_q(lvg_ctx* c) {
@@ -254,6 +257,7 @@ struct L2Window {
 void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int32_t* status_out,
                double* q_start_out) {
   cudaStream_t s = c->stream;
+  c->pristine = false;
   init_state(c->g, c->st, lower, c->cfg.pass_min_gain, c->cfg.max_passes, c->arena, s);
   L2Window l2(c, c->st);
   // The first pass runs the singleton kernels and a level usually stops at
@@ -317,6 +321,7 @@ void one_level(lvg_ctx* c, double lower, double* q_out, int32_t* passes_out, int
 // high end for the rest of the run.
 int32_t renumber_level(lvg_ctx* c) {
   const int32_t V = c->g.V;
+  c->pristine = false;
   c->arena.hi = c->run_hi;
   int32_t* part = c->arena.hi_n<int32_t>(V);
   int32_t* labels = c->arena.hi_n<int32_t>(V);
@@ -577,7 +582,7 @@ lvg_status lvg_run(lvg_ctx* c, lvg_result* res) {
   lvg_status s = guarded(c, [&] {
     check_ctx(c);
     require(c->loaded, LVG_ERR_STATE, "no graph loaded");
-    if (c->level != 0 || c->renumbered || !c->levels.empty()) reset_to_level0(c);
+    if (!c->pristine) reset_to_level0(c);   // a run starts from level 0 as loaded
     if (res) std::memset(res, 0, sizeof *res);
     if (c->E0 == 0) {
       // LouvainCPP.cpp:211-230: an empty edge list yields one identity partition
@@ -762,6 +767,7 @@ lvg_status lvg_set_communities(lvg_ctx* c, const int32_t* comm) {
     HiScope hs(c->arena);
     int32_t* d = c->arena.hi_n<int32_t>(V);
     if (V > 0) LVG_CUDA(cudaMemcpyAsync(d, comm, sizeof(int32_t) * V, cudaMemcpyHostToDevice, c->stream));
+    c->pristine = false;
     set_state_from(c->g, c->st, d, c->stream);
     sync(c);
   });
@@ -915,7 +921,7 @@ extern "C" lvg_status lvg_autotune(lvg_ctx* c, const lvg_tune_space* sp, lvg_tun
     require(!cands.empty(), LVG_ERR_INVALID_ARG, "no candidate pair has tile_max_degree <= block_max_degree");
     if (n_points) *n_points = 0;
     const int32_t pref_tile = c->tune.warp_max, pref_block = c->tune.block_max;
-    if (c->level != 0 || c->renumbered || !c->levels.empty()) reset_to_level0(c);
+    if (!c->pristine) reset_to_level0(c);   // tune from level 0 as loaded
     if (c->E0 == 0 || c->g.nnz == 0) {   // no move pass to time (lvg_run runs none either)
       if (best) *best = lvg_tune_point{pref_tile, pref_block, -1.0f, -1.0f};
       return;

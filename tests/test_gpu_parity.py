@@ -364,3 +364,23 @@ def test_coarsening_bit_exact(Louvain, oracle, gen, case):
             np.testing.assert_array_equal(ed, od)
             np.testing.assert_array_equal(ew, ow)
             csr_equal(lv, oracle.Csr(C, os_, od, ow))
+
+
+def test_run_after_steps_matches_a_fresh_run(Louvain, oracle, gen):
+    """lvg_run after one_level / set_communities / renumber calls on the same
+    load restarts from the loaded level 0: same levels, Q and partition as
+    the oracle's run (the singleton Q is the first level's floor)."""
+    n, s, d, w = gen.sbm(3000, 30, 0.05, 0.002, 1, 4, seed=2)
+    orun = oracle.Run(n, s, d, w)
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        q0 = lv.modularity()
+        lv.one_level(q0)
+        lv.one_level(q0)
+        res = lv.run()
+        run_equal(lv, res, orun, n, s, d, w, oracle)
+        lv.load_edges(s, d, w, n)
+        lv.set_communities(np.random.default_rng(3).integers(0, n // 5, n).astype(np.int32))
+        lv.renumber()
+        res = lv.run()
+        run_equal(lv, res, orun, n, s, d, w, oracle)
