@@ -37,7 +37,7 @@ struct VInfo {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kHubChunk = 2048;
+constexpr int kHubChunk = 4096;
 constexpr int kNone = INT_MAX;
 
 __device__ __forceinline__ uint32_t hash_c(int32_t c, int logT) {
@@ -416,26 +416,9 @@ __device__ __forceinline__ bool table_insert(int32_t* keys, Acc* vals, int logT,
   return false;
 }
 
-// Packed (community << 32 | integer sum) slots, all ones when empty: one
-// 64-bit atomic per entry (the add cannot carry into the key: integral
-// weights keep a sum below 2^30).
+// Packed (community << 32 | integer sum) slots are all ones when empty; the
+// add of an integral weight cannot carry into the key (sums stay below 2^30).
 constexpr unsigned long long kPackedEmpty = ~0ull;
-__device__ __forceinline__ bool packed_insert(unsigned long long* t, int logT, int32_t c, uint32_t w) {
-  const uint32_t T = 1u << logT;
-  uint32_t h = hash_c(c, logT);
-  for (uint32_t p = 0; p < T; ++p) {
-    const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(t + h);
-    const uint32_t k = (uint32_t)(cur >> 32);
-    if (k == (uint32_t)c) { atomicAdd(t + h, (unsigned long long)w); return true; }
-    if (cur == kPackedEmpty) {
-      const unsigned long long prev = atomicCAS(t + h, kPackedEmpty, ((unsigned long long)(uint32_t)c << 32) | w);
-      if (prev == kPackedEmpty) return true;
-      if ((uint32_t)(prev >> 32) == (uint32_t)c) { atomicAdd(t + h, (unsigned long long)w); return true; }
-    }
-    h = (h + 1) & (T - 1);
-  }
-  return false;
-}
 
 // Entries [e0 + u*stride) of a row, u < 4: columns and weights first, then
 // the four community gathers, so that each thread keeps several loads in
@@ -1174,126 +1157,293 @@ __global__ void int_weights_kernel(const float* cw, int64_t nnz, const double* k
     if (!(k[i] < 1073741824.0)) atomicOr(notint, 1u);
 }
 
-// Hubs: chunks of a hub's row insert into the hub's global table ...
+// Hubs: rows longer than block_max.  A pass aggregates a hub's neighbour
+// communities in three launches, with no global-memory atomics on the sums:
+//  (1) hub_part_kernel -- one block per 4096-entry chunk of a hub row gathers
+//      the neighbours' communities and writes the chunk's (community, weight)
+//      pairs grouped by bucket (top bits of a hash of the community; a hub of
+//      degree d has about d/1024 buckets, a power of two) to a staging area,
+//      with the chunk's bucket offsets;
+//  (2) hub_agg_kernel -- one block per (hub, bucket) reads that bucket's
+//      pairs from every chunk of the hub, sums equal communities in a
+//      shared-memory table and keeps the bucket's best candidate and its
+//      count of distinct communities;
+//  (3) hub_decide_kernel -- one thread per hub combines its buckets in order
+//      and decides.
+// A bucket holds a disjoint set of communities, so its best candidate and
+// count are those of the row restricted to that set, and combining buckets
+// with `better` gives the row's argmax and tie-break.
+constexpr int kHubItems = kHubChunk / kThreads;   // entries per thread of a chunk
+constexpr int kHubBucketTarget = 1024;            // mean entries of a bucket
+constexpr int kHubMaxBucketsLog = 12;
+constexpr int kAggLog = 12;                       // shared table of 4096 slots
+constexpr int kAggSlots = 1 << kAggLog;
+constexpr int kAggFull = kAggSlots / 2;           // more claims: the bucket is split into sub-passes
+constexpr int kAggMaxSplitLog = 16;               // beyond 2^16 sub-passes: report, give up
+static_assert(kHubChunk % kThreads == 0 && kHubChunk <= 65535, "chunk offsets are 16-bit");
+
+__device__ __forceinline__ uint32_t hub_bucket(int32_t c, int plog) {
+  return plog == 0 ? 0u : (uint32_t)(((uint64_t)(uint32_t)c * 0x9E3779B97F4A7C15ull) >> (64 - plog));
+}
+// sub-pass of a community inside its bucket (an independent hash)
+__device__ __forceinline__ uint32_t hub_sub(int32_t c, int slog) {
+  return slog == 0 ? 0u : (uint32_t)(((uint64_t)(uint32_t)c * 0xD6E8FEB86659FD93ull) >> (64 - slog));
+}
+// table slot (a third hash: the communities of one bucket share the top bits of the first)
+__device__ __forceinline__ uint32_t agg_slot(int32_t c) {
+  return (uint32_t)(((uint64_t)(uint32_t)c * 0xC2B2AE3D27D4EB4Full) >> (64 - kAggLog));
+}
+
 struct HubArgs {
-  const int32_t* hubs;
-  const int32_t* chunk_hub;
-  const int64_t* chunk_beg;
-  const int64_t* toff;
-  const int32_t* tlog;
-  int32_t* keys;
-  double* vals;
-  uint32_t* sawown;
+  const int32_t* hubs;        // [nhub] hub vertices
+  const int32_t* chunk_hub;   // [nchunk] hub of each chunk (a hub's chunks are consecutive)
+  const int64_t* chunk_beg;   // [nchunk] first CSR entry of the chunk
+  const int64_t* chunk_cbo;   // [nchunk] first of the chunk's bucket offsets in cb_off
+  const int64_t* chunk_stg;   // [nchunk] first staging slot of the chunk (hub entries in CSR order)
+  const int32_t* hub_plog;    // [nhub] log2 of the hub's bucket count
+  const int32_t* hub_cb0;     // [nhub + 1] first chunk of each hub
+  const int32_t* hub_bb0;     // [nhub + 1] first bucket of each hub
+  const int32_t* bucket_hub;  // [nbucket] hub of each bucket
+  uint16_t* cb_off;           // per chunk: 2^plog + 1 bucket offsets inside the chunk
+  unsigned long long* stage;  // [hub entries] community << 32 | weight bits, grouped by bucket per chunk
+  uint32_t* sawown;           // [nhub] a neighbour is in the hub's own community
+  HubPartial* part;           // [nbucket] best candidate and distinct count of each bucket
+  int64_t nbucket;
+};
+
+__global__ void __launch_bounds__(kThreads) hub_part_kernel(MoveArgs P, HubArgs H) {
+  __shared__ uint32_t cnt[1 << kHubMaxBucketsLog];
+  if (P.ctl->done) return;
+  const int64_t ch = blockIdx.x;
+  const int32_t h = H.chunk_hub[ch];
+  const int32_t i = H.hubs[h];
+  const int32_t own = P.comm[i];
+  const int64_t beg = H.chunk_beg[ch];
+  const int64_t end = min(beg + (int64_t)kHubChunk, P.off[i + 1]);
+  const int plog = H.hub_plog[h];
+  const int nb = 1 << plog;
+  for (int x = threadIdx.x; x < nb; x += kThreads) cnt[x] = 0;
+  __syncthreads();
+  int32_t c[kHubItems];
+  float w[kHubItems];
+#pragma unroll
+  for (int u = 0; u < kHubItems; ++u) {
+    const int64_t e = beg + u * kThreads + threadIdx.x;
+    c[u] = e < end ? __ldcs(P.col + e) : -1;
+    w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
+  }
+#pragma unroll
+  for (int u = 0; u < kHubItems; ++u) c[u] = c[u] >= 0 ? P.comm[c[u]] : -1;   // all gathers in flight
+  bool sawown = false;
+  uint32_t bk[kHubItems], rk[kHubItems];
+#pragma unroll
+  for (int u = 0; u < kHubItems; ++u) {
+    bk[u] = 0u;
+    rk[u] = 0u;
+    if (c[u] >= 0) {
+      sawown |= c[u] == own;
+      bk[u] = hub_bucket(c[u], plog);
+      rk[u] = atomicAdd(&cnt[bk[u]], 1u);
+    }
+  }
+  __syncthreads();
+  // bucket starts: each thread scans a run of consecutive buckets
+  const int per = (nb + kThreads - 1) / kThreads;
+  const int x0 = min((int)threadIdx.x * per, nb), x1 = min(x0 + per, nb);
+  uint32_t local = 0;
+  for (int x = x0; x < x1; ++x) local += cnt[x];
+  uint32_t total;
+  uint32_t run = block_exclusive_scan256<uint32_t>(local, &total);
+  uint16_t* off = H.cb_off + H.chunk_cbo[ch];
+  for (int x = x0; x < x1; ++x) {
+    const uint32_t v = cnt[x];
+    cnt[x] = run;
+    off[x] = (uint16_t)run;
+    run += v;
+  }
+  if (threadIdx.x == 0) off[nb] = (uint16_t)total;
+  __syncthreads();
+  unsigned long long* st = H.stage + H.chunk_stg[ch];
+#pragma unroll
+  for (int u = 0; u < kHubItems; ++u)
+    if (c[u] >= 0) st[cnt[bk[u]] + rk[u]] = ((unsigned long long)(uint32_t)c[u] << 32) | __float_as_uint(w[u]);
+  if (__syncthreads_or(sawown) && threadIdx.x == 0) atomicOr(&H.sawown[h], 1u);
+}
+
+// Shared-memory tables of hub_agg_kernel.  Packed (integral weights):
+// community << 32 | integer sum, all ones when empty, one atomic per entry.
+template <bool PACKED>
+struct AggTable {
+  unsigned long long slot[kAggSlots];
+  __device__ __forceinline__ void clear(int s) { slot[s] = kPackedEmpty; }
+  __device__ __forceinline__ void get(int s, int32_t& c, double& W) const {
+    c = (int32_t)(uint32_t)(slot[s] >> 32);
+    W = (double)(uint32_t)slot[s];
+  }
+  // 1: added to an existing community, 2: claimed a slot, 0: table full
+  __device__ __forceinline__ int insert(int32_t c, float w, uint32_t& where) {
+    const uint32_t wi = (uint32_t)w;
+    uint32_t h = agg_slot(c);
+    for (int p = 0; p < kAggSlots; ++p) {
+      const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&slot[h]);
+      if ((uint32_t)(cur >> 32) == (uint32_t)c) { atomicAdd(&slot[h], (unsigned long long)wi); return 1; }
+      if (cur == kPackedEmpty) {
+        const unsigned long long prev = atomicCAS(&slot[h], kPackedEmpty, ((unsigned long long)(uint32_t)c << 32) | wi);
+        if (prev == kPackedEmpty) { where = h; return 2; }
+        if ((uint32_t)(prev >> 32) == (uint32_t)c) { atomicAdd(&slot[h], (unsigned long long)wi); return 1; }
+      }
+      h = (h + 1) & (kAggSlots - 1);
+    }
+    return 0;
+  }
+};
+
+template <>
+struct AggTable<false> {
+  int32_t key[kAggSlots];
+  double val[kAggSlots];
+  __device__ __forceinline__ void clear(int s) { key[s] = -1; val[s] = 0.0; }
+  __device__ __forceinline__ void get(int s, int32_t& c, double& W) const { c = key[s]; W = val[s]; }
+  __device__ __forceinline__ int insert(int32_t c, float w, uint32_t& where) {
+    uint32_t h = agg_slot(c);
+    for (int p = 0; p < kAggSlots; ++p) {
+      const int32_t prev = atomicCAS(&key[h], -1, c);
+      if (prev == -1 || prev == c) {
+        atomicAdd(&val[h], (double)w);
+        if (prev == -1) { where = h; return 2; }
+        return 1;
+      }
+      h = (h + 1) & (kAggSlots - 1);
+    }
+    return 0;
+  }
+};
+
+struct AggCtl {
+  int64_t segbase[kThreads];   // staging slot of each segment's first pair
+  uint16_t claimed[kAggSlots];
+  int32_t segpre[kThreads + 1];
+  double rg[kThreads / 32], rw[kThreads / 32];
+  int32_t rc[kThreads / 32], rn[kThreads / 32];
+  int32_t nclaimed;
+  int32_t full;
 };
 
 template <bool PACKED>
-__global__ void __launch_bounds__(kThreads) hub_insert_kernel(MoveArgs P, HubArgs H) {
-  if (P.ctl->done) return;
-  int32_t h = H.chunk_hub[blockIdx.x];
-  int32_t i = H.hubs[h];
-  int32_t own = P.comm[i];
-  int64_t beg = H.chunk_beg[blockIdx.x];
-  int64_t end = min(beg + (int64_t)kHubChunk, P.off[i + 1]);
-  int32_t* keys = H.keys + H.toff[h];
-  double* vals = H.vals + H.toff[h];
-  unsigned long long* packed = reinterpret_cast<unsigned long long*>(vals);
-  int logT = H.tlog[h];
-  bool sawown = false, overflow = false;
-  for (int64_t e0 = beg + threadIdx.x; e0 < end; e0 += kUnroll * kThreads) {
-    int32_t c[kUnroll];
-    float wv[kUnroll];
-    gather4(P, e0, kThreads, end, c, wv);
-#pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      if (c[u] != kNone) {
-        sawown |= (c[u] == own);
-        const bool ok = PACKED ? packed_insert(packed, logT, c[u], (uint32_t)wv[u])
-                               : table_insert<double>(keys, vals, logT, c[u], (double)wv[u]);
-        if (!ok) overflow = true;
-      }
-    }
-  }
-  if (__syncthreads_or(sawown) && threadIdx.x == 0) atomicOr(&H.sawown[h], 1u);
-  if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
+constexpr size_t agg_smem_bytes() {
+  return sizeof(AggTable<PACKED>) + sizeof(AggCtl);
 }
 
-// ... then blocks scan 1024-slot segments of the hub tables (best candidate,
-// occupancy, clearing the slots) and one thread per hub combines its segments
-// in order and decides.
-constexpr int kHubSeg = 1024;
-
+// One block per (hub, bucket), blocks persistent over the buckets.  When a
+// bucket claims more than half the table, its communities are split by a
+// second hash into 2, 4, ... sub-passes, each re-reading the bucket's pairs,
+// until every sub-pass fits; a bucket still too full at 2^16 sub-passes sets
+// the pass's error flag (reported as a capacity error, never a wrong sum).
 template <bool PACKED>
-__global__ void __launch_bounds__(kThreads) hub_scan_kernel(MoveArgs P, HubArgs H, const int32_t* seg_hub,
-                                                            const int64_t* seg_beg, HubPartial* part) {
-  __shared__ double rg[kThreads / 32], rw[kThreads / 32];
-  __shared__ int32_t rc[kThreads / 32], rn[kThreads / 32];
+__global__ void __launch_bounds__(kThreads) hub_agg_kernel(MoveArgs P, HubArgs H) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  AggTable<PACKED>& T = *reinterpret_cast<AggTable<PACKED>*>(smem);
+  AggCtl& S = *reinterpret_cast<AggCtl*>(smem + sizeof(AggTable<PACKED>));
   if (P.ctl->done) return;
-  int32_t h = seg_hub[blockIdx.x];
-  int32_t i = H.hubs[h];
-  int64_t T = (int64_t)1 << H.tlog[h];
-  int64_t b0 = seg_beg[blockIdx.x];
-  int64_t b1 = min(b0 + (int64_t)kHubSeg, T);
-  int32_t* keys = H.keys + H.toff[h];
-  double* vals = H.vals + H.toff[h];
-  unsigned long long* packed = reinterpret_cast<unsigned long long*>(vals);
-  double kf = P.kfrac[i];
-  double bg = 0.0, bw = 0.0;
-  int32_t bc = kNone;
-  int nocc = 0;
-  for (int64_t s0 = b0 + threadIdx.x; s0 < b1; s0 += kUnroll * kThreads) {
-    int32_t c[kUnroll];
-    double W[kUnroll], t[kUnroll];
-#pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      const int64_t sl = s0 + u * kThreads;
-      if (PACKED) {
-        const unsigned long long x = sl < b1 ? packed[sl] : kPackedEmpty;
-        c[u] = x == kPackedEmpty ? -1 : (int32_t)(uint32_t)(x >> 32);
-        W[u] = c[u] >= 0 ? (double)(uint32_t)x : 0.0;
-      } else {
-        c[u] = sl < b1 ? keys[sl] : -1;
-        W[u] = c[u] >= 0 ? vals[sl] : 0.0;
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kUnroll; ++u) t[u] = (c[u] >= 0 && W[u] != 0.0) ? P.tot[c[u]] : 0.0;
-#pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      const int64_t sl = s0 + u * kThreads;
-      if (c[u] >= 0) {
-        ++nocc;
-        if (W[u] != 0.0) {
-          const double g = __dsub_rn(W[u], __dmul_rn(t[u], kf));
-          if (g > 0.0 && better(g, c[u], bg, bc)) { bg = g; bc = c[u]; bw = W[u]; }
-        }
-        if (PACKED) {
-          packed[sl] = kPackedEmpty;
-        } else {
-          keys[sl] = -1;
-          vals[sl] = 0.0;
-        }
-      }
-    }
-  }
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  warp_best(bg, bc, bw);
-  nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
-  if (lane == 0) { rg[w] = bg; rc[w] = bc; rw[w] = bw; rn[w] = nocc; }
+  for (int x = threadIdx.x; x < kAggSlots; x += kThreads) T.clear(x);
+  if (threadIdx.x == 0) { S.nclaimed = 0; S.full = 0; }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double g = rg[0], ww = rw[0];
-    int32_t c = rc[0];
-    int n = rn[0];
-    for (int k2 = 1; k2 < kThreads / 32; ++k2) {
-      if (better(rg[k2], rc[k2], g, c)) { g = rg[k2]; c = rc[k2]; ww = rw[k2]; }
-      n += rn[k2];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int64_t gb = blockIdx.x; gb < H.nbucket; gb += gridDim.x) {
+    const int32_t h = H.bucket_hub[gb];
+    const int32_t b = (int32_t)(gb - H.hub_bb0[h]);
+    const int32_t c0 = H.hub_cb0[h], K = H.hub_cb0[h + 1] - c0;
+    const double kf = P.kfrac[H.hubs[h]];
+    double bg = 0.0, bw = 0.0;
+    int32_t bc = kNone;
+    int nocc = 0;
+    for (int slog = 0;; ++slog) {
+      bg = 0.0; bw = 0.0; bc = kNone; nocc = 0;
+      bool split = false;
+      for (uint32_t sub = 0; sub < (1u << slog) && !split; ++sub) {
+        for (int32_t k0 = 0; k0 < K; k0 += kThreads) {
+          const int32_t k = k0 + (int32_t)threadIdx.x;
+          int64_t base = 0;
+          int32_t len = 0;
+          if (k < K) {
+            const uint16_t* off = H.cb_off + H.chunk_cbo[c0 + k];
+            base = H.chunk_stg[c0 + k] + off[b];
+            len = (int32_t)off[b + 1] - (int32_t)off[b];
+          }
+          int32_t tot;
+          const int32_t pre = block_exclusive_scan256<int32_t>(len, &tot);
+          S.segpre[threadIdx.x] = pre;
+          S.segbase[threadIdx.x] = base;
+          __syncthreads();
+          const int nseg = min(kThreads, K - k0);
+          for (int32_t q = threadIdx.x; q < tot; q += kThreads) {
+            if (*reinterpret_cast<volatile int32_t*>(&S.full)) break;   // this sub-pass is discarded anyway
+            int jlo = 0, jhi = nseg - 1;                 // last segment starting at or before q
+            while (jlo < jhi) {
+              const int mid = (jlo + jhi + 1) >> 1;
+              if (S.segpre[mid] <= q) jlo = mid; else jhi = mid - 1;
+            }
+            const unsigned long long x = H.stage[S.segbase[jlo] + (q - S.segpre[jlo])];
+            const int32_t c = (int32_t)(uint32_t)(x >> 32);
+            if (slog > 0 && hub_sub(c, slog) != sub) continue;
+            uint32_t where = 0;
+            const int r = T.insert(c, __uint_as_float((uint32_t)x), where);
+            if (r == 2) {
+              const int n = atomicAdd(&S.nclaimed, 1);
+              S.claimed[n] = (uint16_t)where;
+              if (n + 1 > kAggFull) S.full = 1;
+            } else if (r == 0) {
+              S.full = 1;
+            }
+          }
+          __syncthreads();
+        }
+        const bool full = S.full != 0;
+        const int nc = S.nclaimed;
+        for (int x = threadIdx.x; x < nc; x += kThreads) {
+          const int sl = S.claimed[x];
+          if (!full) {
+            int32_t c;
+            double W;
+            T.get(sl, c, W);
+            ++nocc;
+            if (W != 0.0) {                                            // OneLevelKernel.cu:303
+              const double g = __dsub_rn(W, __dmul_rn(P.tot[c], kf));  // OneLevelKernel.cu:307-313
+              if (g > 0.0 && better(g, c, bg, bc)) { bg = g; bc = c; bw = W; }
+            }
+          }
+          T.clear(sl);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) { S.nclaimed = 0; S.full = 0; }
+        __syncthreads();
+        split = full;
+      }
+      if (!split) break;
+      if (slog == kAggMaxSplitLog) {
+        if (threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
+        break;
+      }
     }
-    part[blockIdx.x] = HubPartial{g, ww, c, n};
+    warp_best(bg, bc, bw);
+    nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
+    if (lane == 0) { S.rg[wid] = bg; S.rc[wid] = bc; S.rw[wid] = bw; S.rn[wid] = nocc; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double g = S.rg[0], ww = S.rw[0];
+      int32_t c = S.rc[0];
+      int n = S.rn[0];
+      for (int k2 = 1; k2 < kThreads / 32; ++k2) {
+        if (better(S.rg[k2], S.rc[k2], g, c)) { g = S.rg[k2]; c = S.rc[k2]; ww = S.rw[k2]; }
+        n += S.rn[k2];
+      }
+      H.part[gb] = HubPartial{g, ww, c, n};
+    }
+    __syncthreads();
   }
 }
 
-__global__ void hub_decide_kernel(MoveArgs P, HubArgs H, const int32_t* hub_seg0, const HubPartial* part,
-                                  int64_t nhub) {
+__global__ void hub_decide_kernel(MoveArgs P, HubArgs H, int64_t nhub) {
   if (P.ctl->done) return;
   int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (h >= nhub) return;
@@ -1302,8 +1452,8 @@ __global__ void hub_decide_kernel(MoveArgs P, HubArgs H, const int32_t* hub_seg0
   double g = 0.0, ww = 0.0;
   int32_t c = kNone;
   int n = 0;
-  for (int32_t sg = hub_seg0[h]; sg < hub_seg0[h + 1]; ++sg) {
-    HubPartial q = part[sg];
+  for (int32_t bk = H.hub_bb0[h]; bk < H.hub_bb0[h + 1]; ++bk) {
+    HubPartial q = H.part[bk];
     if (better(q.g, q.c, g, c)) { g = q.g; c = q.c; ww = q.w; }
     n += q.n;
   }
@@ -1879,9 +2029,9 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
     k32_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, g.k, g.k32);
     LVG_LAUNCH();
   }
-  // hub tables
+  // hubs: chunks of kHubChunk entries and ~kHubBucketTarget entries per bucket
   g.nchunk = 0;
-  g.hub_slots = 0;
+  g.nhub_bucket = 0;
   const int64_t nhub = g.nbucket[kBHub];
   if (nhub > 0) {
     const int32_t* hubs = g.blist + g.bstart[kBHub];
@@ -1894,52 +2044,51 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
       LVG_CUDA(cudaMemcpyAsync(be.data(), d_be, sizeof(int64_t) * 2 * nhub, cudaMemcpyDeviceToHost, s));
       LVG_CUDA(cudaStreamSynchronize(s));
     }
-    std::vector<int64_t> toff(nhub);
-    std::vector<int32_t> tlog(nhub), chub, shub, seg0(nhub + 1);
-    std::vector<int64_t> cbeg, sbeg;
-    int64_t slots = 0;
+    std::vector<int32_t> plog(nhub), cb0(nhub + 1), bb0(nhub + 1), chub, bhub;
+    std::vector<int64_t> cbeg, cbo, cstg;
+    int64_t noff = 0, nstg = 0;
     for (int64_t h = 0; h < nhub; ++h) {
-      int64_t d = be[2 * h + 1] - be[2 * h];
-      int l = 5;
-      while (((int64_t)1 << l) < 2 * d) ++l;
-      toff[h] = slots;
-      tlog[h] = l;
-      slots += (int64_t)1 << l;
+      const int64_t d = be[2 * h + 1] - be[2 * h];
+      int l = 0;
+      while (l < kHubMaxBucketsLog && ((int64_t)kHubBucketTarget << l) < d) ++l;
+      plog[h] = l;
+      cb0[h] = (int32_t)chub.size();
+      bb0[h] = (int32_t)bhub.size();
       for (int64_t b = be[2 * h]; b < be[2 * h + 1]; b += kHubChunk) {
         chub.push_back((int32_t)h);
         cbeg.push_back(b);
+        cbo.push_back(noff);
+        cstg.push_back(nstg + (b - be[2 * h]));
+        noff += ((int64_t)1 << l) + 1;
       }
-      seg0[h] = (int32_t)shub.size();
-      for (int64_t b = 0; b < ((int64_t)1 << l); b += kHubSeg) {
-        shub.push_back((int32_t)h);
-        sbeg.push_back(b);
-      }
+      nstg += d;
+      bhub.insert(bhub.end(), (size_t)1 << l, (int32_t)h);
     }
-    seg0[nhub] = (int32_t)shub.size();
-    g.nseg = (int64_t)shub.size();
-    g.seg_hub = a.lo_n<int32_t>(g.nseg);
-    g.seg_beg = a.lo_n<int64_t>(g.nseg);
-    g.hub_seg0 = a.lo_n<int32_t>(nhub + 1);
-    g.hub_part = a.lo_n<HubPartial>(g.nseg);
-    LVG_CUDA(cudaMemcpyAsync(g.seg_hub, shub.data(), sizeof(int32_t) * g.nseg, cudaMemcpyHostToDevice, s));
-    LVG_CUDA(cudaMemcpyAsync(g.seg_beg, sbeg.data(), sizeof(int64_t) * g.nseg, cudaMemcpyHostToDevice, s));
-    LVG_CUDA(cudaMemcpyAsync(g.hub_seg0, seg0.data(), sizeof(int32_t) * (nhub + 1), cudaMemcpyHostToDevice, s));
-    g.hub_slots = slots;
+    cb0[nhub] = (int32_t)chub.size();
+    bb0[nhub] = (int32_t)bhub.size();
     g.nchunk = (int64_t)chub.size();
-    g.hub_toff = a.lo_n<int64_t>(nhub);
-    g.hub_tlog = a.lo_n<int32_t>(nhub);
+    g.nhub_bucket = (int64_t)bhub.size();
     g.chunk_hub = a.lo_n<int32_t>(g.nchunk);
     g.chunk_beg = a.lo_n<int64_t>(g.nchunk);
-    g.hub_keys = a.lo_n<int32_t>(slots);
-    g.hub_vals = a.lo_n<double>(slots);
+    g.chunk_cbo = a.lo_n<int64_t>(g.nchunk);
+    g.chunk_stg = a.lo_n<int64_t>(g.nchunk);
+    g.hub_plog = a.lo_n<int32_t>(nhub);
+    g.hub_cb0 = a.lo_n<int32_t>(nhub + 1);
+    g.hub_bb0 = a.lo_n<int32_t>(nhub + 1);
+    g.bucket_hub = a.lo_n<int32_t>(g.nhub_bucket);
+    g.cb_off = a.lo_n<uint16_t>(noff);
+    g.stage = a.lo_n<unsigned long long>(nstg);
     g.hub_sawown = a.lo_n<uint32_t>(nhub);
-    LVG_CUDA(cudaMemcpyAsync(g.hub_toff, toff.data(), sizeof(int64_t) * nhub, cudaMemcpyHostToDevice, s));
-    LVG_CUDA(cudaMemcpyAsync(g.hub_tlog, tlog.data(), sizeof(int32_t) * nhub, cudaMemcpyHostToDevice, s));
+    g.hub_part = a.lo_n<HubPartial>(g.nhub_bucket);
     LVG_CUDA(cudaMemcpyAsync(g.chunk_hub, chub.data(), sizeof(int32_t) * g.nchunk, cudaMemcpyHostToDevice, s));
     LVG_CUDA(cudaMemcpyAsync(g.chunk_beg, cbeg.data(), sizeof(int64_t) * g.nchunk, cudaMemcpyHostToDevice, s));
-    LVG_CUDA(cudaMemsetAsync(g.hub_keys, 0xff, sizeof(int32_t) * slots, s));
-    // integral weights: hub_vals holds packed (community, sum) slots, empty = all ones
-    LVG_CUDA(cudaMemsetAsync(g.hub_vals, g.int_acc ? 0xff : 0, sizeof(double) * slots, s));
+    LVG_CUDA(cudaMemcpyAsync(g.chunk_cbo, cbo.data(), sizeof(int64_t) * g.nchunk, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.chunk_stg, cstg.data(), sizeof(int64_t) * g.nchunk, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.hub_plog, plog.data(), sizeof(int32_t) * nhub, cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.hub_cb0, cb0.data(), sizeof(int32_t) * (nhub + 1), cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.hub_bb0, bb0.data(), sizeof(int32_t) * (nhub + 1), cudaMemcpyHostToDevice, s));
+    LVG_CUDA(cudaMemcpyAsync(g.bucket_hub, bhub.data(), sizeof(int32_t) * g.nhub_bucket, cudaMemcpyHostToDevice,
+                             s));
     LVG_CUDA(cudaMemsetAsync(g.hub_sawown, 0, sizeof(uint32_t) * nhub, s));
     LVG_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
   }
@@ -2048,6 +2197,10 @@ static void set_move_attributes(int block_log) {
                                 (int)sizeof(TileSmem<double>)));
   LVG_CUDA(cudaFuncSetAttribute(move_tile_packed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(TilePackedSmem)));
+  LVG_CUDA(cudaFuncSetAttribute(hub_agg_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)agg_smem_bytes<true>()));
+  LVG_CUDA(cudaFuncSetAttribute(hub_agg_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)agg_smem_bytes<false>()));
   size_t smem = ((size_t)1 << block_log) * (sizeof(double) + sizeof(int32_t));
   LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   smem = ((size_t)1 << block_log) * (sizeof(int32_t) + sizeof(int32_t));
@@ -2094,20 +2247,19 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
   if (nhub > 0) {
     HubArgs H;
     H.hubs = g.blist + g.bstart[kBHub];
-    H.chunk_hub = g.chunk_hub; H.chunk_beg = g.chunk_beg;
-    H.toff = g.hub_toff; H.tlog = g.hub_tlog;
-    H.keys = g.hub_keys; H.vals = g.hub_vals; H.sawown = g.hub_sawown;
-    if (g.int_acc) {
-      hub_insert_kernel<true><<<(unsigned)g.nchunk, kThreads, 0, sh>>>(P, H);
-      LVG_LAUNCH();
-      hub_scan_kernel<true><<<(unsigned)g.nseg, kThreads, 0, sh>>>(P, H, g.seg_hub, g.seg_beg, g.hub_part);
-    } else {
-      hub_insert_kernel<false><<<(unsigned)g.nchunk, kThreads, 0, sh>>>(P, H);
-      LVG_LAUNCH();
-      hub_scan_kernel<false><<<(unsigned)g.nseg, kThreads, 0, sh>>>(P, H, g.seg_hub, g.seg_beg, g.hub_part);
-    }
+    H.chunk_hub = g.chunk_hub; H.chunk_beg = g.chunk_beg; H.chunk_cbo = g.chunk_cbo; H.chunk_stg = g.chunk_stg;
+    H.hub_plog = g.hub_plog; H.hub_cb0 = g.hub_cb0; H.hub_bb0 = g.hub_bb0; H.bucket_hub = g.bucket_hub;
+    H.cb_off = g.cb_off; H.stage = g.stage; H.sawown = g.hub_sawown; H.part = g.hub_part;
+    H.nbucket = g.nhub_bucket;
+    hub_part_kernel<<<(unsigned)g.nchunk, kThreads, 0, sh>>>(P, H);
     LVG_LAUNCH();
-    hub_decide_kernel<<<grid_for(nhub, 128), 128, 0, sh>>>(P, H, g.hub_seg0, g.hub_part, nhub);
+    const size_t smem = g.int_acc ? agg_smem_bytes<true>() : agg_smem_bytes<false>();
+    const int per_sm = std::max(1, std::min(8, (int)((227u * 1024u) / (smem + 1024))));
+    const int64_t grid = std::min<int64_t>(g.nhub_bucket, (int64_t)sm_count() * per_sm);
+    if (g.int_acc) hub_agg_kernel<true><<<(unsigned)grid, kThreads, smem, sh>>>(P, H);
+    else hub_agg_kernel<false><<<(unsigned)grid, kThreads, smem, sh>>>(P, H);
+    LVG_LAUNCH();
+    hub_decide_kernel<<<grid_for(nhub, 128), 128, 0, sh>>>(P, H, nhub);
     LVG_LAUNCH();
   }
   if (g.nbucket[kBBlock] > 0) {

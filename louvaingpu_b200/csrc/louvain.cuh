@@ -64,21 +64,22 @@ struct LevelGraph {
   int64_t ntiles = 0;
   bool int_acc = false;           // integral weights, degrees < 2^30: exact int32 sums
   int32_t* k32 = nullptr;         // k as int32 when int_acc (the first pass's gathered totals)
-  // hub tables
-  int64_t hub_slots = 0;
-  int64_t* hub_toff = nullptr;    // [nhub] table offset
-  int32_t* hub_tlog = nullptr;    // [nhub] log2 table size
+  // hubs: 4096-entry chunks of the hub rows, each hub's communities hashed
+  // into a power-of-two number of buckets (see hub_part/hub_agg kernels)
   int32_t* chunk_hub = nullptr;   // [nchunk] hub index of the chunk
   int64_t* chunk_beg = nullptr;   // [nchunk] first CSR entry of the chunk
+  int64_t* chunk_cbo = nullptr;   // [nchunk] first of the chunk's bucket offsets in cb_off
+  int64_t* chunk_stg = nullptr;   // [nchunk] first staging slot of the chunk
   int64_t nchunk = 0;
-  int32_t* hub_keys = nullptr;
-  double* hub_vals = nullptr;
+  int32_t* hub_plog = nullptr;    // [nhub] log2 bucket count
+  int32_t* hub_cb0 = nullptr;     // [nhub+1] first chunk of each hub
+  int32_t* hub_bb0 = nullptr;     // [nhub+1] first bucket of each hub
+  int32_t* bucket_hub = nullptr;  // [nhub_bucket] hub of each bucket
+  int64_t nhub_bucket = 0;
+  uint16_t* cb_off = nullptr;     // per chunk: bucket offsets inside the chunk
+  unsigned long long* stage = nullptr;  // [hub entries] pairs grouped by bucket per chunk
   uint32_t* hub_sawown = nullptr;
-  int64_t nseg = 0;               // 8192-slot segments of the hub tables
-  int32_t* seg_hub = nullptr;
-  int64_t* seg_beg = nullptr;
-  int32_t* hub_seg0 = nullptr;    // [nhub+1] first segment of each hub
-  struct HubPartial* hub_part = nullptr;
+  struct HubPartial* hub_part = nullptr;  // [nhub_bucket]
   // singleton first pass: chunks {vertex, piece} of the rows longer than 32,
   // rows of more than one chunk {vertex, first chunk}, per-chunk partials
   int2* sp_chunk = nullptr;
