@@ -40,14 +40,6 @@ constexpr int kThreads = 256;
 constexpr int kHubChunk = 4096;
 constexpr int kNone = INT_MAX;
 
-__device__ __forceinline__ uint32_t hash_c(int32_t c, int logT) {
-  return (uint32_t)(((uint64_t)(uint32_t)c * 0x9E3779B97F4A7C15ull) >> (64 - logT));
-}
-
-__device__ __forceinline__ int ceil_log2(int64_t x) {  // x >= 1
-  return x <= 1 ? 0 : 64 - __clzll((unsigned long long)(x - 1));
-}
-
 // ------------------------------------------------------------------ validate
 __global__ void validate_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
                                 int32_t V, uint32_t* bad) {
@@ -403,124 +395,9 @@ __device__ __forceinline__ void apply_decision(const MoveArgs& P, int32_t i, int
   }
 }
 
-// Open-addressing insert of (c, w) into a table of 2^logT slots.
-template <typename Acc>
-__device__ __forceinline__ bool table_insert(int32_t* keys, Acc* vals, int logT, int32_t c, Acc w) {
-  uint32_t T = 1u << logT;
-  uint32_t h = hash_c(c, logT);
-  for (uint32_t p = 0; p < T; ++p) {
-    int32_t prev = atomicCAS(&keys[h], -1, c);
-    if (prev == -1 || prev == c) { atomicAdd(&vals[h], w); return true; }
-    h = (h + 1) & (T - 1);
-  }
-  return false;
-}
-
 // Packed (community << 32 | integer sum) slots are all ones when empty; the
 // add of an integral weight cannot carry into the key (sums stay below 2^30).
 constexpr unsigned long long kPackedEmpty = ~0ull;
-
-// Entries [e0 + u*stride) of a row, u < 4: columns and weights first, then
-// the four community gathers, so that each thread keeps several loads in
-// flight; kNone marks entries past `end`.
-constexpr int kUnroll = 4;
-__device__ __forceinline__ void gather4(const MoveArgs& P, int64_t e0, int64_t stride, int64_t end,
-                                        int32_t (&c)[kUnroll], float (&w)[kUnroll]) {
-  int32_t col[kUnroll];
-#pragma unroll
-  for (int u = 0; u < kUnroll; ++u) {
-    const int64_t e = e0 + u * stride;
-    col[u] = e < end ? __ldcs(P.col + e) : -1;
-    w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
-  }
-#pragma unroll
-  for (int u = 0; u < kUnroll; ++u) c[u] = col[u] >= 0 ? P.comm[col[u]] : kNone;
-}
-
-// Block per vertex (degree up to block_max), table in dynamic shared memory;
-// int32 sums when the weights are integral (exact, half the table bytes).
-template <typename Acc>
-__global__ void __launch_bounds__(kThreads) move_block_kernel(MoveArgs P, int maxLog, int64_t dlo, int64_t dhi) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ double rg[kThreads / 32], rw[kThreads / 32];
-  __shared__ int32_t rc[kThreads / 32], rn[kThreads / 32], rs[kThreads / 32];
-  if (P.ctl->done) return;
-  const int Tmax = 1 << maxLog;
-  Acc* vals = reinterpret_cast<Acc*>(smem);
-  int32_t* keys = reinterpret_cast<int32_t*>(vals + Tmax);
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int s = threadIdx.x; s < Tmax; s += kThreads) { keys[s] = -1; vals[s] = Acc(0); }
-  __syncthreads();
-  bool overflow = false;
-  for (int64_t item = blockIdx.x; item < P.n; item += gridDim.x) {
-    int32_t i = P.list[item];
-    int64_t beg = P.off[i], end = P.off[i + 1];
-    if (end - beg <= dlo || end - beg > dhi) continue;   // another launch takes this degree
-    int32_t own = P.comm[i];
-    int logT = min(maxLog, max(5, ceil_log2(2 * (end - beg))));
-    int T = 1 << logT;
-    bool sawown = false;
-    for (int64_t e0 = beg + threadIdx.x; e0 < end; e0 += kUnroll * kThreads) {
-      int32_t c[kUnroll];
-      float wv[kUnroll];
-      gather4(P, e0, kThreads, end, c, wv);
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        if (c[u] != kNone) {
-          sawown |= (c[u] == own);
-          if (!table_insert<Acc>(keys, vals, logT, c[u], (Acc)wv[u])) overflow = true;
-        }
-      }
-    }
-    __syncthreads();
-    double kf = P.kfrac[i];
-    double bg = 0.0, bw = 0.0;
-    int32_t bc = kNone;
-    int nocc = 0;
-    for (int s0 = threadIdx.x; s0 < T; s0 += kUnroll * kThreads) {
-      int32_t c[kUnroll];
-      double W[kUnroll], t[kUnroll];
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        const int s = s0 + u * kThreads;
-        c[u] = s < T ? keys[s] : -1;
-        W[u] = c[u] >= 0 ? (double)vals[s] : 0.0;
-        if (c[u] >= 0) { keys[s] = -1; vals[s] = Acc(0); }
-      }
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) t[u] = (c[u] >= 0 && W[u] != 0.0) ? P.tot[c[u]] : 0.0;
-#pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
-        if (c[u] >= 0) {
-          ++nocc;
-          if (W[u] != 0.0) {                                            // OneLevelKernel.cu:303
-            const double g = __dsub_rn(W[u], __dmul_rn(t[u], kf));      // OneLevelKernel.cu:307-313
-            if (g > 0.0 && better(g, c[u], bg, bc)) { bg = g; bc = c[u]; bw = W[u]; }
-          }
-        }
-      }
-    }
-    warp_best(bg, bc, bw);
-    nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
-    int so = __any_sync(0xffffffffu, sawown) ? 1 : 0;
-    if (lane == 0) { rg[w] = bg; rc[w] = bc; rw[w] = bw; rn[w] = nocc; rs[w] = so; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double g = rg[0], ww = rw[0];
-      int32_t c = rc[0];
-      int n = rn[0], sw = rs[0];
-      for (int k2 = 1; k2 < kThreads / 32; ++k2) {
-        if (better(rg[k2], rc[k2], g, c)) { g = rg[k2]; c = rc[k2]; ww = rw[k2]; }
-        n += rn[k2];
-        sw |= rs[k2];
-      }
-      int32_t nseg = n + ((P.has_loop[i] && !sw) ? 1 : 0);
-      apply_decision(P, i, own, c, ww, nseg);
-    }
-    __syncthreads();
-  }
-  if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
-}
 
 // ----------------------------------------------------------------- ELL kernels
 // Degree <= 32: vertices of class D (4, 8, 16, 32) keep their entries in a
@@ -666,7 +543,6 @@ __global__ void __launch_bounds__(kThreads) sp_thread_kernel(MoveArgs P, EllArgs
 // sp_combine_kernel.
 constexpr int kSpChunk = 512;
 constexpr int kSpUnroll = 4;     // entries per lane in flight
-constexpr bool kBlockSplit = true;
 
 __global__ void __launch_bounds__(kThreads) sp_chunk_kernel(MoveArgs P, const int2* chunks, int64_t nch,
                                                             HubPartial* part) {
@@ -1319,6 +1195,11 @@ struct AggTable<false> {
   }
 };
 
+struct int2x64 {
+  int64_t base;
+  int32_t len;
+};
+
 struct AggCtl {
   int64_t segbase[kThreads];   // staging slot of each segment's first pair
   uint16_t claimed[kAggSlots];
@@ -1334,112 +1215,138 @@ constexpr size_t agg_smem_bytes() {
   return sizeof(AggTable<PACKED>) + sizeof(AggCtl);
 }
 
-// One block per (hub, bucket), blocks persistent over the buckets.  When a
-// bucket claims more than half the table, its communities are split by a
-// second hash into 2, 4, ... sub-passes, each re-reading the bucket's pairs,
-// until every sub-pass fits; a bucket still too full at 2^16 sub-passes sets
-// the pass's error flag (reported as a capacity error, never a wrong sum).
+struct AggBest {
+  double g, w;
+  int32_t c, n;
+};
+
+// Sums the staged pairs of K segments (segment k starts at staging slot
+// seg(k).x and holds seg(k).y pairs) per community in the shared table T,
+// and leaves the best candidate (gain w - tot_c * kf, higher gain then lower
+// community; OneLevelKernel.cu:303,307-313,330,358) and the count of distinct
+// communities in thread 0.  The table is left empty.  When the pairs claim
+// more than half the table, the communities are split by a second hash into
+// 2, 4, ... sub-passes, each re-reading the pairs, until every sub-pass fits;
+// still too full at 2^16 sub-passes, the pass's error flag is set (reported
+// as a capacity error, never a wrong sum).  All threads of the block call it.
+template <bool PACKED, typename SegFn>
+__device__ AggBest agg_segments(const MoveArgs& P, AggTable<PACKED>& T, AggCtl& S, const unsigned long long* stage,
+                                int32_t K, SegFn seg, double kf) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double bg = 0.0, bw = 0.0;
+  int32_t bc = kNone;
+  int nocc = 0;
+  for (int slog = 0;; ++slog) {
+    bg = 0.0; bw = 0.0; bc = kNone; nocc = 0;
+    bool split = false;
+    for (uint32_t sub = 0; sub < (1u << slog) && !split; ++sub) {
+      for (int32_t k0 = 0; k0 < K; k0 += kThreads) {
+        const int32_t k = k0 + (int32_t)threadIdx.x;
+        int64_t base = 0;
+        int32_t len = 0;
+        if (k < K) {
+          const int2x64 sg = seg(k);
+          base = sg.base;
+          len = sg.len;
+        }
+        int32_t tot;
+        const int32_t pre = block_exclusive_scan256<int32_t>(len, &tot);
+        S.segpre[threadIdx.x] = pre;
+        S.segbase[threadIdx.x] = base;
+        __syncthreads();
+        const int nseg = min(kThreads, K - k0);
+        for (int32_t q = threadIdx.x; q < tot; q += kThreads) {
+          if (*reinterpret_cast<volatile int32_t*>(&S.full)) break;   // this sub-pass is discarded anyway
+          int jlo = 0, jhi = nseg - 1;                 // last segment starting at or before q
+          while (jlo < jhi) {
+            const int mid = (jlo + jhi + 1) >> 1;
+            if (S.segpre[mid] <= q) jlo = mid; else jhi = mid - 1;
+          }
+          const unsigned long long x = stage[S.segbase[jlo] + (q - S.segpre[jlo])];
+          const int32_t c = (int32_t)(uint32_t)(x >> 32);
+          if (slog > 0 && hub_sub(c, slog) != sub) continue;
+          uint32_t where = 0;
+          const int r = T.insert(c, __uint_as_float((uint32_t)x), where);
+          if (r == 2) {
+            const int n = atomicAdd(&S.nclaimed, 1);
+            S.claimed[n] = (uint16_t)where;
+            if (n + 1 > kAggFull) S.full = 1;
+          } else if (r == 0) {
+            S.full = 1;
+          }
+        }
+        __syncthreads();
+      }
+      const bool full = S.full != 0;
+      const int nc = S.nclaimed;
+      for (int x = threadIdx.x; x < nc; x += kThreads) {
+        const int sl = S.claimed[x];
+        if (!full) {
+          int32_t c;
+          double W;
+          T.get(sl, c, W);
+          ++nocc;
+          if (W != 0.0) {                                            // OneLevelKernel.cu:303
+            const double g = __dsub_rn(W, __dmul_rn(P.tot[c], kf));  // OneLevelKernel.cu:307-313
+            if (g > 0.0 && better(g, c, bg, bc)) { bg = g; bc = c; bw = W; }
+          }
+        }
+        T.clear(sl);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) { S.nclaimed = 0; S.full = 0; }
+      __syncthreads();
+      split = full;
+    }
+    if (!split) break;
+    if (slog == kAggMaxSplitLog) {
+      if (threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
+      break;
+    }
+  }
+  warp_best(bg, bc, bw);
+  nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
+  if (lane == 0) { S.rg[wid] = bg; S.rc[wid] = bc; S.rw[wid] = bw; S.rn[wid] = nocc; }
+  __syncthreads();
+  AggBest r{S.rg[0], S.rw[0], S.rc[0], S.rn[0]};
+  if (threadIdx.x == 0) {
+    for (int k2 = 1; k2 < kThreads / 32; ++k2) {
+      if (better(S.rg[k2], S.rc[k2], r.g, r.c)) { r.g = S.rg[k2]; r.c = S.rc[k2]; r.w = S.rw[k2]; }
+      r.n += S.rn[k2];
+    }
+  }
+  __syncthreads();
+  return r;   // valid in thread 0
+}
+
+template <bool PACKED>
+__device__ __forceinline__ void agg_init(AggTable<PACKED>& T, AggCtl& S) {
+  for (int x = threadIdx.x; x < kAggSlots; x += kThreads) T.clear(x);
+  if (threadIdx.x == 0) { S.nclaimed = 0; S.full = 0; }
+  __syncthreads();
+}
+
+// One block per (hub, bucket), blocks persistent over the buckets: the
+// bucket's segments are its slice of every chunk of the hub.
 template <bool PACKED>
 __global__ void __launch_bounds__(kThreads) hub_agg_kernel(MoveArgs P, HubArgs H) {
   extern __shared__ __align__(16) unsigned char smem[];
   AggTable<PACKED>& T = *reinterpret_cast<AggTable<PACKED>*>(smem);
   AggCtl& S = *reinterpret_cast<AggCtl*>(smem + sizeof(AggTable<PACKED>));
   if (P.ctl->done) return;
-  for (int x = threadIdx.x; x < kAggSlots; x += kThreads) T.clear(x);
-  if (threadIdx.x == 0) { S.nclaimed = 0; S.full = 0; }
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  agg_init(T, S);
   for (int64_t gb = blockIdx.x; gb < H.nbucket; gb += gridDim.x) {
     const int32_t h = H.bucket_hub[gb];
     const int32_t b = (int32_t)(gb - H.hub_bb0[h]);
     const int32_t c0 = H.hub_cb0[h], K = H.hub_cb0[h + 1] - c0;
-    const double kf = P.kfrac[H.hubs[h]];
-    double bg = 0.0, bw = 0.0;
-    int32_t bc = kNone;
-    int nocc = 0;
-    for (int slog = 0;; ++slog) {
-      bg = 0.0; bw = 0.0; bc = kNone; nocc = 0;
-      bool split = false;
-      for (uint32_t sub = 0; sub < (1u << slog) && !split; ++sub) {
-        for (int32_t k0 = 0; k0 < K; k0 += kThreads) {
-          const int32_t k = k0 + (int32_t)threadIdx.x;
-          int64_t base = 0;
-          int32_t len = 0;
-          if (k < K) {
-            const uint16_t* off = H.cb_off + H.chunk_cbo[c0 + k];
-            base = H.chunk_stg[c0 + k] + off[b];
-            len = (int32_t)off[b + 1] - (int32_t)off[b];
-          }
-          int32_t tot;
-          const int32_t pre = block_exclusive_scan256<int32_t>(len, &tot);
-          S.segpre[threadIdx.x] = pre;
-          S.segbase[threadIdx.x] = base;
-          __syncthreads();
-          const int nseg = min(kThreads, K - k0);
-          for (int32_t q = threadIdx.x; q < tot; q += kThreads) {
-            if (*reinterpret_cast<volatile int32_t*>(&S.full)) break;   // this sub-pass is discarded anyway
-            int jlo = 0, jhi = nseg - 1;                 // last segment starting at or before q
-            while (jlo < jhi) {
-              const int mid = (jlo + jhi + 1) >> 1;
-              if (S.segpre[mid] <= q) jlo = mid; else jhi = mid - 1;
-            }
-            const unsigned long long x = H.stage[S.segbase[jlo] + (q - S.segpre[jlo])];
-            const int32_t c = (int32_t)(uint32_t)(x >> 32);
-            if (slog > 0 && hub_sub(c, slog) != sub) continue;
-            uint32_t where = 0;
-            const int r = T.insert(c, __uint_as_float((uint32_t)x), where);
-            if (r == 2) {
-              const int n = atomicAdd(&S.nclaimed, 1);
-              S.claimed[n] = (uint16_t)where;
-              if (n + 1 > kAggFull) S.full = 1;
-            } else if (r == 0) {
-              S.full = 1;
-            }
-          }
-          __syncthreads();
-        }
-        const bool full = S.full != 0;
-        const int nc = S.nclaimed;
-        for (int x = threadIdx.x; x < nc; x += kThreads) {
-          const int sl = S.claimed[x];
-          if (!full) {
-            int32_t c;
-            double W;
-            T.get(sl, c, W);
-            ++nocc;
-            if (W != 0.0) {                                            // OneLevelKernel.cu:303
-              const double g = __dsub_rn(W, __dmul_rn(P.tot[c], kf));  // OneLevelKernel.cu:307-313
-              if (g > 0.0 && better(g, c, bg, bc)) { bg = g; bc = c; bw = W; }
-            }
-          }
-          T.clear(sl);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) { S.nclaimed = 0; S.full = 0; }
-        __syncthreads();
-        split = full;
-      }
-      if (!split) break;
-      if (slog == kAggMaxSplitLog) {
-        if (threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
-        break;
-      }
-    }
-    warp_best(bg, bc, bw);
-    nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
-    if (lane == 0) { S.rg[wid] = bg; S.rc[wid] = bc; S.rw[wid] = bw; S.rn[wid] = nocc; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double g = S.rg[0], ww = S.rw[0];
-      int32_t c = S.rc[0];
-      int n = S.rn[0];
-      for (int k2 = 1; k2 < kThreads / 32; ++k2) {
-        if (better(S.rg[k2], S.rc[k2], g, c)) { g = S.rg[k2]; c = S.rc[k2]; ww = S.rw[k2]; }
-        n += S.rn[k2];
-      }
-      H.part[gb] = HubPartial{g, ww, c, n};
-    }
-    __syncthreads();
+    const AggBest r = agg_segments<PACKED>(
+        P, T, S, H.stage, K,
+        [&](int32_t k) {
+          const uint16_t* off = H.cb_off + H.chunk_cbo[c0 + k];
+          return int2x64{H.chunk_stg[c0 + k] + off[b], (int32_t)off[b + 1] - (int32_t)off[b]};
+        },
+        P.kfrac[H.hubs[h]]);
+    if (threadIdx.x == 0) H.part[gb] = HubPartial{r.g, r.w, r.c, r.n};
   }
 }
 
@@ -1461,6 +1368,78 @@ __global__ void hub_decide_kernel(MoveArgs P, HubArgs H, int64_t nhub) {
   H.sawown[h] = 0;
   int32_t nseg = n + ((P.has_loop[i] && !sw) ? 1 : 0);
   apply_decision(P, i, own, c, ww, nseg);
+}
+
+// Block class (tile_max < degree <= block_max), two launches per pass:
+// block_stage_kernel -- a warp per row gathers the neighbours' communities
+// and writes the row's (community, weight) pairs to staging (up to eight
+// gathers in flight per lane, no shared memory, no block barriers);
+// block_agg_kernel -- a block per row sums the staged pairs in a shared
+// table and decides.  Splitting the gathers from the table work keeps many
+// loads in flight per SM where one kernel would wait on them between its
+// barriers.
+struct BlockArgs {
+  const int32_t* list;        // [n] rows of the class
+  const int64_t* stg;         // [n] first staging slot of each row
+  unsigned long long* stage;
+  uint8_t* sawown;            // [n] a neighbour is in the row's own community
+  int64_t n;
+};
+
+constexpr int kStageUnroll = 8;
+
+__global__ void __launch_bounds__(kThreads) block_stage_kernel(MoveArgs P, BlockArgs B) {
+  if (P.ctl->done) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (kThreads / 32);
+  for (int64_t r = blockIdx.x * (int64_t)(kThreads / 32) + (threadIdx.x >> 5); r < B.n; r += nwarps) {
+    const int32_t i = B.list[r];
+    const int64_t beg = P.off[i], end = P.off[i + 1];
+    const int32_t own = P.comm[i];
+    const int64_t s0 = B.stg[r] - beg;   // staging slot of entry e: s0 + e
+    bool saw = false;
+    for (int64_t e0 = beg + lane; e0 < end; e0 += kStageUnroll * 32) {
+      int32_t c[kStageUnroll];
+      float w[kStageUnroll];
+#pragma unroll
+      for (int u = 0; u < kStageUnroll; ++u) {
+        const int64_t e = e0 + u * 32;
+        c[u] = e < end ? __ldcs(P.col + e) : -1;
+        w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kStageUnroll; ++u) c[u] = c[u] >= 0 ? P.comm[c[u]] : -1;
+#pragma unroll
+      for (int u = 0; u < kStageUnroll; ++u) {
+        if (c[u] >= 0) {
+          saw |= c[u] == own;
+          B.stage[s0 + e0 + u * 32] = ((unsigned long long)(uint32_t)c[u] << 32) | __float_as_uint(w[u]);
+        }
+      }
+    }
+    saw = __any_sync(0xffffffffu, saw);
+    if (lane == 0) B.sawown[r] = saw ? 1 : 0;
+  }
+}
+
+template <bool PACKED>
+__global__ void __launch_bounds__(kThreads) block_agg_kernel(MoveArgs P, BlockArgs B) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  AggTable<PACKED>& T = *reinterpret_cast<AggTable<PACKED>*>(smem);
+  AggCtl& S = *reinterpret_cast<AggCtl*>(smem + sizeof(AggTable<PACKED>));
+  if (P.ctl->done) return;
+  agg_init(T, S);
+  for (int64_t r = blockIdx.x; r < B.n; r += gridDim.x) {
+    const int32_t i = B.list[r];
+    const int32_t d = (int32_t)(P.off[i + 1] - P.off[i]);
+    const int64_t base = B.stg[r];
+    const AggBest best = agg_segments<PACKED>(
+        P, T, S, B.stage, 1, [&](int32_t) { return int2x64{base, d}; }, P.kfrac[i]);
+    if (threadIdx.x == 0) {
+      const int32_t nseg = best.n + ((P.has_loop[i] && !B.sawown[r]) ? 1 : 0);
+      apply_decision(P, i, P.comm[i], best.c, best.w, nseg);
+    }
+  }
 }
 
 // ------------------------------------------------------------------ commit + Q
@@ -1806,10 +1785,12 @@ MoveArgs move_args(const LevelGraph& g, CommState& st) {
   return P;
 }
 
-int block_table_log(const Tuning& t) {
-  int l = 5;
-  while ((1 << l) < 2 * t.block_max) ++l;
-  return l;
+// Staging slots of the block-class rows: the row degrees, scanned on the host side.
+__global__ void row_degree_kernel(const int32_t* list, int64_t n, const int64_t* off, int64_t* deg) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t i = list[j];
+    deg[j] = off[i + 1] - off[i];
+  }
 }
 
 }  // namespace
@@ -1832,7 +1813,7 @@ bool validate_edges(const int32_t* src, const int32_t* dst, const float* w, int6
 
 // Sort-free CSR build; returns false (and builds nothing) unless the level
 // list is strictly sorted and symmetric.
-static void set_move_attributes(int block_log);
+static void set_move_attributes();
 
 static bool build_csr_fast(LevelGraph& g, Arena& a, cudaStream_t s) {
   const int32_t V = g.V;
@@ -2119,8 +2100,21 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
       LVG_LAUNCH();
     }
   }
-  g.block_log = block_table_log(t);
-  set_move_attributes(g.block_log);
+  // block class: staging slots per row (prefix of the row degrees)
+  g.block_n = g.nbucket[kBBlock];
+  if (g.block_n > 0) {
+    g.block_stg = a.lo_n<int64_t>(g.block_n + 1);
+    g.block_sawown = a.lo_n<uint8_t>(g.block_n);
+    row_degree_kernel<<<sm_grid(g.block_n, kThreads), kThreads, 0, s>>>(g.blist + g.bstart[kBBlock], g.block_n,
+                                                                          g.off, g.block_stg);
+    LVG_LAUNCH();
+    scan_i64(g.block_stg, g.block_stg, g.block_n, a, s);
+    int64_t tot = 0;
+    LVG_CUDA(cudaMemcpyAsync(&tot, g.block_stg + g.block_n, sizeof tot, cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaStreamSynchronize(s));
+    g.block_stage = a.lo_n<unsigned long long>(tot);
+  }
+  set_move_attributes();
 }
 
 void alloc_state(const LevelGraph& g, CommState& st, Arena& a) {
@@ -2186,11 +2180,16 @@ void launch_q(const LevelGraph& g, CommState& st, double* dst, cudaStream_t s) {
 }
 
 // Dynamic shared memory limits of the move kernels, set before any capture.
-static void set_move_attributes(int block_log) {
+// Dynamic shared memory limits of the move kernels, set once per device
+// before any capture.
+static void set_move_attributes() {
+  constexpr int kDevs = 64;
   static std::mutex mu;
-  static int done_log = -1;
+  static bool done[kDevs] = {};
+  int dev = 0;
+  LVG_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);   // contexts on several host threads
-  if (done_log >= block_log) return;
+  if (dev >= 0 && dev < kDevs && done[dev]) return;
   LVG_CUDA(cudaFuncSetAttribute(move_tile_kernel<int>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(TileSmem<int>)));
   LVG_CUDA(cudaFuncSetAttribute(move_tile_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2201,11 +2200,11 @@ static void set_move_attributes(int block_log) {
                                 (int)agg_smem_bytes<true>()));
   LVG_CUDA(cudaFuncSetAttribute(hub_agg_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)agg_smem_bytes<false>()));
-  size_t smem = ((size_t)1 << block_log) * (sizeof(double) + sizeof(int32_t));
-  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  smem = ((size_t)1 << block_log) * (sizeof(int32_t) + sizeof(int32_t));
-  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<int>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  done_log = block_log;
+  LVG_CUDA(cudaFuncSetAttribute(block_agg_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)agg_smem_bytes<true>()));
+  LVG_CUDA(cudaFuncSetAttribute(block_agg_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)agg_smem_bytes<false>()));
+  if (dev >= 0 && dev < kDevs) done[dev] = true;
 }
 
 template <typename Acc>
@@ -2262,26 +2261,21 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     hub_decide_kernel<<<grid_for(nhub, 128), 128, 0, sh>>>(P, H, nhub);
     LVG_LAUNCH();
   }
-  if (g.nbucket[kBBlock] > 0) {
-    MoveArgs Q = P;
-    Q.list = g.blist + g.bstart[kBBlock];
-    Q.n = g.nbucket[kBBlock];
-    int lg = g.block_log;
-    if (g.int_acc) {
-      // two launches when the table is large: degrees up to 2^(lg-2) get half
-      // the table, so twice the blocks fit on an SM
-      int64_t split = kBlockSplit && lg >= 12 ? ((int64_t)1 << (lg - 2)) : 0;
-      if (split > 0) {
-        size_t smem = ((size_t)1 << (lg - 1)) * (sizeof(int32_t) + sizeof(int32_t));
-        move_block_kernel<int><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg - 1, 0, split);
-        LVG_LAUNCH();
-      }
-      size_t smem = ((size_t)1 << lg) * (sizeof(int32_t) + sizeof(int32_t));
-      move_block_kernel<int><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg, split, INT64_MAX);
-    } else {
-      size_t smem = ((size_t)1 << lg) * (sizeof(double) + sizeof(int32_t));
-      move_block_kernel<double><<<sm_grid(Q.n, 1), kThreads, smem, sb>>>(Q, lg, 0, INT64_MAX);
-    }
+  if (g.block_n > 0) {
+    BlockArgs B;
+    B.list = g.blist + g.bstart[kBBlock];
+    B.stg = g.block_stg;
+    B.stage = g.block_stage;
+    B.sawown = g.block_sawown;
+    B.n = g.block_n;
+    const int64_t wblocks = std::min<int64_t>((B.n + kThreads / 32 - 1) / (kThreads / 32), (int64_t)sm_count() * 8);
+    block_stage_kernel<<<(unsigned)std::max<int64_t>(wblocks, 1), kThreads, 0, sb>>>(P, B);
+    LVG_LAUNCH();
+    const size_t smem = g.int_acc ? agg_smem_bytes<true>() : agg_smem_bytes<false>();
+    const int per_sm = std::max(1, std::min(8, (int)((227u * 1024u) / (smem + 1024))));
+    const int64_t grid = std::min<int64_t>(B.n, (int64_t)sm_count() * per_sm);
+    if (g.int_acc) block_agg_kernel<true><<<(unsigned)grid, kThreads, smem, sb>>>(P, B);
+    else block_agg_kernel<false><<<(unsigned)grid, kThreads, smem, sb>>>(P, B);
     LVG_LAUNCH();
   }
   if (g.ntiles > 0) {

@@ -53,7 +53,11 @@ struct LevelGraph {
   int64_t nbucket[kNumBuckets] = {};
   int64_t bstart[kNumBuckets] = {};
   int32_t max_deg = 0;
-  int block_log = 13;             // log2 slots of the block-per-vertex table
+  // block class (tile_max < degree <= block_max): staging of each row's pairs
+  int64_t block_n = 0;
+  int64_t* block_stg = nullptr;   // [block_n+1] first staging slot of each row
+  uint8_t* block_sawown = nullptr;
+  unsigned long long* block_stage = nullptr;
   // sliced-ELL copies of the degree classes up to 32 (slots of class b from ell_base[b])
   int32_t* ell_col = nullptr;
   float* ell_w = nullptr;
