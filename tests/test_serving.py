@@ -42,7 +42,7 @@ def test_dead_slots_fail_queued_requests_without_a_gpu():
 
 
 @pytest.mark.gpu
-def test_results_same_alone_and_in_the_mix(gen):
+def test_results_same_alone_and_in_the_mix(gen, oracle):
     import torch
     if not torch.cuda.is_available():
         pytest.fail("CUDA device required for gpu tests")
@@ -84,3 +84,20 @@ def test_results_same_alone_and_in_the_mix(gen):
         np.testing.assert_array_equal(r.part, part, err_msg=f"request {r.tag}")
         assert r.q_final == q and r.n_levels == nl and r.n_comms == nc
         assert r.t_submit <= r.t_start <= r.t_done
+    # a sample of the served results against the oracle (both giants included)
+    hs, hd, hw = dg.to_host()
+    host = {}
+    for g in range(dg.n_graphs):
+        e0, e1 = int(dg.entry_off[g]), int(dg.entry_off[g + 1])
+        host[g] = (int(dg.vertex_off[g + 1] - dg.vertex_off[g]), hs[e0:e1], hd[e0:e1], hw[e0:e1])
+    for k, x in enumerate(giants):
+        host[dg.n_graphs + k] = (x.n_vertices, *x.to_host())
+    by_tag = {r.tag: r for r in out}
+    sample = list(np.random.default_rng(2).choice(dg.n_graphs, 10, replace=False)) + [dg.n_graphs, dg.n_graphs + 1]
+    for t in sample:
+        n, s_, d_, w_ = host[int(t)]
+        ref = oracle.Run(n, s_, d_, w_)
+        r = by_tag[int(t)]
+        np.testing.assert_array_equal(r.part, ref.final, err_msg=f"request {t}")
+        assert r.n_levels == len(ref.levels)
+        assert r.q_final == pytest.approx(oracle.modularity_fp64(n, s_, d_, w_, ref.final), abs=1e-9)
