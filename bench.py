@@ -507,7 +507,18 @@ def run_batched(args, world, rank, local, pg):
     # workers: contexts (own streams) that take the sub-batches in turn, so
     # one batch's host checks and small kernels overlap another's work
     nw = max(1, min(args.batch_workers, len(dgs)))
-    ctxs = [Louvain(device=local) for _ in range(nw)]
+    # degree thresholds tuned once on the batch's largest graph (outside the
+    # timed region); every worker context builds its levels with that pair
+    tune = {"tile_max_degree": 512, "block_max_degree": 4096, "autotuned": False}
+    if not args.no_autotune:
+        big = max(((d, g) for d in dgs for g in range(d.n_graphs)), key=lambda x: x[0].graph_ptrs(x[1])[3])
+        with Louvain(device=local) as tl:
+            tl.load_edges_device(*big[0].graph_ptrs(big[1]))
+            best, _ = tl.autotune(reps=2)
+        tune = {"tile_max_degree": best[0], "block_max_degree": best[1], "autotuned": True,
+                "tuned_on": "largest graph of the batch"}
+    ctxs = [Louvain(device=local, tile_max_degree=tune["tile_max_degree"], block_max_degree=tune["block_max_degree"])
+            for _ in range(nw)]
     if nw == 1:
         ctxs[0].set_stream(stream.cuda_stream)
     lv = ctxs[0]
@@ -552,7 +563,7 @@ def run_batched(args, world, rank, local, pg):
     launches = kernel_launches() - l0
     t_ms = e0.elapsed_time(e1)
     # plain loop: one context, one graph at a time, same device-resident lists
-    pl = Louvain(device=local)
+    pl = Louvain(device=local, tile_max_degree=tune["tile_max_degree"], block_max_degree=tune["block_max_degree"])
     pl.set_stream(stream.cuda_stream)
     torch.cuda.synchronize()
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -616,6 +627,7 @@ def run_batched(args, world, rank, local, pg):
                    "weights": "integer 1..4", "sub_batches": len(dgs), "batch_workers": nw, "seed": 3,
                    "inputs": "device-resident packed lists (device generator)",
                    "l2": "inputs larger than L2"},
+        "tuning": tune,
         "plain": {"value": plain, "unit": "graphs/s", "ms_per_sweep": t_plain,
                   "speedup_batched_over_plain": value / plain,
                   "partitions_differing": mism, "max_abs_dq": dq_max},
@@ -663,10 +675,21 @@ def run_serving(args, world, rank, local, pg):
     budget = int(min(150e9, free - 6e9))
     digest = lambda a: hashlib.blake2b(a.tobytes(), digest_size=8).hexdigest()  # noqa: E731
 
+    # degree thresholds tuned once on a giant (the giants carry most of the
+    # entries), outside the timed region; served and plain paths use the pair
+    tune = {"tile_max_degree": 512, "block_max_degree": 4096, "autotuned": False}
+    if not args.no_autotune and giants:
+        with Louvain(device=local) as tl:
+            x = giants[0]
+            tl.load_edges_device(x.src, x.dst, x.w, x.n_entries, x.n_vertices)
+            best, _ = tl.autotune(reps=2)
+        tune = {"tile_max_degree": best[0], "block_max_degree": best[1], "autotuned": True,
+                "tuned_on": "R-MAT scale-22 giant"}
     clocks = Clocks(local)
     clocks.start()
     # served: submit at the arrival times, results collected at the end
-    with Server(n_slots=args.slots, hbm_budget=budget, max_batch_entries=int(args.batch_entries)) as srv:
+    with Server(n_slots=args.slots, hbm_budget=budget, max_batch_entries=int(args.batch_entries),
+                tile_max_degree=tune["tile_max_degree"], block_max_degree=tune["block_max_degree"]) as srv:
         warm = [reqs[k] for k in range(min(64, R))]
         for s_, d_, w_, e_, n_ in warm:                       # warm-up requests (not timed)
             srv.submit(s_, d_, w_, e_, n_)
@@ -694,7 +717,7 @@ def run_serving(args, world, rank, local, pg):
     served_q = np.array([r.q_final for r in out])
     bad_status = sum(1 for r in out if r.status != 0)
     # plain: one context, one request at a time, same arrival times
-    pl = Louvain(device=local)
+    pl = Louvain(device=local, tile_max_degree=tune["tile_max_degree"], block_max_degree=tune["block_max_degree"])
     torch.cuda.synchronize()
     plain_lat = np.zeros(R)
     mism, dq_max = 0, 0.0
@@ -728,6 +751,7 @@ def run_serving(args, world, rank, local, pg):
                    "giant_graphs_distinct": len(giants), "small": "SBMs of the batched distribution",
                    "small_pool_graphs": len(small), "hbm_budget_bytes": budget, "slots": args.slots,
                    "max_batch_entries": int(args.batch_entries), "l2": "inputs larger than L2"},
+        "tuning": tune,
         "served": dict(pct(served_lat), graphs_per_s=value, span_s=served_span, batches=stats["batches"],
                        failed=bad_status, wall_s=wall),
         "plain": dict(pct(plain_lat), graphs_per_s=R / plain_span, span_s=plain_span),

@@ -38,13 +38,20 @@ class ServeResult:
 
 class Server:
     def __init__(self, n_slots=4, hbm_budget=150e9, max_batch_entries=2.5e8, max_batch_graphs=4096, device=0,
-                 pass_min_gain=1e-7, level_min_gain=1e-7):
+                 pass_min_gain=1e-7, level_min_gain=1e-7, tile_max_degree=0, block_max_degree=0):
+        """tile_max_degree / block_max_degree: the slots' degree thresholds
+        (0: the defaults), e.g. a pair Louvain.autotune picked on a
+        representative graph."""
         self._L = _lib.load()
         cfg = _lib.LvgConfig()
         _lib.check(None, self._L.lvg_config_default(ctypes.byref(cfg)))
         cfg.device = int(device)
         cfg.pass_min_gain = float(pass_min_gain)
         cfg.level_min_gain = float(level_min_gain)
+        if tile_max_degree:
+            cfg.tile_max_degree = int(tile_max_degree)
+        if block_max_degree:
+            cfg.block_max_degree = int(block_max_degree)
         h = ctypes.c_void_p()
         st = self._L.lvg_server_create(ctypes.byref(cfg), int(n_slots), int(hbm_budget), int(max_batch_entries),
                                        int(max_batch_graphs), ctypes.byref(h))
