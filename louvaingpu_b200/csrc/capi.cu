@@ -1192,7 +1192,7 @@ void batch_run(lvg_ctx* c, const BatchInput& in, int32_t* part_out, double* q_ou
     st.gdone = C.done;
     batch_init(g, st, s);
     reset_ctl(st, 0.0, c->cfg.pass_min_gain, -1, s);
-    batch_commit(0, bp, gm, st, C, s);
+    batch_commit(0, bp, gm, g.k, st, C, s);
     batch_ctl(1, bp, st, C, G, s);
     std::vector<double> q0(G), hv(G);
     LVG_CUDA(cudaMemcpyAsync(q0.data(), C.q_prev, sizeof(double) * G, cudaMemcpyDeviceToHost, s));
@@ -1226,7 +1226,7 @@ void batch_run(lvg_ctx* c, const BatchInput& in, int32_t* part_out, double* q_ou
         for (int p = 0; p < chunk; ++p) {
           if (launched == 0) launch_moves_singleton(g, st, s, &c->side);   // from batch_init's singletons
           else launch_moves(g, st, s, &c->side);
-          batch_commit(1, bp, gm, st, C, s);
+          batch_commit(1, bp, gm, g.k, st, C, s);
           batch_ctl(0, bp, st, C, G, s);
           ++launched;
         }
@@ -1238,7 +1238,7 @@ void batch_run(lvg_ctx* c, const BatchInput& in, int32_t* part_out, double* q_ou
       }
     }
     launch_merge_deltas(g, st, s);
-    batch_commit(2, bp, gm, st, C, s);
+    batch_commit(2, bp, gm, g.k, st, C, s);
     batch_ctl(2, bp, st, C, G, s);
     std::vector<double> qret(G);
     std::vector<int32_t> passes(G), stat(G);

@@ -6,7 +6,7 @@
 //                     (doubled list, equal (u,v) merged, self loops removed)
 //   per vertex        k/kfrac double, loopw float, has_loop u8
 //   community state   comm/next int32, tot/in double, size int32, deltas
-//                     dtot/din double + dsize int32, cand int32
+//                     deltas (tot, in, size: one 32-byte sector per community), cand int32
 //
 // Every FP64 expression that feeds a decision is written with explicit
 // round-to-nearest intrinsics so it rounds exactly as the CPU oracle does.
@@ -35,6 +35,22 @@ struct VInfo {
 };
 
 namespace {
+
+__device__ __forceinline__ void delta_clear(Delta& d) {
+  d.tot = 0.0; d.in = 0.0; d.size = 0; d.out = 0; d.iw_out = 0.0;
+}
+
+// Commit of one community's pass deltas (communitySetKernel,
+// OneLevelKernel.cu:93-107): tot/in/size move by the deltas, and a vertex
+// that left its singleton community takes its degree and weight out of it.
+__device__ __forceinline__ void delta_commit(Delta& d, double kc, double& tot, double& in, int32_t& size) {
+  double t = tot, x = in;
+  if (d.out) { t = __dsub_rn(t, kc); x = __dsub_rn(x, d.iw_out); }
+  tot = __dadd_rn(t, d.tot);
+  in = __dadd_rn(x, d.in);
+  size += d.size - d.out;
+  delta_clear(d);
+}
 
 constexpr int kThreads = 256;
 constexpr int kHubChunk = 4096;
@@ -290,7 +306,7 @@ __global__ void hub_info_kernel(const int32_t* hubs, int64_t nhub, const int64_t
 // ------------------------------------------------------------------ state
 __global__ void init_state_kernel(int32_t V, const double* k, const float* loopw, double m, double* kfrac,
                                   int32_t* comm, int32_t* next, double* tot, double* in, int32_t* size,
-                                  double* dtot, double* din, int32_t* dsize, int32_t* cand) {
+                                  Delta* delta, int32_t* cand) {
   double twom = __dmul_rn(2.0, m);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
     comm[i] = (int32_t)i;                 // InitKernel.cu:213-215
@@ -298,7 +314,7 @@ __global__ void init_state_kernel(int32_t V, const double* k, const float* loopw
     tot[i] = k[i];                        // InitKernel.cu:236
     in[i] = (double)loopw[i];             // InitKernel.cu:242
     size[i] = 1;                          // OneLevelKernel.cu:87
-    dtot[i] = 0.0; din[i] = 0.0; dsize[i] = 0;
+    delta_clear(delta[i]);
     cand[i] = -1;
     kfrac[i] = m > 0.0 ? __ddiv_rn(k[i], twom) : 0.0;  // OneLevelKernel.cu:307
   }
@@ -319,9 +335,7 @@ struct MoveArgs {
   const uint8_t* has_loop;
   int32_t* next;
   int32_t* cand;
-  double* dtot;
-  double* din;
-  int32_t* dsize;
+  Delta* delta;
   PassCtl* ctl;
   const int32_t* k32;    // degrees as int32 (integral weights), else nullptr: the singleton tot
   const int32_t* gid;    // batched runs: graph of each vertex (nullptr for one graph)
@@ -346,6 +360,24 @@ __device__ __forceinline__ void warp_best(double& bg, int32_t& bc, double& bw) {
   }
 }
 
+// remove/insert (OneLevelKernel.cu:52-78) of a vertex of degree ki moving
+// with weight iw from community own to best.  SINGLETON: own holds only this
+// vertex, so its side is two plain stores the commit applies.
+template <bool SINGLETON>
+__device__ __forceinline__ void move_deltas(Delta* d, int32_t own, int32_t best, double ki, double iw) {
+  if (SINGLETON) {
+    d[own].out = 1;
+    d[own].iw_out = iw;
+  } else {
+    atomicAdd(&d[own].tot, -ki);
+    atomicAdd(&d[own].in, -iw);
+    atomicAdd(&d[own].size, -1);
+  }
+  atomicAdd(&d[best].tot, ki);
+  atomicAdd(&d[best].in, iw);
+  atomicAdd(&d[best].size, 1);
+}
+
 // The decision for one vertex from its best candidate: singleton-pair rule
 // (OneLevelKernel.cu:407-410), remove/insert into the delta buffers
 // (OneLevelKernel.cu:52-78, 412-421) and the isolated-merge candidate
@@ -362,15 +394,7 @@ __device__ __forceinline__ void apply_decision_kl(const MoveArgs& P, int32_t i, 
   if (so == 1 && sb == 1 && raw > own) best = own;
   P.next[i] = best;
   P.cand[i] = (so == 1 && nseg == 1 && raw != own && own < raw) ? raw : -1;
-  if (best != own) {
-    double iw = __dadd_rn(bw, (double)loopw);
-    atomicAdd(&P.dtot[own], -ki);
-    atomicAdd(&P.dtot[best], ki);
-    atomicAdd(&P.din[own], -iw);
-    atomicAdd(&P.din[best], iw);
-    atomicAdd(&P.dsize[own], -1);
-    atomicAdd(&P.dsize[best], 1);
-  }
+  if (best != own) move_deltas<SINGLETON>(P.delta, own, best, ki, __dadd_rn(bw, (double)loopw));
 }
 
 template <bool SINGLETON = false>
@@ -383,16 +407,7 @@ __device__ __forceinline__ void apply_decision(const MoveArgs& P, int32_t i, int
   if (so == 1 && sb == 1 && raw > own) best = own;
   P.next[i] = best;
   P.cand[i] = (so == 1 && nseg == 1 && raw != own && own < raw) ? raw : -1;
-  if (best != own) {
-    double ki = P.k[i];
-    double iw = __dadd_rn(bw, (double)P.loopw[i]);
-    atomicAdd(&P.dtot[own], -ki);
-    atomicAdd(&P.dtot[best], ki);
-    atomicAdd(&P.din[own], -iw);
-    atomicAdd(&P.din[best], iw);
-    atomicAdd(&P.dsize[own], -1);
-    atomicAdd(&P.dsize[best], 1);
-  }
+  if (best != own) move_deltas<SINGLETON>(P.delta, own, best, P.k[i], __dadd_rn(bw, (double)P.loopw[i]));
 }
 
 // Packed (community << 32 | integer sum) slots are all ones when empty; the
@@ -1459,9 +1474,8 @@ enum { kCommitInit = 0, kCommitPass = 1, kCommitForce = 2 };
 // unconditionally (mergeSetKernel, :122-136).  kCommitInit only sums Q.
 template <int MODE>
 __global__ void __launch_bounds__(kRedThreads) commit_kernel(int32_t V, double m, int32_t* comm, const int32_t* next,
-                                                             double* tot, double* in, int32_t* size, double* dtot,
-                                                             double* din, int32_t* dsize, double* partials,
-                                                             PassCtl* ctl) {
+                                                             double* tot, double* in, int32_t* size, Delta* delta,
+                                                             const double* k, double* partials, PassCtl* ctl) {
   __shared__ double ws[8];
   int64_t base = (int64_t)blockIdx.x * kGroup + threadIdx.x;
   if (MODE == kCommitPass) {
@@ -1471,7 +1485,7 @@ __global__ void __launch_bounds__(kRedThreads) commit_kernel(int32_t V, double m
     if (stop || capped) {
       for (int j = 0; j < 8; ++j) {
         int64_t c = base + (int64_t)j * 256;
-        if (c < V) { dtot[c] = 0.0; din[c] = 0.0; dsize[c] = 0; }
+        if (c < V) delta_clear(delta[c]);
       }
       if (blockIdx.x == 0 && threadIdx.x == 0) ctl->stop_now = stop ? 1 : 2;
       return;
@@ -1485,11 +1499,10 @@ __global__ void __launch_bounds__(kRedThreads) commit_kernel(int32_t V, double m
     if (c < V) {
       double t, x;
       if (MODE != kCommitInit) {
-        t = __dadd_rn(tot[c], dtot[c]);
-        x = __dadd_rn(in[c], din[c]);
-        tot[c] = t; in[c] = x;
-        size[c] += dsize[c];
-        dtot[c] = 0.0; din[c] = 0.0; dsize[c] = 0;
+        t = tot[c]; x = in[c];
+        int32_t sz = size[c];
+        delta_commit(delta[c], k[c], t, x, sz);
+        tot[c] = t; in[c] = x; size[c] = sz;
         comm[c] = next[c];
       } else {
         t = tot[c]; x = in[c];
@@ -1563,20 +1576,14 @@ __global__ void ctl_init_kernel(PassCtl* ctl, double lower, double pass_min, int
 // Isolated-vertex merge (OneLevelKernel.cu:138-171) from the candidates of
 // the last pass; weight 0, so `in` moves by the loop weight only.
 __global__ void merge_kernel(int32_t V, const int32_t* comm, int32_t* next, const int32_t* cand, const double* k,
-                             const float* loopw, double* dtot, double* din, int32_t* dsize) {
+                             const float* loopw, Delta* delta) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
     int32_t c = cand[i];
     if (c >= 0) {
       int32_t own = comm[i];
       next[i] = c;
       double ki = k[i];
-      double iw = __dadd_rn(0.0, (double)loopw[i]);
-      atomicAdd(&dtot[own], -ki);
-      atomicAdd(&dtot[c], ki);
-      atomicAdd(&din[own], -iw);
-      atomicAdd(&din[c], iw);
-      atomicAdd(&dsize[own], -1);
-      atomicAdd(&dsize[c], 1);
+      move_deltas<false>(delta, own, c, ki, __dadd_rn(0.0, (double)loopw[i]));
     }
   }
 }
@@ -1593,9 +1600,9 @@ __global__ void set_state_kernel(int32_t V, const int32_t* src_comm, const doubl
   }
 }
 
-__global__ void clear_deltas_kernel(int32_t V, double* dtot, double* din, int32_t* dsize, int32_t* cand) {
+__global__ void clear_deltas_kernel(int32_t V, Delta* delta, int32_t* cand) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
-    dtot[i] = 0.0; din[i] = 0.0; dsize[i] = 0;
+    delta_clear(delta[i]);
     if (cand) cand[i] = -1;
   }
 }
@@ -1777,7 +1784,7 @@ MoveArgs move_args(const LevelGraph& g, CommState& st) {
   P.comm = st.comm; P.tot = st.tot; P.size = st.size;
   P.kfrac = g.kfrac; P.k = g.k; P.loopw = g.loopw; P.has_loop = g.has_loop;
   P.next = st.next; P.cand = st.cand;
-  P.dtot = st.dtot; P.din = st.din; P.dsize = st.dsize;
+  P.delta = st.delta;
   P.ctl = st.ctl;
   P.k32 = g.k32;
   P.gid = st.gid;
@@ -2127,9 +2134,7 @@ void alloc_state(const LevelGraph& g, CommState& st, Arena& a) {
   st.hot_bytes = (size_t)((char*)(st.size + std::max<int32_t>(V, 1)) - (char*)st.tot);
   st.next = a.lo_n<int32_t>(V);
   st.in = a.lo_n<double>(V);
-  st.dtot = a.lo_n<double>(V);
-  st.din = a.lo_n<double>(V);
-  st.dsize = a.lo_n<int32_t>(V);
+  st.delta = a.lo_n<Delta>(V);
   st.cand = a.lo_n<int32_t>(V);
   st.ngroups = (V + kGroup - 1) / kGroup;
   if (st.ngroups == 0) st.ngroups = 1;
@@ -2163,8 +2168,7 @@ void init_state(const LevelGraph& g, CommState& st, double lower, double pass_mi
   const int32_t V = g.V;
   if (V > 0) {
     init_state_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, g.k, g.loopw, g.m, g.kfrac, st.comm, st.next,
-                                                                st.tot, st.in, st.size, st.dtot, st.din, st.dsize,
-                                                                st.cand);
+                                                                st.tot, st.in, st.size, st.delta, st.cand);
     LVG_LAUNCH();
   }
   ctl_init_kernel<<<1, 1, 0, s>>>(st.ctl, lower, pass_min, max_passes);
@@ -2174,7 +2178,7 @@ void init_state(const LevelGraph& g, CommState& st, double lower, double pass_mi
 
 void launch_q(const LevelGraph& g, CommState& st, double* dst, cudaStream_t s) {
   commit_kernel<kCommitInit><<<(unsigned)st.ngroups, kRedThreads, 0, s>>>(
-      g.V, g.m, st.comm, st.next, st.tot, st.in, st.size, st.dtot, st.din, st.dsize, st.partials, st.ctl);
+      g.V, g.m, st.comm, st.next, st.tot, st.in, st.size, st.delta, g.k, st.partials, st.ctl);
   LVG_LAUNCH();
   q_tail(st, dst, s, false);
 }
@@ -2358,7 +2362,7 @@ void launch_pass(const LevelGraph& g, CommState& st, cudaStream_t s, const SideS
 
 void launch_commit(const LevelGraph& g, CommState& st, cudaStream_t s) {
   commit_kernel<kCommitPass><<<(unsigned)st.ngroups, kRedThreads, 0, s>>>(
-      g.V, g.m, st.comm, st.next, st.tot, st.in, st.size, st.dtot, st.din, st.dsize, st.partials, st.ctl);
+      g.V, g.m, st.comm, st.next, st.tot, st.in, st.size, st.delta, g.k, st.partials, st.ctl);
   LVG_LAUNCH();
   q_tail(st, nullptr, s, true);
 }
@@ -2366,12 +2370,11 @@ void launch_commit(const LevelGraph& g, CommState& st, cudaStream_t s) {
 void launch_merge(const LevelGraph& g, CommState& st, cudaStream_t s) {
   const int32_t V = g.V;
   if (V > 0) {
-    merge_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, st.comm, st.next, st.cand, g.k, g.loopw, st.dtot,
-                                                          st.din, st.dsize);
+    merge_kernel<<<sm_grid(V, kThreads), kThreads, 0, s>>>(V, st.comm, st.next, st.cand, g.k, g.loopw, st.delta);
     LVG_LAUNCH();
   }
   commit_kernel<kCommitForce><<<(unsigned)st.ngroups, kRedThreads, 0, s>>>(
-      V, g.m, st.comm, st.next, st.tot, st.in, st.size, st.dtot, st.din, st.dsize, st.partials, st.ctl);
+      V, g.m, st.comm, st.next, st.tot, st.in, st.size, st.delta, g.k, st.partials, st.ctl);
   LVG_LAUNCH();
   q_tail(st, &st.ctl->q_ret, s, false);
 }
@@ -2395,7 +2398,7 @@ void reset_ctl(CommState& st, double lower, double pass_min, int32_t max_passes,
 
 void clear_deltas(const LevelGraph& g, CommState& st, cudaStream_t s) {
   if (g.V == 0) return;
-  clear_deltas_kernel<<<sm_grid(g.V, kThreads), kThreads, 0, s>>>(g.V, st.dtot, st.din, st.dsize, st.cand);
+  clear_deltas_kernel<<<sm_grid(g.V, kThreads), kThreads, 0, s>>>(g.V, st.delta, st.cand);
   LVG_LAUNCH();
 }
 
@@ -2622,15 +2625,14 @@ __global__ void batch_m_kernel(const int32_t* src, const float* w, int64_t E, co
 }
 
 __global__ void batch_init_kernel(int32_t V, const double* k, const float* loopw, int32_t* comm, int32_t* next,
-                                  double* tot, double* in, int32_t* size, double* dtot, double* din, int32_t* dsize,
-                                  int32_t* cand) {
+                                  double* tot, double* in, int32_t* size, Delta* delta, int32_t* cand) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x) {
     comm[i] = (int32_t)i;
     next[i] = (int32_t)i;
     tot[i] = k[i];
     in[i] = (double)loopw[i];
     size[i] = 1;
-    dtot[i] = 0.0; din[i] = 0.0; dsize[i] = 0;
+    delta_clear(delta[i]);
     cand[i] = -1;
   }
 }
@@ -2638,7 +2640,7 @@ __global__ void batch_init_kernel(int32_t V, const double* k, const float* loopw
 template <int MODE>
 __global__ void __launch_bounds__(kRedThreads) batch_commit_kernel(
     const int32_t* blk_g, const int32_t* blk_c0, const int32_t* vbase, const double* gm, int32_t* comm,
-    const int32_t* next, double* tot, double* in, int32_t* size, double* dtot, double* din, int32_t* dsize,
+    const int32_t* next, double* tot, double* in, int32_t* size, Delta* delta, const double* k,
     double* partials, BatchCtl C) {
   __shared__ double ws[8];
   const int32_t g = blk_g[blockIdx.x];
@@ -2652,7 +2654,7 @@ __global__ void __launch_bounds__(kRedThreads) batch_commit_kernel(
     if (stop || capped) {
       for (int j = 0; j < 8; ++j) {
         int64_t c = base + (int64_t)j * 256;
-        if (c < cend) { dtot[c] = 0.0; din[c] = 0.0; dsize[c] = 0; }
+        if (c < cend) delta_clear(delta[c]);
       }
       if (c0 == vbase[g] && threadIdx.x == 0) C.stop_now[g] = stop ? 1 : 2;
       return;
@@ -2667,11 +2669,10 @@ __global__ void __launch_bounds__(kRedThreads) batch_commit_kernel(
     if (c < cend) {
       double t, x;
       if (MODE != kCommitInit) {
-        t = __dadd_rn(tot[c], dtot[c]);
-        x = __dadd_rn(in[c], din[c]);
-        tot[c] = t; in[c] = x;
-        size[c] += dsize[c];
-        dtot[c] = 0.0; din[c] = 0.0; dsize[c] = 0;
+        t = tot[c]; x = in[c];
+        int32_t sz = size[c];
+        delta_commit(delta[c], k[c], t, x, sz);
+        tot[c] = t; in[c] = x; size[c] = sz;
         comm[c] = next[c];
       } else {
         t = tot[c]; x = in[c];
@@ -2851,26 +2852,26 @@ void batch_m(const int32_t* src, const float* w, int64_t E, const int32_t* vgid,
 void batch_init(const LevelGraph& g, CommState& st, cudaStream_t s) {
   if (g.V == 0) return;
   batch_init_kernel<<<sm_grid(g.V, kThreads), kThreads, 0, s>>>(g.V, g.k, g.loopw, st.comm, st.next, st.tot, st.in,
-                                                                st.size, st.dtot, st.din, st.dsize, st.cand);
+                                                                st.size, st.delta, st.cand);
   LVG_LAUNCH();
 }
 
-void batch_commit(int mode, const BatchPlan& bp, const double* gm, CommState& st, const BatchCtl& C,
-                  cudaStream_t s) {
+void batch_commit(int mode, const BatchPlan& bp, const double* gm, const double* g_k, CommState& st,
+                  const BatchCtl& C, cudaStream_t s) {
   const unsigned nb = (unsigned)bp.nblk;
   if (nb == 0) return;
   if (mode == kCommitInit)
     batch_commit_kernel<kCommitInit><<<nb, kRedThreads, 0, s>>>(bp.blk_g, bp.blk_c0, bp.vbase, gm, st.comm, st.next,
-                                                                st.tot, st.in, st.size, st.dtot, st.din, st.dsize,
+                                                                st.tot, st.in, st.size, st.delta, g_k,
                                                                 st.partials, C);
   else if (mode == kCommitPass)
     batch_commit_kernel<kCommitPass><<<nb, kRedThreads, 0, s>>>(bp.blk_g, bp.blk_c0, bp.vbase, gm, st.comm, st.next,
-                                                                st.tot, st.in, st.size, st.dtot, st.din, st.dsize,
+                                                                st.tot, st.in, st.size, st.delta, g_k,
                                                                 st.partials, C);
   else
     batch_commit_kernel<kCommitForce><<<nb, kRedThreads, 0, s>>>(bp.blk_g, bp.blk_c0, bp.vbase, gm, st.comm,
-                                                                 st.next, st.tot, st.in, st.size, st.dtot, st.din,
-                                                                 st.dsize, st.partials, C);
+                                                                 st.next, st.tot, st.in, st.size, st.delta, g_k,
+                                                                 st.partials, C);
   LVG_LAUNCH();
 }
 
@@ -2884,8 +2885,7 @@ void batch_ctl(int mode, const BatchPlan& bp, const CommState& st, const BatchCt
 
 void launch_merge_deltas(const LevelGraph& g, CommState& st, cudaStream_t s) {
   if (g.V == 0) return;
-  merge_kernel<<<sm_grid(g.V, kThreads), kThreads, 0, s>>>(g.V, st.comm, st.next, st.cand, g.k, g.loopw, st.dtot,
-                                                          st.din, st.dsize);
+  merge_kernel<<<sm_grid(g.V, kThreads), kThreads, 0, s>>>(g.V, st.comm, st.next, st.cand, g.k, g.loopw, st.delta);
   LVG_LAUNCH();
 }
 

@@ -93,15 +93,26 @@ struct LevelGraph {
   struct HubPartial* sp_part = nullptr;
 };
 
+// Pass deltas of one community in one 32-byte sector, so that a move's three
+// updates of a community (total, internal weight, size) touch one sector.
+// `out` / `iw_out` carry the own side of a move out of a singleton community
+// (the first pass of a level): written without atomics by the community's
+// only vertex, applied by the commit.
+struct __align__(32) Delta {
+  double tot;
+  double in;
+  int32_t size;
+  int32_t out;
+  double iw_out;
+};
+
 struct CommState {
   int32_t* comm = nullptr;
   int32_t* next = nullptr;
   double* tot = nullptr;
   double* in = nullptr;
   int32_t* size = nullptr;
-  double* dtot = nullptr;
-  double* din = nullptr;
-  int32_t* dsize = nullptr;
+  Delta* delta = nullptr;
   int32_t* cand = nullptr;
   double* partials = nullptr;     // level-1 group partials of Q
   double* partials2 = nullptr;
@@ -216,8 +227,9 @@ void batch_m(const int32_t* src, const float* w, int64_t E, const int32_t* vgid,
              cudaStream_t s);
 void batch_init(const LevelGraph& g, CommState& st, cudaStream_t s);
 // mode: 0 init (Q only), 1 pass (per-graph ΔQ test + commit), 2 force commit
-void batch_commit(int mode, const BatchPlan& bp, const double* gm, CommState& st, const BatchCtl& C,
-                  cudaStream_t s);
+// g_k: degrees of the level's vertices (the own side of first-pass moves).
+void batch_commit(int mode, const BatchPlan& bp, const double* gm, const double* g_k, CommState& st,
+                  const BatchCtl& C, cudaStream_t s);
 // mode: 0 end of pass, 1 Q of the state into q_prev, 2 into q_ret
 void batch_ctl(int mode, const BatchPlan& bp, const CommState& st, const BatchCtl& C, int32_t G, cudaStream_t s);
 void launch_merge_deltas(const LevelGraph& g, CommState& st, cudaStream_t s);
