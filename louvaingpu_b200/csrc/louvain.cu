@@ -1255,7 +1255,26 @@ __device__ AggBest agg_segments(const MoveArgs& P, AggTable<PACKED>& T, AggCtl& 
     bg = 0.0; bw = 0.0; bc = kNone; nocc = 0;
     bool split = false;
     for (uint32_t sub = 0; sub < (1u << slog) && !split; ++sub) {
-      for (int32_t k0 = 0; k0 < K; k0 += kThreads) {
+      if (K == 1) {   // one segment (a block-class row): no scan, no search
+        const int2x64 sg = seg(0);
+        for (int32_t q = threadIdx.x; q < sg.len; q += kThreads) {
+          if (*reinterpret_cast<volatile int32_t*>(&S.full)) break;
+          const unsigned long long x = stage[sg.base + q];
+          const int32_t c = (int32_t)(uint32_t)(x >> 32);
+          if (slog > 0 && hub_sub(c, slog) != sub) continue;
+          uint32_t where = 0;
+          const int r = T.insert(c, __uint_as_float((uint32_t)x), where);
+          if (r == 2) {
+            const int n = atomicAdd(&S.nclaimed, 1);
+            S.claimed[n] = (uint16_t)where;
+            if (n + 1 > kAggFull) S.full = 1;
+          } else if (r == 0) {
+            S.full = 1;
+          }
+        }
+        __syncthreads();
+      }
+      for (int32_t k0 = 0; K > 1 && k0 < K; k0 += kThreads) {
         const int32_t k = k0 + (int32_t)threadIdx.x;
         int64_t base = 0;
         int32_t len = 0;
