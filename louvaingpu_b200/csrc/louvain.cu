@@ -1235,6 +1235,25 @@ struct AggBest {
   int32_t c, n;
 };
 
+// One staged pair into the table, when its community belongs to sub-pass
+// `sub` of 2^slog; a claimed slot is listed, and a table past half full
+// marks the sub-pass as split.
+template <bool PACKED>
+__device__ __forceinline__ void agg_insert(AggTable<PACKED>& T, AggCtl& S, unsigned long long x, int slog,
+                                           uint32_t sub) {
+  const int32_t c = (int32_t)(uint32_t)(x >> 32);
+  if (slog > 0 && hub_sub(c, slog) != sub) return;
+  uint32_t where = 0;
+  const int r = T.insert(c, __uint_as_float((uint32_t)x), where);
+  if (r == 2) {
+    const int n = atomicAdd(&S.nclaimed, 1);
+    S.claimed[n] = (uint16_t)where;
+    if (n + 1 > kAggFull) S.full = 1;
+  } else if (r == 0) {
+    S.full = 1;
+  }
+}
+
 // Sums the staged pairs of K segments (segment k starts at staging slot
 // seg(k).x and holds seg(k).y pairs) per community in the shared table T,
 // and leaves the best candidate (gain w - tot_c * kf, higher gain then lower
@@ -1260,17 +1279,7 @@ __device__ AggBest agg_segments(const MoveArgs& P, AggTable<PACKED>& T, AggCtl& 
         for (int32_t q = threadIdx.x; q < sg.len; q += kThreads) {
           if (*reinterpret_cast<volatile int32_t*>(&S.full)) break;
           const unsigned long long x = stage[sg.base + q];
-          const int32_t c = (int32_t)(uint32_t)(x >> 32);
-          if (slog > 0 && hub_sub(c, slog) != sub) continue;
-          uint32_t where = 0;
-          const int r = T.insert(c, __uint_as_float((uint32_t)x), where);
-          if (r == 2) {
-            const int n = atomicAdd(&S.nclaimed, 1);
-            S.claimed[n] = (uint16_t)where;
-            if (n + 1 > kAggFull) S.full = 1;
-          } else if (r == 0) {
-            S.full = 1;
-          }
+          agg_insert(T, S, x, slog, sub);
         }
         __syncthreads();
       }
@@ -1297,17 +1306,7 @@ __device__ AggBest agg_segments(const MoveArgs& P, AggTable<PACKED>& T, AggCtl& 
             if (S.segpre[mid] <= q) jlo = mid; else jhi = mid - 1;
           }
           const unsigned long long x = stage[S.segbase[jlo] + (q - S.segpre[jlo])];
-          const int32_t c = (int32_t)(uint32_t)(x >> 32);
-          if (slog > 0 && hub_sub(c, slog) != sub) continue;
-          uint32_t where = 0;
-          const int r = T.insert(c, __uint_as_float((uint32_t)x), where);
-          if (r == 2) {
-            const int n = atomicAdd(&S.nclaimed, 1);
-            S.claimed[n] = (uint16_t)where;
-            if (n + 1 > kAggFull) S.full = 1;
-          } else if (r == 0) {
-            S.full = 1;
-          }
+          agg_insert(T, S, x, slog, sub);
         }
         __syncthreads();
       }
