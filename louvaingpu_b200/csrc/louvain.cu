@@ -414,6 +414,132 @@ __device__ __forceinline__ void apply_decision(const MoveArgs& P, int32_t i, int
 // add of an integral weight cannot carry into the key (sums stay below 2^30).
 constexpr unsigned long long kPackedEmpty = ~0ull;
 
+__device__ __forceinline__ uint32_t hash_c(int32_t c, int logT) {
+  return (uint32_t)(((uint64_t)(uint32_t)c * 0x9E3779B97F4A7C15ull) >> (64 - logT));
+}
+
+__device__ __forceinline__ int ceil_log2(int64_t x) {  // x >= 1
+  return x <= 1 ? 0 : 64 - __clzll((unsigned long long)(x - 1));
+}
+
+// Open-addressing insert of (c, w) into a table of 2^logT slots.
+template <typename Acc>
+__device__ __forceinline__ bool table_insert(int32_t* keys, Acc* vals, int logT, int32_t c, Acc w) {
+  uint32_t T = 1u << logT;
+  uint32_t h = hash_c(c, logT);
+  for (uint32_t p = 0; p < T; ++p) {
+    int32_t prev = atomicCAS(&keys[h], -1, c);
+    if (prev == -1 || prev == c) { atomicAdd(&vals[h], w); return true; }
+    h = (h + 1) & (T - 1);
+  }
+  return false;
+}
+
+// Entries [e0 + u*stride) of a row, u < 4: columns and weights first, then
+// the four community gathers, so that each thread keeps several loads in
+// flight; kNone marks entries past `end`.
+constexpr int kUnroll = 4;
+__device__ __forceinline__ void gather4(const MoveArgs& P, int64_t e0, int64_t stride, int64_t end,
+                                        int32_t (&c)[kUnroll], float (&w)[kUnroll]) {
+  int32_t col[kUnroll];
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    const int64_t e = e0 + u * stride;
+    col[u] = e < end ? __ldcs(P.col + e) : -1;
+    w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
+  }
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) c[u] = col[u] >= 0 ? P.comm[col[u]] : kNone;
+}
+
+// Block per vertex for the block class (tile_max < degree <= block_max),
+// launched once per degree band (dlo, dhi] with a shared table of
+// 2^maxLog >= 2 dhi slots: the narrow bands of low degrees take small tables
+// and NT = 128 threads, so that many blocks fit on an SM; int32 sums when
+// the weights are integral (exact, half the table bytes).
+template <typename Acc, int NT>
+__global__ void __launch_bounds__(NT) move_block_kernel(MoveArgs P, int maxLog, int64_t dlo, int64_t dhi) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double rg[NT / 32], rw[NT / 32];
+  __shared__ int32_t rc[NT / 32], rn[NT / 32], rs[NT / 32];
+  if (P.ctl->done) return;
+  const int Tmax = 1 << maxLog;
+  Acc* vals = reinterpret_cast<Acc*>(smem);
+  int32_t* keys = reinterpret_cast<int32_t*>(vals + Tmax);
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int s = threadIdx.x; s < Tmax; s += NT) { keys[s] = -1; vals[s] = Acc(0); }
+  __syncthreads();
+  bool overflow = false;
+  for (int64_t item = blockIdx.x; item < P.n; item += gridDim.x) {
+    int32_t i = P.list[item];
+    int64_t beg = P.off[i], end = P.off[i + 1];
+    if (end - beg <= dlo || end - beg > dhi) continue;   // another band takes this degree
+    int32_t own = P.comm[i];
+    int logT = min(maxLog, max(5, ceil_log2(2 * (end - beg))));
+    int T = 1 << logT;
+    bool sawown = false;
+    for (int64_t e0 = beg + threadIdx.x; e0 < end; e0 += kUnroll * NT) {
+      int32_t c[kUnroll];
+      float wv[kUnroll];
+      gather4(P, e0, NT, end, c, wv);
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        if (c[u] != kNone) {
+          sawown |= (c[u] == own);
+          if (!table_insert<Acc>(keys, vals, logT, c[u], (Acc)wv[u])) overflow = true;
+        }
+      }
+    }
+    __syncthreads();
+    double kf = P.kfrac[i];
+    double bg = 0.0, bw = 0.0;
+    int32_t bc = kNone;
+    int nocc = 0;
+    for (int s0 = threadIdx.x; s0 < T; s0 += kUnroll * NT) {
+      int32_t c[kUnroll];
+      double W[kUnroll], t[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int s = s0 + u * NT;
+        c[u] = s < T ? keys[s] : -1;
+        W[u] = c[u] >= 0 ? (double)vals[s] : 0.0;
+        if (c[u] >= 0) { keys[s] = -1; vals[s] = Acc(0); }
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) t[u] = (c[u] >= 0 && W[u] != 0.0) ? P.tot[c[u]] : 0.0;
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        if (c[u] >= 0) {
+          ++nocc;
+          if (W[u] != 0.0) {                                            // OneLevelKernel.cu:303
+            const double g = __dsub_rn(W[u], __dmul_rn(t[u], kf));      // OneLevelKernel.cu:307-313
+            if (g > 0.0 && better(g, c[u], bg, bc)) { bg = g; bc = c[u]; bw = W[u]; }
+          }
+        }
+      }
+    }
+    warp_best(bg, bc, bw);
+    nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
+    int so = __any_sync(0xffffffffu, sawown) ? 1 : 0;
+    if (lane == 0) { rg[w] = bg; rc[w] = bc; rw[w] = bw; rn[w] = nocc; rs[w] = so; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double g = rg[0], ww = rw[0];
+      int32_t c = rc[0];
+      int n = rn[0], sw = rs[0];
+      for (int k2 = 1; k2 < NT / 32; ++k2) {
+        if (better(rg[k2], rc[k2], g, c)) { g = rg[k2]; c = rc[k2]; ww = rw[k2]; }
+        n += rn[k2];
+        sw |= rs[k2];
+      }
+      int32_t nseg = n + ((P.has_loop[i] && !sw) ? 1 : 0);
+      apply_decision(P, i, own, c, ww, nseg);
+    }
+    __syncthreads();
+  }
+  if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(&P.ctl->err, kErrProbe);
+}
+
 // ----------------------------------------------------------------- ELL kernels
 // Degree <= 32: vertices of class D (4, 8, 16, 32) keep their entries in a
 // sliced-ELL copy of the CSR built once per level: vertex j of the class owns
@@ -1403,78 +1529,6 @@ __global__ void hub_decide_kernel(MoveArgs P, HubArgs H, int64_t nhub) {
   apply_decision(P, i, own, c, ww, nseg);
 }
 
-// Block class (tile_max < degree <= block_max), two launches per pass:
-// block_stage_kernel -- a warp per row gathers the neighbours' communities
-// and writes the row's (community, weight) pairs to staging (up to eight
-// gathers in flight per lane, no shared memory, no block barriers);
-// block_agg_kernel -- a block per row sums the staged pairs in a shared
-// table and decides.  Splitting the gathers from the table work keeps many
-// loads in flight per SM where one kernel would wait on them between its
-// barriers.
-struct BlockArgs {
-  const int32_t* list;        // [n] rows of the class
-  const int64_t* stg;         // [n] first staging slot of each row
-  unsigned long long* stage;
-  uint8_t* sawown;            // [n] a neighbour is in the row's own community
-  int64_t n;
-};
-
-constexpr int kStageUnroll = 8;
-
-__global__ void __launch_bounds__(kThreads) block_stage_kernel(MoveArgs P, BlockArgs B) {
-  if (P.ctl->done) return;
-  const int lane = threadIdx.x & 31;
-  const int64_t nwarps = (int64_t)gridDim.x * (kThreads / 32);
-  for (int64_t r = blockIdx.x * (int64_t)(kThreads / 32) + (threadIdx.x >> 5); r < B.n; r += nwarps) {
-    const int32_t i = B.list[r];
-    const int64_t beg = P.off[i], end = P.off[i + 1];
-    const int32_t own = P.comm[i];
-    const int64_t s0 = B.stg[r] - beg;   // staging slot of entry e: s0 + e
-    bool saw = false;
-    for (int64_t e0 = beg + lane; e0 < end; e0 += kStageUnroll * 32) {
-      int32_t c[kStageUnroll];
-      float w[kStageUnroll];
-#pragma unroll
-      for (int u = 0; u < kStageUnroll; ++u) {
-        const int64_t e = e0 + u * 32;
-        c[u] = e < end ? __ldcs(P.col + e) : -1;
-        w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
-      }
-#pragma unroll
-      for (int u = 0; u < kStageUnroll; ++u) c[u] = c[u] >= 0 ? P.comm[c[u]] : -1;
-#pragma unroll
-      for (int u = 0; u < kStageUnroll; ++u) {
-        if (c[u] >= 0) {
-          saw |= c[u] == own;
-          B.stage[s0 + e0 + u * 32] = ((unsigned long long)(uint32_t)c[u] << 32) | __float_as_uint(w[u]);
-        }
-      }
-    }
-    saw = __any_sync(0xffffffffu, saw);
-    if (lane == 0) B.sawown[r] = saw ? 1 : 0;
-  }
-}
-
-template <bool PACKED>
-__global__ void __launch_bounds__(kThreads) block_agg_kernel(MoveArgs P, BlockArgs B) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  AggTable<PACKED>& T = *reinterpret_cast<AggTable<PACKED>*>(smem);
-  AggCtl& S = *reinterpret_cast<AggCtl*>(smem + sizeof(AggTable<PACKED>));
-  if (P.ctl->done) return;
-  agg_init(T, S);
-  for (int64_t r = blockIdx.x; r < B.n; r += gridDim.x) {
-    const int32_t i = B.list[r];
-    const int32_t d = (int32_t)(P.off[i + 1] - P.off[i]);
-    const int64_t base = B.stg[r];
-    const AggBest best = agg_segments<PACKED>(
-        P, T, S, B.stage, 1, [&](int32_t) { return int2x64{base, d}; }, P.kfrac[i]);
-    if (threadIdx.x == 0) {
-      const int32_t nseg = best.n + ((P.has_loop[i] && !B.sawown[r]) ? 1 : 0);
-      apply_decision(P, i, P.comm[i], best.c, best.w, nseg);
-    }
-  }
-}
-
 // ------------------------------------------------------------------ commit + Q
 // term_c = in_c/m - (tot_c/2m)^2 (OneLevelKernel.cu:447-448), zero when m <= 0.
 __device__ __forceinline__ double q_term(double in, double tot, double m, double twom) {
@@ -1810,14 +1864,6 @@ MoveArgs move_args(const LevelGraph& g, CommState& st) {
   return P;
 }
 
-// Staging slots of the block-class rows: the row degrees, scanned on the host side.
-__global__ void row_degree_kernel(const int32_t* list, int64_t n, const int64_t* off, int64_t* deg) {
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t i = list[j];
-    deg[j] = off[i + 1] - off[i];
-  }
-}
-
 }  // namespace
 
 // ============================================================================ host
@@ -2125,20 +2171,7 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
       LVG_LAUNCH();
     }
   }
-  // block class: staging slots per row (prefix of the row degrees)
-  g.block_n = g.nbucket[kBBlock];
-  if (g.block_n > 0) {
-    g.block_stg = a.lo_n<int64_t>(g.block_n + 1);
-    g.block_sawown = a.lo_n<uint8_t>(g.block_n);
-    row_degree_kernel<<<sm_grid(g.block_n, kThreads), kThreads, 0, s>>>(g.blist + g.bstart[kBBlock], g.block_n,
-                                                                          g.off, g.block_stg);
-    LVG_LAUNCH();
-    scan_i64(g.block_stg, g.block_stg, g.block_n, a, s);
-    int64_t tot = 0;
-    LVG_CUDA(cudaMemcpyAsync(&tot, g.block_stg + g.block_n, sizeof tot, cudaMemcpyDeviceToHost, s));
-    LVG_CUDA(cudaStreamSynchronize(s));
-    g.block_stage = a.lo_n<unsigned long long>(tot);
-  }
+  g.block_max = t.block_max;
   set_move_attributes();
 }
 
@@ -2222,10 +2255,12 @@ static void set_move_attributes() {
                                 (int)agg_smem_bytes<true>()));
   LVG_CUDA(cudaFuncSetAttribute(hub_agg_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)agg_smem_bytes<false>()));
-  LVG_CUDA(cudaFuncSetAttribute(block_agg_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)agg_smem_bytes<true>()));
-  LVG_CUDA(cudaFuncSetAttribute(block_agg_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)agg_smem_bytes<false>()));
+  // block bands: up to 2 * 8192 slots of int32 key + f64 sum (block_max <= 8192)
+  const int big = (int)((size_t)16384 * (sizeof(double) + sizeof(int32_t)));
+  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<int, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<int, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<double, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<double, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   if (dev >= 0 && dev < kDevs) done[dev] = true;
 }
 
@@ -2283,22 +2318,27 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     hub_decide_kernel<<<grid_for(nhub, 128), 128, 0, sh>>>(P, H, nhub);
     LVG_LAUNCH();
   }
-  if (g.block_n > 0) {
-    BlockArgs B;
-    B.list = g.blist + g.bstart[kBBlock];
-    B.stg = g.block_stg;
-    B.stage = g.block_stage;
-    B.sawown = g.block_sawown;
-    B.n = g.block_n;
-    const int64_t wblocks = std::min<int64_t>((B.n + kThreads / 32 - 1) / (kThreads / 32), (int64_t)sm_count() * 8);
-    block_stage_kernel<<<(unsigned)std::max<int64_t>(wblocks, 1), kThreads, 0, sb>>>(P, B);
-    LVG_LAUNCH();
-    const size_t smem = g.int_acc ? agg_smem_bytes<true>() : agg_smem_bytes<false>();
-    const int per_sm = std::max(1, std::min(8, (int)((227u * 1024u) / (smem + 1024))));
-    const int64_t grid = std::min<int64_t>(B.n, (int64_t)sm_count() * per_sm);
-    if (g.int_acc) block_agg_kernel<true><<<(unsigned)grid, kThreads, smem, sb>>>(P, B);
-    else block_agg_kernel<false><<<(unsigned)grid, kThreads, smem, sb>>>(P, B);
-    LVG_LAUNCH();
+  if (g.nbucket[kBBlock] > 0) {
+    MoveArgs Q = P;
+    Q.list = g.blist + g.bstart[kBBlock];
+    Q.n = g.nbucket[kBBlock];
+    // degree bands (lo, hi], hi = 1024, 2048, ..., each with a table of 2 hi slots
+    int64_t lo = 0;
+    for (int64_t hi = 1024; lo < g.block_max; hi *= 2) {
+      const int64_t h = std::min<int64_t>(hi, g.block_max);
+      int lg = 5;
+      while (((int64_t)1 << lg) < 2 * h) ++lg;
+      const size_t slot = g.int_acc ? sizeof(int32_t) + sizeof(int32_t) : sizeof(double) + sizeof(int32_t);
+      const size_t smem = ((size_t)1 << lg) * slot;
+      const bool narrow = h <= 1024;
+      const unsigned grid = (unsigned)std::min<int64_t>(Q.n, (int64_t)sm_count() * (narrow ? 16 : 8));
+      if (g.int_acc && narrow) move_block_kernel<int, 128><<<grid, 128, smem, sb>>>(Q, lg, lo, h);
+      else if (g.int_acc) move_block_kernel<int, 256><<<grid, 256, smem, sb>>>(Q, lg, lo, h);
+      else if (narrow) move_block_kernel<double, 128><<<grid, 128, smem, sb>>>(Q, lg, lo, h);
+      else move_block_kernel<double, 256><<<grid, 256, smem, sb>>>(Q, lg, lo, h);
+      LVG_LAUNCH();
+      lo = h;
+    }
   }
   if (g.ntiles > 0) {
     MoveArgs Q = P;

@@ -53,11 +53,7 @@ struct LevelGraph {
   int64_t nbucket[kNumBuckets] = {};
   int64_t bstart[kNumBuckets] = {};
   int32_t max_deg = 0;
-  // block class (tile_max < degree <= block_max): staging of each row's pairs
-  int64_t block_n = 0;
-  int64_t* block_stg = nullptr;   // [block_n+1] first staging slot of each row
-  uint8_t* block_sawown = nullptr;
-  unsigned long long* block_stage = nullptr;
+  int32_t block_max = 4096;       // largest degree of the block class (the context's threshold)
   // sliced-ELL copies of the degree classes up to 32 (slots of class b from ell_base[b])
   int32_t* ell_col = nullptr;
   float* ell_w = nullptr;
