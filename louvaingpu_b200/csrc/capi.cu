@@ -63,6 +63,7 @@ struct lvg_ctx {
   bool have_state = false;
   bool renumbered = false;
   bool pristine = false;         // level 0 as loaded: no pass, state change or renumbering since
+  bool symmetric0 = false;       // the level-0 list was found sorted and symmetric at load
   int32_t* d_part_cur = nullptr;
   int32_t C_cur = 0;
   std::vector<LevelRec> levels;
@@ -186,6 +187,7 @@ void load_common(lvg_ctx* c, const int32_t* d_src, const int32_t* d_dst, const f
   c->g.dst = d_dst;
   c->g.w = d_w;
   prepare_level(c);
+  c->symmetric0 = c->g.sorted_symmetric;
   c->loaded = true;
   c->pristine = true;
 }
@@ -619,7 +621,7 @@ lvg_status lvg_run(lvg_ctx* c, lvg_result* res) {
       res->pass_entries = pass_entries;
       res->status = run_status;
       res->q_final = modularity_fp64(c->src0, c->dst0, c->w0, c->E0, std::max(c->C_cur, 1), c->composed,
-                                     c->arena, c->stream);
+                                     c->arena, c->stream, c->symmetric0);
     }
     sync(c);
     if (!c->levels.empty()) c->levels.back().info.ms_renumber = elapsed(c->pev[2], c->pev[3]);
@@ -716,7 +718,7 @@ lvg_status lvg_modularity_fp64(lvg_ctx* c, const int32_t* part, double* q) {
     int32_t* dp = c->arena.hi_n<int32_t>(c->V0);
     if (c->V0 > 0)
       LVG_CUDA(cudaMemcpyAsync(dp, part, sizeof(int32_t) * c->V0, cudaMemcpyHostToDevice, c->stream));
-    *q = modularity_fp64(c->src0, c->dst0, c->w0, c->E0, std::max(C, 1), dp, c->arena, c->stream);
+    *q = modularity_fp64(c->src0, c->dst0, c->w0, c->E0, std::max(C, 1), dp, c->arena, c->stream, c->symmetric0);
   });
 }
 

@@ -2535,6 +2535,24 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
   return cnt;
 }
 
+// Kc and Ain of a list known to be symmetric (every (u, v, w) has its
+// (v, u, w)): the destination side of Kc equals the source side, so each
+// entry adds 2w to its source's community only -- one warp-aggregated update
+// per run of equal sources instead of a scattered update per entry -- and
+// 2w to Ain when both ends share a community.
+__global__ void nm_accum_sym_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
+                                    const int32_t* part, double* Kc, double* Ain) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e0 = blockIdx.x * (int64_t)blockDim.x; e0 < E; e0 += stride) {
+    const int64_t e = e0 + threadIdx.x;
+    const bool ok = e < E;
+    const double x = ok ? 2.0 * (double)w[e] : 0.0;
+    const int32_t a = ok ? part[src[e]] : -1, b = ok ? part[dst[e]] : -1;
+    warp_group_add(Kc, a, x);
+    warp_group_add(Ain, (a >= 0 && a == b) ? a : -1, x);
+  }
+}
+
 // Raises the dynamic shared memory limit of nm_accum_smem_kernel on the
 // current device to at least `smem` bytes.  The limit only ever grows, under
 // one lock shared by every caller, so a launch never finds it lowered by a
@@ -2568,7 +2586,7 @@ static void nm_accum(const int32_t* src, const int32_t* dst, const float* w, int
 }
 
 double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
-                       const int32_t* part, Arena& a, cudaStream_t s) {
+                       const int32_t* part, Arena& a, cudaStream_t s, bool symmetric) {
   HiScope hs(a);
   double* Kc = a.hi_n<double>(C);
   double* Ain = a.hi_n<double>(C);
@@ -2576,7 +2594,12 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
   double* twoW = a.hi_n<double>(2);
   LVG_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * std::max(C, 1), s));
   LVG_CUDA(cudaMemsetAsync(Ain, 0, sizeof(double) * std::max(C, 1), s));
-  nm_accum(src, dst, w, E, C, part, Kc, Ain, nullptr, s);   // ids checked on the host
+  if (symmetric && E > 0 && C > kNmSmemMax) {
+    nm_accum_sym_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
+    LVG_LAUNCH();
+  } else {
+    nm_accum(src, dst, w, E, C, part, Kc, Ain, nullptr, s);   // ids checked on the host
+  }
   tree_sum_f64(Kc, C, twoW, a, s);
   nm_term_kernel<<<sm_grid(C, kThreads), kThreads, 0, s>>>(Kc, Ain, C, twoW, t);
   LVG_LAUNCH();

@@ -173,8 +173,10 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
                float** out_w, Arena& a, cudaStream_t s);
 
 // FP64 Newman modularity of part[] (values < C) over an input list (device).
+// symmetric: the list is known to hold (v, u, w) for every (u, v, w) (its
+// community strengths are then summed from the source side alone).
 double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t C,
-                       const int32_t* part, Arena& a, cudaStream_t s);
+                       const int32_t* part, Arena& a, cudaStream_t s, bool symmetric = false);
 
 // The same modularity with caller-provided scratch: Kc, Ain, t of C doubles,
 // partials of ceil(C/2048) doubles; twoW_q[0] = 2W, twoW_q[1] = Q (device).
