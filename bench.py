@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default degree thresholds instead of tuning them on the workload graph")
+    ap.add_argument("--thresholds", default="",
+                    help="TILE,BLOCK: run with these degree thresholds instead of tuning (profiling runs)")
     ap.add_argument("--graphs", type=int, default=8192, help="batched workload: number of graphs")
     ap.add_argument("--batch-entries", type=float, default=1.25e8,
                     help="batched/serving workloads: entries per packed sub-batch")
@@ -337,7 +339,14 @@ def run_ours(args, world, rank, local, pg):
     # degree thresholds of the move kernels: tuned once on this graph, outside
     # the timed region (a shape class is tuned once per process)
     tune = {"tile_max_degree": 512, "block_max_degree": 4096, "autotuned": False}
-    if not args.no_autotune:
+    if args.thresholds:
+        t_, b_ = (int(x) for x in args.thresholds.split(","))
+        lv.close()
+        lv = Louvain(device=local, level_min_gain=level_min, tile_max_degree=t_, block_max_degree=b_)
+        lv.set_stream(stream.cuda_stream)
+        lv.load_edges_device(ds.data_ptr(), dd.data_ptr(), dw.data_ptr(), E, n)
+        tune = {"tile_max_degree": t_, "block_max_degree": b_, "autotuned": False, "given": True}
+    elif not args.no_autotune:
         from louvaingpu_b200 import LvgError
         t_tune = time.perf_counter()
         try:
