@@ -6,7 +6,8 @@
 // 4096-key tile (taken in launch order from a counter) ranks its keys stably
 // in shared memory (warp __match_any_sync multisplit), learns the counts of
 // its digits in all earlier tiles by decoupled look-back (bounded spin, error
-// flag), and writes its keys out digit run by digit run.
+// flag), and writes its keys out digit run by digit run.  A tile is 512
+// threads of 8 keys.
 #include <atomic>
 #include <mutex>
 
@@ -104,10 +105,11 @@ void finish_impl(const double* p, int64_t n, double* d_out, Arena& a, cudaStream
 }
 
 // ---------------------------------------------------------------------------
-constexpr int kRsThreads = 256;
-constexpr int kRsItems = 16;
-constexpr int kRsTile = kRsThreads * kRsItems;  // 4096 keys
-constexpr int kRsWarps = kRsThreads / 32;
+constexpr int kRsThreads = 256;        // histogram kernels: thread = digit
+constexpr int kRsSweepThreads = 512;   // one-sweep tile: 16 warps, 8 keys per thread
+constexpr int kRsItems = 8;
+constexpr int kRsTile = kRsSweepThreads * kRsItems;  // 4096 keys
+constexpr int kRsWarps = kRsSweepThreads / 32;
 constexpr int kRadix = 256;
 
 // One pass over the keys gives the global histogram of every digit position.
@@ -141,6 +143,26 @@ __global__ void __launch_bounds__(kRsThreads) rs_gscan_kernel(uint32_t* ghist, i
   }
 }
 
+// Block (512-thread) exclusive scan of one value per thread.
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan512(T v, T* total) {
+  __shared__ T wsum[16];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const T inc = warp_inclusive_scan(v);
+  if (lane == 31) wsum[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    T x = lane < 16 ? wsum[lane] : T(0);
+    x = warp_inclusive_scan(x);
+    if (lane < 16) wsum[lane] = x;
+  }
+  __syncthreads();
+  const T base = w > 0 ? wsum[w - 1] : T(0);
+  *total = wsum[15];
+  __syncthreads();
+  return base + inc - v;
+}
+
 struct RsSmem {
   uint64_t key[kRsTile];
   float val[kRsTile];
@@ -152,7 +174,9 @@ struct RsSmem {
 
 // Look-back words, one per (tile, digit): code in bits 56..63 (2p+1: this
 // tile's count, 2p+2: count of every tile up to this one, for pass p; codes of
-// earlier passes read as "not yet"), count in bits 0..31.
+// earlier passes read as "not yet"), count in bits 0..31.  A tile is 512
+// threads of 8 keys: twice the warps per SM of 256 threads of 16 keys at the
+// same shared memory per key.
 constexpr int kRsSpinLimit = 1 << 22;
 // Test hook (lvg_debug_radix_hold): a smaller spin limit and one tile that
 // never publishes, so that the bounded wait of its successors runs out.
@@ -167,17 +191,15 @@ __device__ __forceinline__ void rs_publish(unsigned long long* w, unsigned code,
 // by digit in shared memory, learns the keys of its digits in all earlier
 // tiles by decoupled look-back, and writes its keys out digit run by digit
 // run.  Stable: ranks follow key order inside a tile and tiles in order.
-__global__ void __launch_bounds__(kRsThreads) rs_onesweep_kernel(const uint64_t* kin, const float* vin,
-                                                                 uint64_t* kout, float* vout, int64_t n,
-                                                                 int shift, int pass, const uint32_t* gstart,
-                                                                 unsigned long long* look, uint32_t* counter,
-                                                                 uint32_t* err, int spin_limit, int64_t hold) {
+__global__ void __launch_bounds__(kRsSweepThreads, 2) rs_onesweep_kernel(
+    const uint64_t* kin, const float* vin, uint64_t* kout, float* vout, int64_t n, int shift, int pass,
+    const uint32_t* gstart, unsigned long long* look, uint32_t* counter, uint32_t* err, int spin_limit, int64_t hold) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RsSmem& S = *reinterpret_cast<RsSmem*>(smem_raw);
   const unsigned full = 0xffffffffu;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) S.tile = atomicAdd(counter, 1u);
-  for (int i = threadIdx.x; i < kRsWarps * (kRadix + 1); i += kRsThreads) (&S.wc[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < kRsWarps * (kRadix + 1); i += kRsSweepThreads) (&S.wc[0][0])[i] = 0;
   __syncthreads();
   const int64_t tile = S.tile;
   const int64_t tile0 = tile * kRsTile;
@@ -207,38 +229,41 @@ __global__ void __launch_bounds__(kRsThreads) rs_onesweep_kernel(const uint64_t*
     __syncwarp();
   }
   __syncthreads();
-  // thread = digit: prefix over warps, tile count, look-back across tiles
+  // threads 0..255 = digits: prefix over warps, tile count, look-back across tiles
   const int d = threadIdx.x;
-  uint32_t cnt = 0;
+  uint32_t cnt = 0, excl = 0;
+  if (d < kRadix) {
 #pragma unroll
-  for (int ww = 0; ww < kRsWarps; ++ww) {
-    const uint32_t t = S.wc[ww][d];
-    S.wc[ww][d] = cnt;
-    cnt += t;
-  }
-  const unsigned agg = 2u * (unsigned)pass + 1u, inc = agg + 1u;
-  unsigned long long* mine = look + tile * kRadix + d;
-  const bool publish = tile != hold;   // hold: a test makes this tile's successors wait out their limit
-  uint32_t excl = 0;
-  if (tile == 0) {
-    if (publish) rs_publish(mine, inc, cnt);
-  } else {
-    if (publish) rs_publish(mine, agg, cnt);
-    int64_t j = tile - 1;
-    int spins = 0;
-    while (j >= 0) {
-      const unsigned long long x = *reinterpret_cast<volatile unsigned long long*>(look + j * kRadix + d);
-      const unsigned code = (unsigned)(x >> 56);
-      if (code == inc) { excl += (uint32_t)x; break; }
-      if (code == agg) { excl += (uint32_t)x; --j; continue; }
-      if (++spins > spin_limit) { atomicOr(err, 1u); break; }   // bounded wait: report, never hang
+    for (int ww = 0; ww < kRsWarps; ++ww) {
+      const uint32_t t = S.wc[ww][d];
+      S.wc[ww][d] = cnt;
+      cnt += t;
     }
-    if (publish) rs_publish(mine, inc, excl + cnt);
+    const unsigned agg = 2u * (unsigned)pass + 1u, inc = agg + 1u;
+    unsigned long long* mine = look + tile * kRadix + d;
+    const bool publish = tile != hold;   // hold: a test makes this tile's successors wait out their limit
+    if (tile == 0) {
+      if (publish) rs_publish(mine, inc, cnt);
+    } else {
+      if (publish) rs_publish(mine, agg, cnt);
+      int64_t j = tile - 1;
+      int spins = 0;
+      while (j >= 0) {
+        const unsigned long long x = *reinterpret_cast<volatile unsigned long long*>(look + j * kRadix + d);
+        const unsigned code = (unsigned)(x >> 56);
+        if (code == inc) { excl += (uint32_t)x; break; }
+        if (code == agg) { excl += (uint32_t)x; --j; continue; }
+        if (++spins > spin_limit) { atomicOr(err, 1u); break; }   // bounded wait: report, never hang
+      }
+      if (publish) rs_publish(mine, inc, excl + cnt);
+    }
   }
   uint32_t tot;
-  const uint32_t start = block_exclusive_scan<uint32_t>(cnt, &tot);
-  S.dstart[d] = start;
-  S.gbase[d] = gstart[d] + excl;
+  const uint32_t start = block_exclusive_scan512<uint32_t>(d < kRadix ? cnt : 0u, &tot);
+  if (d < kRadix) {
+    S.dstart[d] = start;
+    S.gbase[d] = gstart[d] + excl;
+  }
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < kRsItems; ++j) {
@@ -252,7 +277,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_onesweep_kernel(const uint64_t*
   __syncthreads();
   int64_t tn = n - tile0;
   if (tn > kRsTile) tn = kRsTile;
-  for (int p = threadIdx.x; p < tn; p += kRsThreads) {
+  for (int p = threadIdx.x; p < tn; p += kRsSweepThreads) {
     const uint64_t kk = S.key[p];
     const unsigned dd = (unsigned)(kk >> shift) & (kRadix - 1);
     const uint32_t o = S.gbase[dd] + ((uint32_t)p - S.dstart[dd]);
@@ -307,6 +332,8 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
   std::call_once(attr_once, [] {
     LVG_CUDA(cudaFuncSetAttribute(rs_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(RsSmem)));
+    LVG_CUDA(cudaFuncSetAttribute(rs_onesweep_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
   });
   const int npass = (std::min(bits, 64) + 7) / 8;
   HiScope hs(a);
@@ -326,7 +353,7 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
   uint64_t* K[2] = {k0, k1};
   float* Vv[2] = {v0, v1};
   for (int p = 0; p < npass; ++p) {
-    rs_onesweep_kernel<<<(unsigned)ntiles, kRsThreads, sizeof(RsSmem), s>>>(
+    rs_onesweep_kernel<<<(unsigned)ntiles, kRsSweepThreads, sizeof(RsSmem), s>>>(
         K[cur], Vv[cur], K[cur ^ 1], Vv[cur ^ 1], n, 8 * p, p, ghist + p * kRadix, look, counters + p, err,
         g_rs_spin_limit.load(), g_rs_hold_tile.load());
     LVG_LAUNCH();
