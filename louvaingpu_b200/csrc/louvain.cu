@@ -1196,14 +1196,15 @@ __global__ void int_weights_kernel(const float* cw, int64_t nnz, const double* k
 // A bucket holds a disjoint set of communities, so its best candidate and
 // count are those of the row restricted to that set, and combining buckets
 // with `better` gives the row's argmax and tie-break.
-constexpr int kHubItems = kHubChunk / kThreads;   // entries per thread of a chunk
+constexpr int kHubPartThreads = 512;              // chunk blocks: 16 warps of 8 entries per lane
+constexpr int kHubItems = kHubChunk / kHubPartThreads;
 constexpr int kHubBucketTarget = 1024;            // mean entries of a bucket
 constexpr int kHubMaxBucketsLog = 12;
 constexpr int kAggLog = 11;                       // shared table of 2048 slots
 constexpr int kAggSlots = 1 << kAggLog;
 constexpr int kAggFull = kAggSlots / 2;           // more claims: the bucket is split into sub-passes
 constexpr int kAggMaxSplitLog = 16;               // beyond 2^16 sub-passes: report, give up
-static_assert(kHubChunk % kThreads == 0 && kHubChunk <= 65535, "chunk offsets are 16-bit");
+static_assert(kHubChunk % kHubPartThreads == 0 && kHubChunk <= 65535, "chunk offsets are 16-bit");
 
 __device__ __forceinline__ uint32_t hub_bucket(int32_t c, int plog) {
   return plog == 0 ? 0u : (uint32_t)(((uint64_t)(uint32_t)c * 0x9E3779B97F4A7C15ull) >> (64 - plog));
@@ -1234,7 +1235,7 @@ struct HubArgs {
   int64_t nbucket;
 };
 
-__global__ void __launch_bounds__(kThreads) hub_part_kernel(MoveArgs P, HubArgs H) {
+__global__ void __launch_bounds__(kHubPartThreads) hub_part_kernel(MoveArgs P, HubArgs H) {
   __shared__ uint32_t cnt[1 << kHubMaxBucketsLog];
   if (P.ctl->done) return;
   const int64_t ch = blockIdx.x;
@@ -1245,13 +1246,13 @@ __global__ void __launch_bounds__(kThreads) hub_part_kernel(MoveArgs P, HubArgs 
   const int64_t end = min(beg + (int64_t)kHubChunk, P.off[i + 1]);
   const int plog = H.hub_plog[h];
   const int nb = 1 << plog;
-  for (int x = threadIdx.x; x < nb; x += kThreads) cnt[x] = 0;
+  for (int x = threadIdx.x; x < nb; x += kHubPartThreads) cnt[x] = 0;
   __syncthreads();
   int32_t c[kHubItems];
   float w[kHubItems];
 #pragma unroll
   for (int u = 0; u < kHubItems; ++u) {
-    const int64_t e = beg + u * kThreads + threadIdx.x;
+    const int64_t e = beg + u * kHubPartThreads + threadIdx.x;
     c[u] = e < end ? __ldcs(P.col + e) : -1;
     w[u] = e < end ? __ldcs(P.cw + e) : 0.0f;
   }
@@ -1271,12 +1272,12 @@ __global__ void __launch_bounds__(kThreads) hub_part_kernel(MoveArgs P, HubArgs 
   }
   __syncthreads();
   // bucket starts: each thread scans a run of consecutive buckets
-  const int per = (nb + kThreads - 1) / kThreads;
+  const int per = (nb + kHubPartThreads - 1) / kHubPartThreads;
   const int x0 = min((int)threadIdx.x * per, nb), x1 = min(x0 + per, nb);
   uint32_t local = 0;
   for (int x = x0; x < x1; ++x) local += cnt[x];
   uint32_t total;
-  uint32_t run = block_exclusive_scan256<uint32_t>(local, &total);
+  uint32_t run = block_exclusive_scan512<uint32_t>(local, &total);
   uint16_t* off = H.cb_off + H.chunk_cbo[ch];
   for (int x = x0; x < x1; ++x) {
     const uint32_t v = cnt[x];
@@ -2313,7 +2314,7 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     H.hub_plog = g.hub_plog; H.hub_cb0 = g.hub_cb0; H.hub_bb0 = g.hub_bb0; H.bucket_hub = g.bucket_hub;
     H.cb_off = g.cb_off; H.stage = g.stage; H.sawown = g.hub_sawown; H.part = g.hub_part;
     H.nbucket = g.nhub_bucket;
-    hub_part_kernel<<<(unsigned)g.nchunk, kThreads, 0, sh>>>(P, H);
+    hub_part_kernel<<<(unsigned)g.nchunk, kHubPartThreads, 0, sh>>>(P, H);
     LVG_LAUNCH();
     const size_t smem = g.int_acc ? agg_smem_bytes<true>() : agg_smem_bytes<false>();
     const int per_sm = std::max(1, std::min(8, (int)((227u * 1024u) / (smem + 1024))));

@@ -164,6 +164,26 @@ __device__ __forceinline__ T block_exclusive_scan256(T v, T* total) {
   return base + inc - v;
 }
 
+// Block (512-thread) exclusive scan of one value per thread.
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan512(T v, T* total) {
+  __shared__ T wsum[16];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const T inc = warp_inclusive_scan(v);
+  if (lane == 31) wsum[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    T x = lane < 16 ? wsum[lane] : T(0);
+    x = warp_inclusive_scan(x);
+    if (lane < 16) wsum[lane] = x;
+  }
+  __syncthreads();
+  const T base = w > 0 ? wsum[w - 1] : T(0);
+  *total = wsum[15];
+  __syncthreads();
+  return base + inc - v;
+}
+
 // Counter-based random numbers (splitmix64 finaliser), identical on host and
 // device so that generated graphs do not depend on where they are generated.
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {

@@ -143,26 +143,6 @@ __global__ void __launch_bounds__(kRsThreads) rs_gscan_kernel(uint32_t* ghist, i
   }
 }
 
-// Block (512-thread) exclusive scan of one value per thread.
-template <typename T>
-__device__ __forceinline__ T block_exclusive_scan512(T v, T* total) {
-  __shared__ T wsum[16];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const T inc = warp_inclusive_scan(v);
-  if (lane == 31) wsum[w] = inc;
-  __syncthreads();
-  if (w == 0) {
-    T x = lane < 16 ? wsum[lane] : T(0);
-    x = warp_inclusive_scan(x);
-    if (lane < 16) wsum[lane] = x;
-  }
-  __syncthreads();
-  const T base = w > 0 ? wsum[w - 1] : T(0);
-  *total = wsum[15];
-  __syncthreads();
-  return base + inc - v;
-}
-
 struct RsSmem {
   uint64_t key[kRsTile];
   float val[kRsTile];
