@@ -422,20 +422,14 @@ __device__ __forceinline__ int ceil_log2(int64_t x) {  // x >= 1
   return x <= 1 ? 0 : 64 - __clzll((unsigned long long)(x - 1));
 }
 
-// Open-addressing insert of (c, w) into a table of 2^logT slots; a slot the
-// insert claims is appended to the claimed list.
+// Open-addressing insert of (c, w) into a table of 2^logT slots.
 template <typename Acc>
-__device__ __forceinline__ bool table_insert(int32_t* keys, Acc* vals, int logT, int32_t c, Acc w,
-                                             uint16_t* claimed, int* nclaimed) {
+__device__ __forceinline__ bool table_insert(int32_t* keys, Acc* vals, int logT, int32_t c, Acc w) {
   uint32_t T = 1u << logT;
   uint32_t h = hash_c(c, logT);
   for (uint32_t p = 0; p < T; ++p) {
     int32_t prev = atomicCAS(&keys[h], -1, c);
-    if (prev == -1 || prev == c) {
-      atomicAdd(&vals[h], w);
-      if (prev == -1) claimed[atomicAdd(nclaimed, 1)] = (uint16_t)h;
-      return true;
-    }
+    if (prev == -1 || prev == c) { atomicAdd(&vals[h], w); return true; }
     h = (h + 1) & (T - 1);
   }
   return false;
@@ -467,16 +461,13 @@ template <typename Acc, int NT>
 __global__ void __launch_bounds__(NT) move_block_kernel(MoveArgs P, int maxLog, int64_t dlo, int64_t dhi) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double rg[NT / 32], rw[NT / 32];
-  __shared__ int32_t rc[NT / 32], rs[NT / 32];
-  __shared__ int nclaimed;
+  __shared__ int32_t rc[NT / 32], rn[NT / 32], rs[NT / 32];
   if (P.ctl->done) return;
   const int Tmax = 1 << maxLog;
   Acc* vals = reinterpret_cast<Acc*>(smem);
   int32_t* keys = reinterpret_cast<int32_t*>(vals + Tmax);
-  uint16_t* claimed = reinterpret_cast<uint16_t*>(keys + Tmax);
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int s = threadIdx.x; s < Tmax; s += NT) { keys[s] = -1; vals[s] = Acc(0); }
-  if (threadIdx.x == 0) nclaimed = 0;
   __syncthreads();
   bool overflow = false;
   for (int64_t item = blockIdx.x; item < P.n; item += gridDim.x) {
@@ -485,6 +476,7 @@ __global__ void __launch_bounds__(NT) move_block_kernel(MoveArgs P, int maxLog, 
     if (end - beg <= dlo || end - beg > dhi) continue;   // another band takes this degree
     int32_t own = P.comm[i];
     int logT = min(maxLog, max(5, ceil_log2(2 * (end - beg))));
+    int T = 1 << logT;
     bool sawown = false;
     for (int64_t e0 = beg + threadIdx.x; e0 < end; e0 += kUnroll * NT) {
       int32_t c[kUnroll];
@@ -494,52 +486,54 @@ __global__ void __launch_bounds__(NT) move_block_kernel(MoveArgs P, int maxLog, 
       for (int u = 0; u < kUnroll; ++u) {
         if (c[u] != kNone) {
           sawown |= (c[u] == own);
-          if (!table_insert<Acc>(keys, vals, logT, c[u], (Acc)wv[u], claimed, &nclaimed)) overflow = true;
+          if (!table_insert<Acc>(keys, vals, logT, c[u], (Acc)wv[u])) overflow = true;
         }
       }
     }
     __syncthreads();
-    // only the claimed slots: the distinct neighbour communities
-    const int nc = nclaimed;
     double kf = P.kfrac[i];
     double bg = 0.0, bw = 0.0;
     int32_t bc = kNone;
-    for (int x0 = threadIdx.x; x0 < nc; x0 += kUnroll * NT) {
+    int nocc = 0;
+    for (int s0 = threadIdx.x; s0 < T; s0 += kUnroll * NT) {
       int32_t c[kUnroll];
       double W[kUnroll], t[kUnroll];
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
-        const int x = x0 + u * NT;
-        const int sl = x < nc ? claimed[x] : -1;
-        c[u] = sl >= 0 ? keys[sl] : -1;
-        W[u] = sl >= 0 ? (double)vals[sl] : 0.0;
-        if (sl >= 0) { keys[sl] = -1; vals[sl] = Acc(0); }
+        const int s = s0 + u * NT;
+        c[u] = s < T ? keys[s] : -1;
+        W[u] = c[u] >= 0 ? (double)vals[s] : 0.0;
+        if (c[u] >= 0) { keys[s] = -1; vals[s] = Acc(0); }
       }
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) t[u] = (c[u] >= 0 && W[u] != 0.0) ? P.tot[c[u]] : 0.0;
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u) {
-        if (c[u] >= 0 && W[u] != 0.0) {                                // OneLevelKernel.cu:303
-          const double g = __dsub_rn(W[u], __dmul_rn(t[u], kf));      // OneLevelKernel.cu:307-313
-          if (g > 0.0 && better(g, c[u], bg, bc)) { bg = g; bc = c[u]; bw = W[u]; }
+        if (c[u] >= 0) {
+          ++nocc;
+          if (W[u] != 0.0) {                                            // OneLevelKernel.cu:303
+            const double g = __dsub_rn(W[u], __dmul_rn(t[u], kf));      // OneLevelKernel.cu:307-313
+            if (g > 0.0 && better(g, c[u], bg, bc)) { bg = g; bc = c[u]; bw = W[u]; }
+          }
         }
       }
     }
     warp_best(bg, bc, bw);
+    nocc = __reduce_add_sync(0xffffffffu, (unsigned)nocc);
     int so = __any_sync(0xffffffffu, sawown) ? 1 : 0;
-    if (lane == 0) { rg[w] = bg; rc[w] = bc; rw[w] = bw; rs[w] = so; }
+    if (lane == 0) { rg[w] = bg; rc[w] = bc; rw[w] = bw; rn[w] = nocc; rs[w] = so; }
     __syncthreads();
     if (threadIdx.x == 0) {
       double g = rg[0], ww = rw[0];
       int32_t c = rc[0];
-      int sw = rs[0];
+      int n = rn[0], sw = rs[0];
       for (int k2 = 1; k2 < NT / 32; ++k2) {
         if (better(rg[k2], rc[k2], g, c)) { g = rg[k2]; c = rc[k2]; ww = rw[k2]; }
+        n += rn[k2];
         sw |= rs[k2];
       }
-      int32_t nseg = nc + ((P.has_loop[i] && !sw) ? 1 : 0);
+      int32_t nseg = n + ((P.has_loop[i] && !sw) ? 1 : 0);
       apply_decision(P, i, own, c, ww, nseg);
-      nclaimed = 0;
     }
     __syncthreads();
   }
@@ -2262,8 +2256,8 @@ static void set_move_attributes() {
                                 (int)agg_smem_bytes<true>()));
   LVG_CUDA(cudaFuncSetAttribute(hub_agg_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)agg_smem_bytes<false>()));
-  // block bands: up to 2 * 8192 slots of int32 key + f64 sum + u16 claimed entry (block_max <= 8192)
-  const int big = (int)((size_t)16384 * (sizeof(double) + sizeof(int32_t) + sizeof(uint16_t)));
+  // block bands: up to 2 * 8192 slots of int32 key + f64 sum (block_max <= 8192)
+  const int big = (int)((size_t)16384 * (sizeof(double) + sizeof(int32_t)));
   LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<int, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<int, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   LVG_CUDA(cudaFuncSetAttribute(move_block_kernel<double, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -2335,8 +2329,7 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
       const int64_t h = std::min<int64_t>(hi, g.block_max);
       int lg = 5;
       while (((int64_t)1 << lg) < 2 * h) ++lg;
-      const size_t slot = (g.int_acc ? sizeof(int32_t) + sizeof(int32_t) : sizeof(double) + sizeof(int32_t)) +
-                          sizeof(uint16_t);   // key, sum and a claimed-list entry
+      const size_t slot = g.int_acc ? sizeof(int32_t) + sizeof(int32_t) : sizeof(double) + sizeof(int32_t);
       const size_t smem = ((size_t)1 << lg) * slot;
       const bool narrow = h <= 1024;
       const unsigned grid = (unsigned)std::min<int64_t>(Q.n, (int64_t)sm_count() * (narrow ? 16 : 8));
