@@ -6,8 +6,7 @@
 // 4096-key tile (taken in launch order from a counter) ranks its keys stably
 // in shared memory (warp __match_any_sync multisplit), learns the counts of
 // its digits in all earlier tiles by decoupled look-back (bounded spin, error
-// flag), and writes its keys out digit run by digit run.  A tile is 512
-// threads of 8 keys.
+// flag), and writes its keys out digit run by digit run.
 #include <atomic>
 #include <mutex>
 
@@ -105,11 +104,10 @@ void finish_impl(const double* p, int64_t n, double* d_out, Arena& a, cudaStream
 }
 
 // ---------------------------------------------------------------------------
-constexpr int kRsThreads = 256;        // histogram kernels: thread = digit
-constexpr int kRsSweepThreads = 512;   // one-sweep tile: 16 warps, 8 keys per thread
-constexpr int kRsItems = 8;
-constexpr int kRsTile = kRsSweepThreads * kRsItems;  // 4096 keys
-constexpr int kRsWarps = kRsSweepThreads / 32;
+constexpr int kRsThreads = 256;
+constexpr int kRsItems = 16;
+constexpr int kRsTile = kRsThreads * kRsItems;  // 4096 keys
+constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kRadix = 256;
 
 // One pass over the keys gives the global histogram of every digit position.
@@ -154,9 +152,7 @@ struct RsSmem {
 
 // Look-back words, one per (tile, digit): code in bits 56..63 (2p+1: this
 // tile's count, 2p+2: count of every tile up to this one, for pass p; codes of
-// earlier passes read as "not yet"), count in bits 0..31.  A tile is 512
-// threads of 8 keys: twice the warps per SM of 256 threads of 16 keys at the
-// same shared memory per key.
+// earlier passes read as "not yet"), count in bits 0..31.
 constexpr int kRsSpinLimit = 1 << 22;
 // Test hook (lvg_debug_radix_hold): a smaller spin limit and one tile that
 // never publishes, so that the bounded wait of its successors runs out.
@@ -171,15 +167,17 @@ __device__ __forceinline__ void rs_publish(unsigned long long* w, unsigned code,
 // by digit in shared memory, learns the keys of its digits in all earlier
 // tiles by decoupled look-back, and writes its keys out digit run by digit
 // run.  Stable: ranks follow key order inside a tile and tiles in order.
-__global__ void __launch_bounds__(kRsSweepThreads, 2) rs_onesweep_kernel(
-    const uint64_t* kin, const float* vin, uint64_t* kout, float* vout, int64_t n, int shift, int pass,
-    const uint32_t* gstart, unsigned long long* look, uint32_t* counter, uint32_t* err, int spin_limit, int64_t hold) {
+__global__ void __launch_bounds__(kRsThreads) rs_onesweep_kernel(const uint64_t* kin, const float* vin,
+                                                                 uint64_t* kout, float* vout, int64_t n,
+                                                                 int shift, int pass, const uint32_t* gstart,
+                                                                 unsigned long long* look, uint32_t* counter,
+                                                                 uint32_t* err, int spin_limit, int64_t hold) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RsSmem& S = *reinterpret_cast<RsSmem*>(smem_raw);
   const unsigned full = 0xffffffffu;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) S.tile = atomicAdd(counter, 1u);
-  for (int i = threadIdx.x; i < kRsWarps * (kRadix + 1); i += kRsSweepThreads) (&S.wc[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < kRsWarps * (kRadix + 1); i += kRsThreads) (&S.wc[0][0])[i] = 0;
   __syncthreads();
   const int64_t tile = S.tile;
   const int64_t tile0 = tile * kRsTile;
@@ -209,41 +207,38 @@ __global__ void __launch_bounds__(kRsSweepThreads, 2) rs_onesweep_kernel(
     __syncwarp();
   }
   __syncthreads();
-  // threads 0..255 = digits: prefix over warps, tile count, look-back across tiles
+  // thread = digit: prefix over warps, tile count, look-back across tiles
   const int d = threadIdx.x;
-  uint32_t cnt = 0, excl = 0;
-  if (d < kRadix) {
+  uint32_t cnt = 0;
 #pragma unroll
-    for (int ww = 0; ww < kRsWarps; ++ww) {
-      const uint32_t t = S.wc[ww][d];
-      S.wc[ww][d] = cnt;
-      cnt += t;
+  for (int ww = 0; ww < kRsWarps; ++ww) {
+    const uint32_t t = S.wc[ww][d];
+    S.wc[ww][d] = cnt;
+    cnt += t;
+  }
+  const unsigned agg = 2u * (unsigned)pass + 1u, inc = agg + 1u;
+  unsigned long long* mine = look + tile * kRadix + d;
+  const bool publish = tile != hold;   // hold: a test makes this tile's successors wait out their limit
+  uint32_t excl = 0;
+  if (tile == 0) {
+    if (publish) rs_publish(mine, inc, cnt);
+  } else {
+    if (publish) rs_publish(mine, agg, cnt);
+    int64_t j = tile - 1;
+    int spins = 0;
+    while (j >= 0) {
+      const unsigned long long x = *reinterpret_cast<volatile unsigned long long*>(look + j * kRadix + d);
+      const unsigned code = (unsigned)(x >> 56);
+      if (code == inc) { excl += (uint32_t)x; break; }
+      if (code == agg) { excl += (uint32_t)x; --j; continue; }
+      if (++spins > spin_limit) { atomicOr(err, 1u); break; }   // bounded wait: report, never hang
     }
-    const unsigned agg = 2u * (unsigned)pass + 1u, inc = agg + 1u;
-    unsigned long long* mine = look + tile * kRadix + d;
-    const bool publish = tile != hold;   // hold: a test makes this tile's successors wait out their limit
-    if (tile == 0) {
-      if (publish) rs_publish(mine, inc, cnt);
-    } else {
-      if (publish) rs_publish(mine, agg, cnt);
-      int64_t j = tile - 1;
-      int spins = 0;
-      while (j >= 0) {
-        const unsigned long long x = *reinterpret_cast<volatile unsigned long long*>(look + j * kRadix + d);
-        const unsigned code = (unsigned)(x >> 56);
-        if (code == inc) { excl += (uint32_t)x; break; }
-        if (code == agg) { excl += (uint32_t)x; --j; continue; }
-        if (++spins > spin_limit) { atomicOr(err, 1u); break; }   // bounded wait: report, never hang
-      }
-      if (publish) rs_publish(mine, inc, excl + cnt);
-    }
+    if (publish) rs_publish(mine, inc, excl + cnt);
   }
   uint32_t tot;
-  const uint32_t start = block_exclusive_scan512<uint32_t>(d < kRadix ? cnt : 0u, &tot);
-  if (d < kRadix) {
-    S.dstart[d] = start;
-    S.gbase[d] = gstart[d] + excl;
-  }
+  const uint32_t start = block_exclusive_scan<uint32_t>(cnt, &tot);
+  S.dstart[d] = start;
+  S.gbase[d] = gstart[d] + excl;
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < kRsItems; ++j) {
@@ -257,7 +252,7 @@ __global__ void __launch_bounds__(kRsSweepThreads, 2) rs_onesweep_kernel(
   __syncthreads();
   int64_t tn = n - tile0;
   if (tn > kRsTile) tn = kRsTile;
-  for (int p = threadIdx.x; p < tn; p += kRsSweepThreads) {
+  for (int p = threadIdx.x; p < tn; p += kRsThreads) {
     const uint64_t kk = S.key[p];
     const unsigned dd = (unsigned)(kk >> shift) & (kRadix - 1);
     const uint32_t o = S.gbase[dd] + ((uint32_t)p - S.dstart[dd]);
@@ -312,8 +307,6 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
   std::call_once(attr_once, [] {
     LVG_CUDA(cudaFuncSetAttribute(rs_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(RsSmem)));
-    LVG_CUDA(cudaFuncSetAttribute(rs_onesweep_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  (int)cudaSharedmemCarveoutMaxShared));
   });
   const int npass = (std::min(bits, 64) + 7) / 8;
   HiScope hs(a);
@@ -333,7 +326,7 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
   uint64_t* K[2] = {k0, k1};
   float* Vv[2] = {v0, v1};
   for (int p = 0; p < npass; ++p) {
-    rs_onesweep_kernel<<<(unsigned)ntiles, kRsSweepThreads, sizeof(RsSmem), s>>>(
+    rs_onesweep_kernel<<<(unsigned)ntiles, kRsThreads, sizeof(RsSmem), s>>>(
         K[cur], Vv[cur], K[cur ^ 1], Vv[cur ^ 1], n, 8 * p, p, ghist + p * kRadix, look, counters + p, err,
         g_rs_spin_limit.load(), g_rs_hold_tile.load());
     LVG_LAUNCH();
