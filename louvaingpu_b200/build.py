@@ -19,7 +19,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "liblvg.so")
 GENLIB = os.path.join(HERE, "liblvggen.so")
 
-CU_SOURCES = ["prims.cu", "louvain.cu", "capi.cu", "noalloc.cu", "gen_device.cu", "server.cu"]
+CU_SOURCES = ["prims.cu", "louvain.cu", "induce.cu", "capi.cu", "noalloc.cu", "gen_device.cu", "server.cu"]
 CU_HEADERS = ["lvg_internal.cuh", "prims.cuh", "louvain.cuh"]
 GEN_SOURCES = ["gen_host.cpp"]
 

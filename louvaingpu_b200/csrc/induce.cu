@@ -1,0 +1,668 @@
+// Coarsening of a level whose list is strictly sorted and symmetric (every
+// level after the first, and a first level given in that form), without a
+// device-wide sort of all its entries.
+//
+// The reference maps both endpoints of every entry to communities, sorts the
+// (cu, cv) keys and sums equal keys (InducedGraphKernel.cu:28-48,84-113).
+// Here the list's rows are laid out community by community instead: the
+// members of each community (in vertex order) are found by a stable sort of
+// the V community ids, and the rows of the members of one community, read in
+// member order, form that community's segment -- entries already grouped by
+// cu, at positions known from a scan of the row lengths.  The position range
+// is cut into chunks of 4096 entries.  A 512-thread block takes a chunk:
+// it gathers cv = part[dst] for its entries, sorts (segment, cv) keys in
+// shared memory (stable 8-bit LSD passes over only the bits the chunk needs),
+// and sums equal keys in a fixed order.  A segment that lies inside one chunk
+// is then final.  Segments that cross a chunk boundary (the large
+// communities) leave one partial run per chunk and distinct cv; only those
+// partial runs -- a fraction of the entries -- go through the device-wide
+// radix sort, keyed by (open segment, cv), and are summed again.  A scan of
+// the distinct counts of every community places each community's entries.
+//
+// Output: the same list as the sort-based path (entries ordered by (cu, cv),
+// weights 0 counted as 1, sums in FP64 rounded once to float).  Sums of equal
+// keys run in a fixed order that does not depend on timing.
+#include <algorithm>
+#include <mutex>
+
+#include "louvain.cuh"
+#include "prims.cuh"
+
+namespace lvg {
+namespace {
+
+constexpr int kIcThreads = 512;
+constexpr int kIcItems = 8;
+constexpr int kIcChunk = kIcThreads * kIcItems;   // list positions per chunk
+constexpr int kIcWarps = kIcThreads / 32;
+constexpr int kIcRadix = 256;
+constexpr int kIcRelBits = 13;                    // member index inside a chunk, 0..4096
+constexpr uint32_t kIcRelMask = (1u << kIcRelBits) - 1u;
+constexpr int kIcFlat = 256;                      // threads of the flat kernels
+
+enum : uint32_t { kOpenL = 1u, kOpenR = 2u, kSingle = 4u };
+
+int ic_sms() {
+  static const int sms = [] {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+  }();
+  return sms;
+}
+
+unsigned ic_grid(int64_t n) {
+  int64_t g = (n + kIcFlat - 1) / kIcFlat;
+  const int64_t cap = (int64_t)ic_sms() * 16;
+  if (g > cap) g = cap;
+  return (unsigned)(g > 0 ? g : 1);
+}
+
+#define IC_FOR(i, n) \
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+// ------------------------------------------------------------------ members
+// Sort key of a vertex: its community, or C for a vertex without entries
+// (those sort after every member and take no list positions).
+__global__ void ic_member_keys_kernel(int32_t V, const int64_t* off, const uint8_t* has_loop, const int32_t* part,
+                                      int32_t C, uint64_t* key, float* val, uint32_t* loops) {
+  IC_FOR(i, V) {
+    const int64_t rl = off[i + 1] - off[i] + has_loop[i];
+    key[i] = rl > 0 ? (uint64_t)(uint32_t)part[i] : (uint64_t)(uint32_t)C;
+    val[i] = __int_as_float((int32_t)i);
+    loops[i] = has_loop[i];
+  }
+}
+
+// Members in community order: vertex, community, row length; nz = members
+// with entries (written by the last of them).
+__global__ void ic_member_len_kernel(int32_t V, const uint64_t* skey, const float* sval, const int64_t* off,
+                                     const uint8_t* has_loop, int32_t C, int32_t* mem, int32_t* mcomm,
+                                     int64_t* mlen, int32_t* nz) {
+  IC_FOR(i, V) {
+    const int32_t u = __float_as_int(sval[i]);
+    const int32_t c = (int32_t)skey[i];
+    mem[i] = u;
+    mcomm[i] = c;
+    const bool has = c < C;
+    mlen[i] = has ? off[u + 1] - off[u] + has_loop[u] : 0;
+    if (has && (i + 1 == V || (int32_t)skey[i + 1] >= C)) *nz = (int32_t)(i + 1);
+  }
+}
+
+// cfirst[c] = the member whose positions hold chunk c's first position.
+__global__ void ic_chunk_first_kernel(const int64_t* mscan, const int32_t* nzp, int32_t* cfirst, int64_t nchunks) {
+  const int32_t nz = *nzp;
+  IC_FOR(i, nz) {
+    const int64_t s = mscan[i], e = mscan[i + 1];
+    const int64_t c0 = (s + kIcChunk - 1) / kIcChunk, c1 = (e + kIcChunk - 1) / kIcChunk;
+    for (int64_t c = c0; c < c1; ++c) cfirst[c] = (int32_t)i;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cfirst[nchunks] = nz;
+}
+
+// ------------------------------------------------------------------ chunks
+struct IcSmem {
+  union {
+    uint64_t key[kIcChunk];          // sort keys (from the first ranking on)
+    uint32_t mark[kIcChunk];         // per position: (local segment << 13) | member (gather)
+  } a;
+  union {
+    struct {
+      float val[kIcChunk];
+      uint32_t wc[kIcWarps][kIcRadix + 1];
+      uint32_t dstart[kIcRadix];
+    } s;
+    int64_t ebase[kIcChunk + 1];     // per member: list index minus list position (gather)
+  } b;
+  int32_t loc_a[kIcChunk + 1];       // community of each local segment
+  uint32_t locfirst[kIcChunk + 2];   // first run of each local segment, then the run count
+  uint32_t wmax[kIcWarps];
+  uint32_t wflag[kIcWarps];
+  double wsum[kIcWarps];
+  uint32_t nloc, openL, openR;
+};
+
+// Exclusive max-scan of one value per thread over the 512-thread block.
+__device__ __forceinline__ uint32_t ic_block_excl_max(uint32_t v, uint32_t* wmax) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t u = __shfl_up_sync(full, inc, o);
+    if (lane >= o) inc = max(inc, u);
+  }
+  if (lane == 31) wmax[w] = inc;
+  __syncthreads();
+  uint32_t pre = 0;
+  for (int ww = 0; ww < w; ++ww) pre = max(pre, wmax[ww]);
+  uint32_t ex = __shfl_up_sync(full, inc, 1);
+  if (lane == 0) ex = 0;
+  __syncthreads();
+  return max(pre, ex);
+}
+
+// Exclusive segmented scan over the block of (f, s) pairs: f says a run
+// starts inside the thread's items, s is the sum of the thread's items after
+// its last run start (all of them when f is 0).  The result is the sum of
+// the run open at the thread's first item, over the earlier threads' items.
+// Combine: (f1, s1) then (f2, s2) -> (f1 | f2, f2 ? s2 : s1 + s2), applied in
+// a fixed tree, so the additions do not depend on timing.
+__device__ __forceinline__ double ic_block_seg_carry(uint32_t f, double s, uint32_t* wflag, double* wsum) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t fi = f;
+  double si = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t fu = __shfl_up_sync(full, fi, o);
+    const double su = __shfl_up_sync(full, si, o);
+    if (lane >= o) {
+      si = fi ? si : __dadd_rn(su, si);
+      fi |= fu;
+    }
+  }
+  if (lane == 31) { wflag[w] = fi; wsum[w] = si; }
+  __syncthreads();
+  // prefix of the earlier warps, left to right
+  double ps = 0.0;
+  for (int ww = 0; ww < w; ++ww) ps = wflag[ww] ? wsum[ww] : __dadd_rn(ps, wsum[ww]);
+  uint32_t fe = __shfl_up_sync(full, fi, 1);
+  double se = __shfl_up_sync(full, si, 1);
+  if (lane == 0) { fe = 0; se = 0.0; }
+  __syncthreads();
+  return fe ? se : __dadd_rn(ps, se);
+}
+
+// One chunk of kIcChunk list positions (see the file comment).  Writes its
+// runs (sorted by (local segment, cv), one per distinct key) at tkey/tsum
+// [p0, p0 + runs); for each segment that lies inside the chunk, its run count
+// and first run; and the chunk's summary (runs, runs of the segment open to
+// the left / right, flags, community of the last segment).
+__global__ void __launch_bounds__(kIcThreads, 2) ic_chunk_kernel(
+    int64_t E, int64_t nchunks, int Bb, const int32_t* mem, const int32_t* mcomm, const int64_t* mscan,
+    const int32_t* cfirst, const int64_t* off, const uint32_t* lscan, const int32_t* ldst, const float* lw,
+    const int32_t* part, uint64_t* tkey, double* tsum, uint32_t* dcount, uint32_t* firstrun, uint32_t* c_runs,
+    uint32_t* c_nl, uint32_t* c_nr, uint32_t* c_flags, int32_t* c_ar) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  IcSmem& S = *reinterpret_cast<IcSmem*>(smem_raw);
+  const unsigned full = 0xffffffffu;
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  const int64_t j = blockIdx.x;
+  const int64_t p0 = j * kIcChunk;
+  const int n = (int)(E - p0 < kIcChunk ? E - p0 : (int64_t)kIcChunk);
+  const int64_t p1 = p0 + n;
+  const int32_t i0 = cfirst[j];
+  const int32_t ihi = j + 1 < nchunks ? cfirst[j + 1] : cfirst[nchunks] - 1;
+  const int m = ihi - i0;   // candidate members after i0 (each starts in (p0, p1])
+
+  for (int q = t; q < kIcChunk; q += kIcThreads) S.a.mark[q] = 0u;
+  if (t == 0) {
+    const int32_t u0 = mem[i0];
+    S.b.ebase[0] = off[u0] + (int64_t)lscan[u0] - mscan[i0];
+    S.loc_a[0] = mcomm[i0];
+  }
+  __syncthreads();
+  // members: local segment index by a scan of community changes
+  {
+    uint32_t heads = 0;
+    int32_t cm[kIcItems];
+    bool hd[kIcItems];
+#pragma unroll
+    for (int jj = 0; jj < kIcItems; ++jj) {
+      const int r = 1 + t * kIcItems + jj;
+      hd[jj] = false;
+      cm[jj] = 0;
+      if (r <= m) {
+        const int32_t i = i0 + r;
+        cm[jj] = mcomm[i];
+        hd[jj] = mscan[i] < p1 && cm[jj] != mcomm[i - 1];
+        heads += hd[jj];
+      }
+    }
+    uint32_t tot;
+    uint32_t loc = block_exclusive_scan512<uint32_t>(heads, &tot);
+#pragma unroll
+    for (int jj = 0; jj < kIcItems; ++jj) {
+      const int r = 1 + t * kIcItems + jj;
+      if (r <= m) {
+        const int32_t i = i0 + r;
+        const int64_t st = mscan[i];
+        loc += hd[jj];
+        if (st < p1) {
+          const int32_t u = mem[i];
+          S.a.mark[st - p0] = (loc << kIcRelBits) | (uint32_t)r;
+          S.b.ebase[r] = off[u] + (int64_t)lscan[u] - st;
+          if (hd[jj]) S.loc_a[loc] = cm[jj];
+        }
+      }
+    }
+    if (t == 0) S.nloc = tot + 1;
+  }
+  __syncthreads();
+  // each position's member: inclusive max-scan of the marks (both fields grow)
+  {
+    uint32_t v[kIcItems];
+    uint32_t run = 0;
+#pragma unroll
+    for (int jj = 0; jj < kIcItems; ++jj) {
+      run = max(run, S.a.mark[t * kIcItems + jj]);
+      v[jj] = run;
+    }
+    const uint32_t pre = ic_block_excl_max(run, S.wmax);
+#pragma unroll
+    for (int jj = 0; jj < kIcItems; ++jj) S.a.mark[t * kIcItems + jj] = max(pre, v[jj]);
+  }
+  const uint32_t nloc = S.nloc;
+  if (t == 0) {
+    const int32_t cl = mscan[i0] < p0 ? mcomm[i0] : (p0 > 0 ? mcomm[i0 - 1] : -1);
+    S.openL = p0 > 0 && cl == S.loc_a[0];
+    S.openR = p1 < E && mcomm[cfirst[j + 1]] == S.loc_a[nloc - 1];
+  }
+  __syncthreads();
+  // gather (warp-striped positions: q = w*256 + jj*32 + lane)
+  uint64_t k[kIcItems];
+  float x[kIcItems];
+  const uint64_t bmask = (Bb >= 64) ? ~0ull : ((1ull << Bb) - 1ull);
+#pragma unroll
+  for (int jj = 0; jj < kIcItems; ++jj) {
+    const int q = w * (32 * kIcItems) + jj * 32 + lane;
+    k[jj] = ~0ull;
+    x[jj] = 0.0f;
+    if (q < n) {
+      const uint32_t pk = S.a.mark[q];
+      const int64_t e = S.b.ebase[pk & kIcRelMask] + p0 + q;
+      const int32_t v = __ldg(ldst + e);
+      const float wv = __ldg(lw + e);
+      const uint32_t b = (uint32_t)__ldg(part + v);
+      k[jj] = ((uint64_t)(pk >> kIcRelBits) << Bb) | b;
+      x[jj] = wv == 0.0f ? 1.0f : wv;     // InducedGraphKernel.cu:38-39
+    }
+  }
+  __syncthreads();
+  // stable LSD passes over the bits in use; items past n carry all-ones keys
+  // and stay behind every real item
+  int lb = 0;
+  while ((1u << lb) < nloc) ++lb;
+  const int bits = Bb + lb;
+  const int npass = (bits + 7) / 8;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int p = 0; p < npass; ++p) {
+    const int shift = 8 * p;
+    for (int i = t; i < kIcWarps * (kIcRadix + 1); i += kIcThreads) (&S.b.s.wc[0][0])[i] = 0u;
+    __syncthreads();
+    uint32_t rank[kIcItems];
+#pragma unroll
+    for (int jj = 0; jj < kIcItems; ++jj) {
+      const unsigned d = (unsigned)(k[jj] >> shift) & (kIcRadix - 1);
+      const unsigned peers = __match_any_sync(full, d);
+      const uint32_t before = S.b.s.wc[w][d];
+      rank[jj] = before + __popc(peers & lt);
+      __syncwarp();
+      if ((peers & lt) == 0) S.b.s.wc[w][d] = before + __popc(peers);
+      __syncwarp();
+    }
+    __syncthreads();
+    uint32_t cnt = 0;
+    if (t < kIcRadix) {
+#pragma unroll
+      for (int ww = 0; ww < kIcWarps; ++ww) {
+        const uint32_t c = S.b.s.wc[ww][t];
+        S.b.s.wc[ww][t] = cnt;
+        cnt += c;
+      }
+    }
+    uint32_t tot;
+    const uint32_t st = block_exclusive_scan512<uint32_t>(t < kIcRadix ? cnt : 0u, &tot);
+    if (t < kIcRadix) S.b.s.dstart[t] = st;
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < kIcItems; ++jj) {
+      const unsigned d = (unsigned)(k[jj] >> shift) & (kIcRadix - 1);
+      const uint32_t pos = S.b.s.dstart[d] + S.b.s.wc[w][d] + rank[jj];
+      S.a.key[pos] = k[jj];
+      S.b.s.val[pos] = x[jj];
+    }
+    __syncthreads();
+    if (p + 1 < npass) {
+#pragma unroll
+      for (int jj = 0; jj < kIcItems; ++jj) {
+        const int q = w * (32 * kIcItems) + jj * 32 + lane;
+        k[jj] = S.a.key[q];
+        x[jj] = S.b.s.val[q];
+      }
+    }
+  }
+  if (npass == 0) {
+#pragma unroll
+    for (int jj = 0; jj < kIcItems; ++jj) {
+      const int q = w * (32 * kIcItems) + jj * 32 + lane;
+      S.a.key[q] = k[jj];
+      S.b.s.val[q] = x[jj];
+    }
+    __syncthreads();
+  }
+  // runs of equal keys (blocked positions q = t*8 + jj): count, carry, sums
+  uint32_t hc = 0, f = 0;
+  double sp = 0.0;
+#pragma unroll
+  for (int jj = 0; jj < kIcItems; ++jj) {
+    const int q = t * kIcItems + jj;
+    if (q < n) {
+      const uint64_t kk = S.a.key[q];
+      const float xv = S.b.s.val[q];
+      if (q == 0 || S.a.key[q - 1] != kk) {
+        f = 1u;
+        ++hc;
+        sp = (double)xv;
+      } else {
+        sp = __dadd_rn(sp, (double)xv);
+      }
+    }
+  }
+  uint32_t nruns;
+  const uint32_t hb = block_exclusive_scan512<uint32_t>(hc, &nruns);
+  double acc = ic_block_seg_carry(f, sp, S.wflag, S.wsum);
+  int64_t run = (int64_t)hb - 1;
+#pragma unroll
+  for (int jj = 0; jj < kIcItems; ++jj) {
+    const int q = t * kIcItems + jj;
+    if (q < n) {
+      const uint64_t kk = S.a.key[q];
+      const float xv = S.b.s.val[q];
+      const bool head = q == 0 || S.a.key[q - 1] != kk;
+      if (head) {
+        ++run;
+        acc = (double)xv;
+        if (q == 0 || (S.a.key[q - 1] >> Bb) != (kk >> Bb)) S.locfirst[kk >> Bb] = (uint32_t)run;
+      } else {
+        acc = __dadd_rn(acc, (double)xv);
+      }
+      if (q + 1 == n || S.a.key[q + 1] != kk) {
+        const int32_t a = S.loc_a[kk >> Bb];
+        tkey[p0 + run] = ((uint64_t)(uint32_t)a << 32) | (kk & bmask);
+        tsum[p0 + run] = acc;
+      }
+    }
+  }
+  if (t == 0) S.locfirst[nloc] = nruns;
+  __syncthreads();
+  const bool oL = S.openL != 0, oR = S.openR != 0;
+  for (uint32_t l = t; l < nloc; l += kIcThreads) {
+    const bool open = (l == 0 && oL) || (l + 1 == nloc && oR);
+    if (!open) {
+      const int32_t a = S.loc_a[l];
+      dcount[a] = S.locfirst[l + 1] - S.locfirst[l];
+      firstrun[a] = (uint32_t)p0 + S.locfirst[l];
+    }
+  }
+  if (t == 0) {
+    c_runs[j] = nruns;
+    c_nl[j] = oL ? S.locfirst[1] - S.locfirst[0] : 0u;
+    c_nr[j] = oR ? nruns - S.locfirst[nloc - 1] : 0u;
+    c_flags[j] = (oL ? kOpenL : 0u) | (oR ? kOpenR : 0u) | ((nloc == 1 && oL && oR) ? kSingle : 0u);
+    c_ar[j] = S.loc_a[nloc - 1];
+  }
+}
+
+// ------------------------------------------------------------------ open segments
+// Per chunk: does its last segment start a new open segment, and how many of
+// its runs belong to open segments.
+__global__ void ic_open_count_kernel(int64_t nchunks, const uint32_t* c_runs, const uint32_t* c_nl,
+                                     const uint32_t* c_nr, const uint32_t* c_flags, uint32_t* newr,
+                                     uint32_t* nopen) {
+  IC_FOR(j, nchunks) {
+    const uint32_t fl = c_flags[j];
+    const bool single = (fl & kSingle) != 0;
+    newr[j] = ((fl & kOpenR) && !single) ? 1u : 0u;
+    nopen[j] = single ? c_runs[j] : c_nl[j] + c_nr[j];
+  }
+}
+
+// The runs of open segments, keyed (open segment, cv), with their slot in
+// tkey/tsum as payload; oa = community of each open segment.  A warp per chunk.
+__global__ void ic_open_gather_kernel(int64_t nchunks, int Bb, const uint32_t* c_runs, const uint32_t* c_nl,
+                                      const uint32_t* c_nr, const uint32_t* c_flags, const int32_t* c_ar,
+                                      const uint32_t* newr_x, const uint32_t* nopen_x, const uint64_t* tkey,
+                                      uint64_t* okey, float* oval, int32_t* oa) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t bmask = (1ull << Bb) - 1ull;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x / 32);
+  for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32; j < nchunks; j += nw) {
+    const uint32_t o0 = nopen_x[j], no = nopen_x[j + 1] - o0;
+    if (no == 0) continue;
+    const uint32_t fl = c_flags[j], runs = c_runs[j], nl = c_nl[j], nr = c_nr[j];
+    const uint32_t nnew = newr_x[j + 1] - newr_x[j];
+    const uint32_t orank_l = newr_x[j] - 1u, orank_r = newr_x[j] + nnew - 1u;
+    if (lane == 0 && nnew) oa[orank_r] = c_ar[j];
+    for (uint32_t k = lane; k < no; k += 32) {
+      uint32_t r, orank;
+      if (fl & kSingle) { r = k; orank = orank_r; }
+      else if (k < nl) { r = k; orank = orank_l; }
+      else { r = runs - nr + (k - nl); orank = orank_r; }
+      const uint64_t tt = (uint64_t)j * kIcChunk + r;
+      okey[o0 + k] = ((uint64_t)orank << Bb) | (tkey[tt] & bmask);
+      oval[o0 + k] = __uint_as_float((uint32_t)tt);
+    }
+  }
+}
+
+__global__ void ic_head_kernel(const uint64_t* k, int64_t n, uint32_t* head) {
+  IC_FOR(i, n) head[i] = (i == 0 || k[i - 1] != k[i]) ? 1u : 0u;
+}
+
+// Sums of the open runs by distinct (open segment, cv): lanes of a warp add
+// equal keys first, one FP64 atomic per key and warp.  ofirst[o] = distinct
+// rank of open segment o's first key.  Grid covers n in whole warps.
+__global__ void ic_open_sum_kernel(const uint64_t* k, const float* v, int64_t n, int Bb, const uint32_t* pos,
+                                   const uint32_t* head, const double* tsum, double* osum, uint32_t* ofirst,
+                                   uint32_t n_open) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool valid = i < n;
+  const int64_t g = valid ? (int64_t)pos[i] + (int64_t)head[i] - 1 : -1;
+  double x = valid ? tsum[__float_as_uint(v[i])] : 0.0;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double u = __shfl_up_sync(full, x, o);
+    const int64_t gu = __shfl_up_sync(full, g, o);
+    if (lane >= o && gu == g) x = __dadd_rn(x, u);
+  }
+  const int64_t gn = __shfl_down_sync(full, g, 1);
+  const bool vn = __shfl_down_sync(full, valid, 1);
+  if (valid && (lane == 31 || !vn || gn != g)) atomicAdd(&osum[g], x);
+  if (valid) {
+    const uint64_t o = k[i] >> Bb;
+    if (i == 0 || (k[i - 1] >> Bb) != o) ofirst[o] = (uint32_t)g;
+    if (i + 1 == n) ofirst[n_open] = (uint32_t)g + 1u;
+  }
+}
+
+__global__ void ic_open_dcount_kernel(uint32_t n_open, const uint32_t* ofirst, const int32_t* oa, uint32_t* dcount) {
+  IC_FOR(o, (int64_t)n_open) dcount[oa[o]] = ofirst[o + 1] - ofirst[o];
+}
+
+// ------------------------------------------------------------------ placement
+// Runs of the segments inside one chunk, to their final slots.  A block per chunk.
+__global__ void ic_final_closed_kernel(const uint32_t* c_runs, const uint32_t* c_nl, const uint32_t* c_nr,
+                                       const uint32_t* c_flags, const uint64_t* tkey, const double* tsum,
+                                       const uint32_t* segoff, const uint32_t* firstrun, int32_t* osrc,
+                                       int32_t* odst, float* ow) {
+  const int64_t j = blockIdx.x;
+  if (c_flags[j] & kSingle) return;
+  const uint32_t lo = c_nl[j], hi = c_runs[j] - c_nr[j];
+  for (uint32_t r = lo + threadIdx.x; r < hi; r += blockDim.x) {
+    const uint64_t tt = (uint64_t)j * kIcChunk + r;
+    const uint64_t kk = tkey[tt];
+    const int32_t a = (int32_t)(kk >> 32);
+    const uint64_t p = (uint64_t)segoff[a] + (tt - firstrun[a]);
+    osrc[p] = a;
+    odst[p] = (int32_t)(uint32_t)kk;
+    ow[p] = __double2float_rn(tsum[tt]);
+  }
+}
+
+// Distinct keys of the open segments, to their final slots.
+__global__ void ic_final_open_kernel(const uint64_t* k, int64_t n, int Bb, const uint32_t* pos,
+                                     const uint32_t* head, const uint32_t* ofirst, const int32_t* oa,
+                                     const uint32_t* segoff, const double* osum, int32_t* osrc, int32_t* odst,
+                                     float* ow) {
+  const uint64_t bmask = (1ull << Bb) - 1ull;
+  IC_FOR(i, n) {
+    if (!head[i]) continue;
+    const uint32_t g = pos[i];
+    const uint64_t kk = k[i];
+    const uint32_t o = (uint32_t)(kk >> Bb);
+    const int32_t a = oa[o];
+    const uint64_t p = (uint64_t)segoff[a] + (g - ofirst[o]);
+    osrc[p] = a;
+    odst[p] = (int32_t)(kk & bmask);
+    ow[p] = __double2float_rn(osum[g]);
+  }
+}
+
+// Bytes of scratch induce_sorted may take, at most (the open runs can be all
+// runs in the worst case).
+size_t induce_sorted_scratch(int64_t V, int64_t E, int64_t C) {
+  const int64_t nchunks = (E + kIcChunk - 1) / kIcChunk;
+  const int64_t slots = nchunks * kIcChunk;
+  size_t b = 0;
+  b += (size_t)V * (2 * 12 + 4 + 4 + 4 + 8) + 8 * 256 * (size_t)(V / 4096 + 2);   // member sort, scans
+  b += (size_t)slots * 16 + (size_t)nchunks * 28 + (size_t)C * 12;              // runs, chunk facts, counts
+  b += (size_t)E * (2 * 12 + 4 + 4 + 8 + 4) + 8 * 256 * (size_t)(E / 4096 + 2); // open runs, worst case
+  return b + ((size_t)64 << 10) * 32;                                            // alignment slack
+}
+
+void ic_attributes() {
+  constexpr int kDevs = 64;
+  static std::mutex mu;
+  static bool done[kDevs] = {};
+  int dev = 0;
+  LVG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < kDevs && done[dev]) return;
+  LVG_CUDA(cudaFuncSetAttribute(ic_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(IcSmem)));
+  if (dev >= 0 && dev < kDevs) done[dev] = true;
+}
+
+template <typename T>
+T read_back(const T* d, cudaStream_t s) {
+  T h{};
+  LVG_CUDA(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+}  // namespace
+
+bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t* osrc, int32_t* odst, float* ow,
+                   int64_t* count, Arena& a, cudaStream_t s) {
+  const int32_t V = g.V;
+  const int64_t E = g.E;
+  if (!g.sorted_symmetric || V <= 0 || C <= 0) return false;
+  if (E + 2 * (int64_t)kIcChunk >= ((int64_t)1 << 32)) return false;   // slots and counts are 32-bit
+  if (a.hi < a.lo || a.hi - a.lo < induce_sorted_scratch(V, E, C)) return false;
+  if (E == 0) { *count = 0; return true; }
+  HiScope hs(a);
+  const int64_t nchunks = (E + kIcChunk - 1) / kIcChunk;
+  const int Bb = bits_for(C);
+  // members in community order (stable: vertex order inside a community)
+  uint64_t* mk0 = a.hi_n<uint64_t>(V);
+  float* mv0 = a.hi_n<float>(V);
+  uint64_t* mk1 = a.hi_n<uint64_t>(V);
+  float* mv1 = a.hi_n<float>(V);
+  uint32_t* lscan = a.hi_n<uint32_t>(V + 1);
+  ic_member_keys_kernel<<<ic_grid(V), kIcFlat, 0, s>>>(V, g.off, g.has_loop, part, C, mk0, mv0, lscan);
+  LVG_LAUNCH();
+  const int which = radix_sort_pairs(mk0, mv0, mk1, mv1, V, bits_for((int64_t)C + 1), a, s);
+  scan_u32(lscan, lscan, V, a, s);   // self loops before each vertex: list row start = off + lscan
+  int32_t* mem = a.hi_n<int32_t>(V);
+  int32_t* mcomm = a.hi_n<int32_t>(V);
+  int64_t* mscan = a.hi_n<int64_t>(V + 1);
+  int32_t* nz = a.hi_n<int32_t>(1);
+  LVG_CUDA(cudaMemsetAsync(nz, 0, sizeof(int32_t), s));
+  ic_member_len_kernel<<<ic_grid(V), kIcFlat, 0, s>>>(V, which ? mk1 : mk0, which ? mv1 : mv0, g.off, g.has_loop,
+                                                      C, mem, mcomm, mscan, nz);
+  LVG_LAUNCH();
+  scan_i64(mscan, mscan, V, a, s);
+  if (read_back(mscan + V, s) != E) throw Error(LVG_ERR_CUDA, "coarsening: list rows disagree with the CSR");
+  int32_t* cfirst = a.hi_n<int32_t>(nchunks + 1);
+  ic_chunk_first_kernel<<<ic_grid(V), kIcFlat, 0, s>>>(mscan, nz, cfirst, nchunks);
+  LVG_LAUNCH();
+  // chunks
+  uint64_t* tkey = a.hi_n<uint64_t>(nchunks * kIcChunk);
+  double* tsum = a.hi_n<double>(nchunks * kIcChunk);
+  uint32_t* dcount = a.hi_n<uint32_t>((int64_t)C + 1);
+  uint32_t* firstrun = a.hi_n<uint32_t>(C);
+  uint32_t* c_runs = a.hi_n<uint32_t>(nchunks);
+  uint32_t* c_nl = a.hi_n<uint32_t>(nchunks);
+  uint32_t* c_nr = a.hi_n<uint32_t>(nchunks);
+  uint32_t* c_flags = a.hi_n<uint32_t>(nchunks);
+  int32_t* c_ar = a.hi_n<int32_t>(nchunks);
+  LVG_CUDA(cudaMemsetAsync(dcount, 0, sizeof(uint32_t) * ((size_t)C + 1), s));
+  ic_attributes();
+  ic_chunk_kernel<<<(unsigned)nchunks, kIcThreads, sizeof(IcSmem), s>>>(
+      E, nchunks, Bb, mem, mcomm, mscan, cfirst, g.off, lscan, g.dst, g.w, part, tkey, tsum, dcount, firstrun,
+      c_runs, c_nl, c_nr, c_flags, c_ar);
+  LVG_LAUNCH();
+  // segments open across chunk boundaries
+  uint32_t* newr = a.hi_n<uint32_t>(nchunks + 1);
+  uint32_t* nopen = a.hi_n<uint32_t>(nchunks + 1);
+  ic_open_count_kernel<<<ic_grid(nchunks), kIcFlat, 0, s>>>(nchunks, c_runs, c_nl, c_nr, c_flags, newr, nopen);
+  LVG_LAUNCH();
+  scan_u32(newr, newr, nchunks, a, s);
+  scan_u32(nopen, nopen, nchunks, a, s);
+  const uint32_t n_open = read_back(newr + nchunks, s);
+  const int64_t n_orun = read_back(nopen + nchunks, s);
+  uint64_t* okeys = nullptr;
+  uint32_t *ohead = nullptr, *opos = nullptr, *ofirst = nullptr;
+  int32_t* oa = nullptr;
+  double* osum = nullptr;
+  if (n_orun > 0) {
+    uint64_t* ok0 = a.hi_n<uint64_t>(n_orun);
+    float* ov0 = a.hi_n<float>(n_orun);
+    uint64_t* ok1 = a.hi_n<uint64_t>(n_orun);
+    float* ov1 = a.hi_n<float>(n_orun);
+    oa = a.hi_n<int32_t>(n_open);
+    ic_open_gather_kernel<<<ic_grid(nchunks * 32), kIcFlat, 0, s>>>(nchunks, Bb, c_runs, c_nl, c_nr, c_flags, c_ar,
+                                                                     newr, nopen, tkey, ok0, ov0, oa);
+    LVG_LAUNCH();
+    const int w2 = radix_sort_pairs(ok0, ov0, ok1, ov1, n_orun, bits_for(n_open) + Bb, a, s);
+    okeys = w2 ? ok1 : ok0;
+    const float* ovals = w2 ? ov1 : ov0;
+    ohead = a.hi_n<uint32_t>(n_orun + 1);
+    opos = a.hi_n<uint32_t>(n_orun + 1);
+    ic_head_kernel<<<ic_grid(n_orun), kIcFlat, 0, s>>>(okeys, n_orun, ohead);
+    LVG_LAUNCH();
+    scan_u32(ohead, opos, n_orun, a, s);
+    const uint32_t n_odist = read_back(opos + n_orun, s);
+    osum = a.hi_n<double>(n_odist);
+    ofirst = a.hi_n<uint32_t>((int64_t)n_open + 1);
+    LVG_CUDA(cudaMemsetAsync(osum, 0, sizeof(double) * std::max<uint32_t>(n_odist, 1), s));
+    ic_open_sum_kernel<<<grid_for(n_orun, kIcFlat), kIcFlat, 0, s>>>(okeys, ovals, n_orun, Bb, opos, ohead, tsum,
+                                                                      osum, ofirst, n_open);
+    LVG_LAUNCH();
+    ic_open_dcount_kernel<<<ic_grid(n_open), kIcFlat, 0, s>>>(n_open, ofirst, oa, dcount);
+    LVG_LAUNCH();
+  }
+  // every community's first slot, then the entries
+  uint32_t* segoff = a.hi_n<uint32_t>((int64_t)C + 1);
+  scan_u32(dcount, segoff, C, a, s);
+  const int64_t cnt = read_back(segoff + C, s);
+  ic_final_closed_kernel<<<(unsigned)nchunks, kIcFlat, 0, s>>>(c_runs, c_nl, c_nr, c_flags, tkey, tsum, segoff,
+                                                               firstrun, osrc, odst, ow);
+  LVG_LAUNCH();
+  if (n_orun > 0) {
+    ic_final_open_kernel<<<ic_grid(n_orun), kIcFlat, 0, s>>>(okeys, n_orun, Bb, opos, ohead, ofirst, oa, segoff,
+                                                             osum, osrc, odst, ow);
+    LVG_LAUNCH();
+  }
+  LVG_CUDA(cudaStreamSynchronize(s));
+  *count = cnt;
+  return true;
+}
+
+}  // namespace lvg

@@ -2493,6 +2493,12 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
   int32_t* odst = a.hi_n<int32_t>(E);
   float* ow = a.hi_n<float>(E);
   int64_t cnt = 0;
+  if (induce_sorted(g, part, C, osrc, odst, ow, &cnt, a, s)) {
+    *out_src = osrc;
+    *out_dst = odst;
+    *out_w = ow;
+    return cnt;
+  }
   {
     HiScope hs(a);
     const int B = std::max(1, bits_for(C));

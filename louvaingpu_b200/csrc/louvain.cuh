@@ -169,6 +169,13 @@ int32_t renumber(const LevelGraph& g, const int32_t* comm, int32_t* part, Arena&
 
 // Coarsen (InducedGraphKernel.cu:50-113): writes the next level input list to
 // high-end scratch and returns its size; out_* point into that scratch.
+// Coarsening of a strictly sorted, symmetric level list without a device-wide
+// sort of all its entries (induce.cu).  Writes the same list as the
+// sort-based path into osrc/odst/ow (capacity E) and its length into *count;
+// returns false, having done nothing, when the list is not in that form or
+// the arena lacks room.
+bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t* osrc, int32_t* odst, float* ow,
+                   int64_t* count, Arena& a, cudaStream_t s);
 int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** out_src, int32_t** out_dst,
                float** out_w, Arena& a, cudaStream_t s);
 
