@@ -230,11 +230,24 @@ class Louvain:
         self._check(self._L.lvg_get_level_labels(self._h, int(level), _p(out)))
         return out
 
-    def partition(self, level=-1):
+    def partition(self, level=-1, out=None):
+        """Community of every input vertex at `level` (default: the last).
+        `out`: optional destination -- an int32 numpy array of n_vertices, or
+        a host tensor (e.g. pinned torch memory, for a fast copy) exposing
+        data_ptr() and numel(); it is filled and returned."""
         if level < 0:
             level = self.n_levels - 1
-        out = np.zeros(self.n_vertices, np.int32)
-        self._check(self._L.lvg_get_partition(self._h, int(level), _p(out)))
+        if out is None:
+            out = np.zeros(self.n_vertices, np.int32)
+        if hasattr(out, "data_ptr"):
+            if out.numel() != self.n_vertices or out.element_size() != 4:
+                raise ValueError("out must hold n_vertices int32 values")
+            ptr = ctypes.c_void_p(out.data_ptr())
+        else:
+            if out.dtype != np.int32 or out.size != self.n_vertices or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous int32 array of n_vertices")
+            ptr = _p(out)
+        self._check(self._L.lvg_get_partition(self._h, int(level), ptr))
         return out
 
     def modularity_fp64(self, part):

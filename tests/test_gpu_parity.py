@@ -401,3 +401,24 @@ def test_run_after_steps_matches_a_fresh_run(Louvain, oracle, gen):
         lv.renumber()
         res = lv.run()
         run_equal(lv, res, orun, n, s, d, w, oracle)
+
+
+def test_partition_into_caller_buffers(Louvain, gen):
+    """partition(out=...) fills a numpy array or a pinned host tensor with the
+    same labels as partition(); a buffer of the wrong size or type is refused."""
+    import torch
+    n, s, d, w = make_case(gen, "weighted")
+    with Louvain() as lv:
+        lv.load_edges(s, d, w, n)
+        lv.run()
+        ref = lv.partition()
+        a = np.full(n, -1, np.int32)
+        assert lv.partition(out=a) is a
+        np.testing.assert_array_equal(a, ref)
+        t = torch.full((n,), -1, dtype=torch.int32).pin_memory()
+        lv.partition(out=t)
+        np.testing.assert_array_equal(t.numpy(), ref)
+        with pytest.raises(ValueError):
+            lv.partition(out=np.zeros(n - 1, np.int32))
+        with pytest.raises(ValueError):
+            lv.partition(out=np.zeros(n, np.int64))
