@@ -56,6 +56,10 @@ typedef struct {
   int32_t passes_per_sync; /* passes launched between host checks of convergence (0: default) */
   int32_t use_graphs;      /* replay each pass from CUDA graphs captured once per level (1: on) */
   int32_t l2_persist;      /* keep the gathered community arrays in an L2 persisting window (1: on) */
+  int64_t load_chunk_entries; /* lvg_load_edges: the host list is copied in chunks of this many entries
+                              * while the level-0 CSR is built from the chunks already on the device
+                              * (0: 2^25; rounded up to a multiple of 2048; lists of fewer than two
+                              * chunks are copied whole, then built) */
 } lvg_config;
 
 /* Per-level record of a run (the reference keeps one Partition per level,

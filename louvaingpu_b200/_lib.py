@@ -36,6 +36,7 @@ class LvgConfig(ctypes.Structure):
         ("passes_per_sync", ctypes.c_int32),
         ("use_graphs", ctypes.c_int32),
         ("l2_persist", ctypes.c_int32),
+        ("load_chunk_entries", ctypes.c_int64),
     ]
 
 

@@ -80,6 +80,9 @@ struct lvg_ctx {
   double move_ms = 0.0;
   int64_t move_passes = 0;
   std::vector<float> move_pass_ms;  // move kernels of each pass of the last one-level phase
+  PreCsr pre0;                    // level-0 CSR built during a chunked host upload
+  cudaStream_t copy_stream = nullptr;   // host-list upload chunks (lvg_load_edges)
+  std::vector<cudaEvent_t> load_ev;     // one per upload chunk
 };
 
 namespace {
@@ -186,6 +189,7 @@ void load_common(lvg_ctx* c, const int32_t* d_src, const int32_t* d_dst, const f
   c->g.src = d_src;
   c->g.dst = d_dst;
   c->g.w = d_w;
+  c->g.pre = &c->pre0;
   prepare_level(c);
   c->symmetric0 = c->g.sorted_symmetric;
   c->loaded = true;
@@ -208,6 +212,7 @@ void reset_to_level0(lvg_ctx* c) {
   c->g.src = c->src0;
   c->g.dst = c->dst0;
   c->g.w = c->w0;
+  c->g.pre = &c->pre0;
   prepare_level(c);
   c->pristine = true;
 }
@@ -486,6 +491,8 @@ lvg_status lvg_destroy(lvg_ctx* c) {
     }
     cudaEventDestroy(c->side.fork);
   }
+  for (cudaEvent_t e : c->load_ev) cudaEventDestroy(e);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return LVG_OK;
@@ -507,18 +514,28 @@ lvg_status lvg_load_edges(lvg_ctx* c, const int32_t* src, const int32_t* dst, co
     require(V >= 0 && E >= 0, LVG_ERR_INVALID_ARG, "negative size");
     require(E == 0 || (src && dst && w), LVG_ERR_INVALID_ARG, "null edge array");
     c->loaded = false;
+    c->pre0 = PreCsr();
     size_t need = c->cfg.arena_bytes > 0 ? (size_t)c->cfg.arena_bytes : arena_estimate(V, E, true);
     c->arena.reserve(need);
     int32_t* s = c->arena.lo_n<int32_t>(E);
     int32_t* d = c->arena.lo_n<int32_t>(E);
     float* ww = c->arena.lo_n<float>(E);
-    if (E > 0) {
-      LVG_CUDA(cudaMemcpyAsync(s, src, sizeof(int32_t) * E, cudaMemcpyHostToDevice, c->stream));
-      LVG_CUDA(cudaMemcpyAsync(d, dst, sizeof(int32_t) * E, cudaMemcpyHostToDevice, c->stream));
-      LVG_CUDA(cudaMemcpyAsync(ww, w, sizeof(float) * E, cudaMemcpyHostToDevice, c->stream));
+    int64_t chunk = c->cfg.load_chunk_entries > 0 ? c->cfg.load_chunk_entries : ((int64_t)1 << 25);
+    chunk = (chunk + 2047) / 2048 * 2048;
+    bool ok;
+    if (E >= 2 * chunk) {   // copy in chunks, checking and building level 0 as they arrive
+      if (!c->copy_stream) LVG_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+      ok = stream_load_level0(src, dst, w, s, d, ww, E, V, chunk, c->pre0, c->load_ev, c->arena, c->stream,
+                              c->copy_stream);
+    } else {
+      if (E > 0) {
+        LVG_CUDA(cudaMemcpyAsync(s, src, sizeof(int32_t) * E, cudaMemcpyHostToDevice, c->stream));
+        LVG_CUDA(cudaMemcpyAsync(d, dst, sizeof(int32_t) * E, cudaMemcpyHostToDevice, c->stream));
+        LVG_CUDA(cudaMemcpyAsync(ww, w, sizeof(float) * E, cudaMemcpyHostToDevice, c->stream));
+      }
+      ok = validate_edges(s, d, ww, E, V, c->arena, c->stream);
     }
-    require(validate_edges(s, d, ww, E, V, c->arena, c->stream), LVG_ERR_INVALID_ARG,
-            "edge list has a vertex id out of range or a negative / non-finite weight");
+    require(ok, LVG_ERR_INVALID_ARG, "edge list has a vertex id out of range or a negative / non-finite weight");
     load_common(c, s, d, ww, E, V);
   });
 }
@@ -530,6 +547,7 @@ lvg_status lvg_load_edges_device(lvg_ctx* c, const int32_t* src, const int32_t* 
     require(V >= 0 && E >= 0, LVG_ERR_INVALID_ARG, "negative size");
     require(E == 0 || (src && dst && w), LVG_ERR_INVALID_ARG, "null edge array");
     c->loaded = false;
+    c->pre0 = PreCsr();
     size_t need = c->cfg.arena_bytes > 0 ? (size_t)c->cfg.arena_bytes : arena_estimate(V, E, false);
     c->arena.reserve(need);
     require(validate_edges(src, dst, w, E, V, c->arena, c->stream), LVG_ERR_INVALID_ARG,
@@ -1055,6 +1073,7 @@ void batch_run(lvg_ctx* c, const BatchInput& in, int32_t* part_out, double* q_ou
   }
   require(E0 < ((int64_t)1 << 31), LVG_ERR_CAPACITY, "a batch may hold at most 2^31-1 entries");
   drop_graphs(c);
+  c->pre0 = PreCsr();   // the batch reuses the arena
   c->loaded = false;
   c->have_state = false;
   size_t need = c->cfg.arena_bytes > 0 ? (size_t)c->cfg.arena_bytes

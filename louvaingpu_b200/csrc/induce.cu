@@ -10,7 +10,8 @@
 // member order, form that community's segment -- entries already grouped by
 // cu, at positions known from a scan of the row lengths.  The position range
 // is cut into chunks of 4096 entries.  A 512-thread block takes a chunk:
-// it gathers cv = part[dst] for its entries, sorts (segment, cv) keys in
+// it reads cv = part[dst] of its entries (gathered once in list order by a
+// streaming kernel), sorts (segment, cv) keys in
 // shared memory (stable 8-bit LSD passes over only the bits the chunk needs),
 // and sums equal keys in a fixed order.  A segment that lies inside one chunk
 // is then final.  Segments that cross a chunk boundary (the large
@@ -19,10 +20,17 @@
 // radix sort, keyed by (open segment, cv), and are summed again.  A scan of
 // the distinct counts of every community places each community's entries.
 //
+// A chunk that lies inside one segment continuing on both sides sends all its
+// runs on, so it sums equal cv in a shared-memory hash table instead of
+// sorting them.
+//
 // Output: the same list as the sort-based path (entries ordered by (cu, cv),
-// weights 0 counted as 1, sums in FP64 rounded once to float).  Sums of equal
-// keys run in a fixed order that does not depend on timing.
+// weights 0 counted as 1, sums in FP64 rounded once to float).  Sums inside a
+// sorted chunk run in a fixed order; the hash tables and the sums across
+// chunks use FP64 atomics, whose order does not matter for integer weights
+// (every partial sum is exact).
 #include <algorithm>
+#include <cstddef>
 #include <mutex>
 
 #include "louvain.cuh"
@@ -89,6 +97,13 @@ __global__ void ic_member_len_kernel(int32_t V, const uint64_t* skey, const floa
     mlen[i] = has ? off[u + 1] - off[u] + has_loop[u] : 0;
     if (has && (i + 1 == V || (int32_t)skey[i + 1] >= C)) *nz = (int32_t)(i + 1);
   }
+}
+
+// cv of every list entry, in list order: the one random gather of the
+// coarsening, made by a streaming kernel (many loads in flight per SM) so
+// that the chunk kernel reads cv coalesced along the rows.
+__global__ void ic_cv_kernel(const int32_t* ldst, const int32_t* part, int64_t E, int32_t* cvl) {
+  IC_FOR(e, E) cvl[e] = __ldg(part + __ldg(ldst + e));
 }
 
 // cfirst[c] = the member whose positions hold chunk c's first position.
@@ -176,6 +191,79 @@ __device__ __forceinline__ double ic_block_seg_carry(uint32_t f, double s, uint3
   return fe ? se : __dadd_rn(ps, se);
 }
 
+// Hash-table reduction of a chunk inside one segment (items in registers,
+// keys = cv).  A table of 2 x kIcChunk slots over the shared memory of the
+// sort layout: keys 32-bit (empty = all ones; cv < 2^31), sums FP64.  Lanes
+// of a warp holding the same cv add first, then one shared atomic per cv.
+// Writes the distinct (community, cv) runs in table order at p0.., and
+// leaves the run count in S.nloc and the community in S.openL (after a
+// barrier) for the caller's chunk summary.
+constexpr int kIcHashSlots = 2 * kIcChunk;
+constexpr uint32_t kIcEmpty = 0xffffffffu;
+static_assert(sizeof(uint32_t) * kIcHashSlots + sizeof(double) * kIcHashSlots <=
+                  offsetof(IcSmem, wmax), "hash table fits below the block's scalars");
+
+__device__ __forceinline__ void ic_chunk_hash(IcSmem& S, unsigned char* raw, const uint64_t* k, const float* x,
+                                              int n, int64_t p0, uint64_t* tkey, double* tsum) {
+  const unsigned full = 0xffffffffu;
+  const int t = threadIdx.x, lane = t & 31;
+  const int32_t a0 = S.loc_a[0];
+  __syncthreads();   // the table overwrites the gather layout
+  uint32_t* hk = reinterpret_cast<uint32_t*>(raw);
+  double* hv = reinterpret_cast<double*>(raw + sizeof(uint32_t) * kIcHashSlots);
+  for (int i = t; i < kIcHashSlots; i += kIcThreads) {
+    hk[i] = kIcEmpty;
+    hv[i] = 0.0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int jj = 0; jj < kIcItems; ++jj) {
+    const uint32_t key = k[jj] == ~0ull ? kIcEmpty : (uint32_t)k[jj];
+    double v = (double)x[jj];
+    const unsigned peers = __match_any_sync(full, key);
+    if (__any_sync(full, __popc(peers) > 1)) {
+      double sum = 0.0;
+#pragma unroll
+      for (int l = 0; l < 32; ++l) {
+        const double u = __shfl_sync(full, v, l);
+        if ((peers >> l) & 1u) sum = __dadd_rn(sum, u);
+      }
+      v = sum;
+    }
+    if (key != kIcEmpty && lane == __ffs(peers) - 1) {
+      uint32_t slot = (key * 0x9E3779B1u) >> (32 - 13);
+      static_assert(kIcHashSlots == 1 << 13, "13-bit slots");
+      while (true) {
+        const uint32_t prev = atomicCAS(&hk[slot], kIcEmpty, key);
+        if (prev == kIcEmpty || prev == key) break;
+        slot = (slot + 1) & (kIcHashSlots - 1);
+      }
+      atomicAdd(&hv[slot], v);
+    }
+  }
+  __syncthreads();
+  constexpr int kPer = kIcHashSlots / kIcThreads;
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) cnt += hk[t * kPer + i] != kIcEmpty;
+  uint32_t tot;
+  uint32_t o = block_exclusive_scan512<uint32_t>(cnt, &tot);
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    const int slot = t * kPer + i;
+    if (hk[slot] != kIcEmpty) {
+      tkey[p0 + o] = ((uint64_t)(uint32_t)a0 << 32) | hk[slot];
+      tsum[p0 + o] = hv[slot];
+      ++o;
+    }
+  }
+  if (t == 0) {
+    S.nloc = tot;
+    S.openL = (uint32_t)a0;
+  }
+  __syncthreads();
+}
+
 // One chunk of kIcChunk list positions (see the file comment).  Writes its
 // runs (sorted by (local segment, cv), one per distinct key) at tkey/tsum
 // [p0, p0 + runs); for each segment that lies inside the chunk, its run count
@@ -183,8 +271,8 @@ __device__ __forceinline__ double ic_block_seg_carry(uint32_t f, double s, uint3
 // the left / right, flags, community of the last segment).
 __global__ void __launch_bounds__(kIcThreads, 2) ic_chunk_kernel(
     int64_t E, int64_t nchunks, int Bb, const int32_t* mem, const int32_t* mcomm, const int64_t* mscan,
-    const int32_t* cfirst, const int64_t* off, const uint32_t* lscan, const int32_t* ldst, const float* lw,
-    const int32_t* part, uint64_t* tkey, double* tsum, uint32_t* dcount, uint32_t* firstrun, uint32_t* c_runs,
+    const int32_t* cfirst, const int64_t* off, const uint32_t* lscan, const int32_t* cvl, const float* lw,
+    uint64_t* tkey, double* tsum, uint32_t* dcount, uint32_t* firstrun, uint32_t* c_runs,
     uint32_t* c_nl, uint32_t* c_nr, uint32_t* c_flags, int32_t* c_ar) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   IcSmem& S = *reinterpret_cast<IcSmem*>(smem_raw);
@@ -274,14 +362,28 @@ __global__ void __launch_bounds__(kIcThreads, 2) ic_chunk_kernel(
     if (q < n) {
       const uint32_t pk = S.a.mark[q];
       const int64_t e = S.b.ebase[pk & kIcRelMask] + p0 + q;
-      const int32_t v = __ldg(ldst + e);
+      const uint32_t b = (uint32_t)__ldg(cvl + e);
       const float wv = __ldg(lw + e);
-      const uint32_t b = (uint32_t)__ldg(part + v);
       k[jj] = ((uint64_t)(pk >> kIcRelBits) << Bb) | b;
       x[jj] = wv == 0.0f ? 1.0f : wv;     // InducedGraphKernel.cu:38-39
     }
   }
   __syncthreads();
+  if (nloc == 1 && S.openL && S.openR) {
+    // The chunk lies inside one segment that continues on both sides: its
+    // runs all go on to the device-wide sort, so they need no order here.
+    // Equal cv are summed in a shared-memory hash table instead of sorted.
+    ic_chunk_hash(S, smem_raw, k, x, n, p0, tkey, tsum);
+    if (t == 0) {
+      const uint32_t runs = S.nloc;   // set by ic_chunk_hash
+      c_runs[j] = runs;
+      c_nl[j] = runs;
+      c_nr[j] = runs;
+      c_flags[j] = kOpenL | kOpenR | kSingle;
+      c_ar[j] = S.openL;               // community, set by ic_chunk_hash
+    }
+    return;
+  }
   // stable LSD passes over the bits in use; items past n carry all-ones keys
   // and stay behind every real item
   int lb = 0;
@@ -531,7 +633,7 @@ size_t induce_sorted_scratch(int64_t V, int64_t E, int64_t C) {
   const int64_t slots = nchunks * kIcChunk;
   size_t b = 0;
   b += (size_t)V * (2 * 12 + 4 + 4 + 4 + 8) + 8 * 256 * (size_t)(V / 4096 + 2);   // member sort, scans
-  b += (size_t)slots * 16 + (size_t)nchunks * 28 + (size_t)C * 12;              // runs, chunk facts, counts
+  b += (size_t)E * 4 + (size_t)slots * 16 + (size_t)nchunks * 28 + (size_t)C * 12;   // cv, runs, chunk facts
   b += (size_t)E * (2 * 12 + 4 + 4 + 8 + 4) + 8 * 256 * (size_t)(E / 4096 + 2); // open runs, worst case
   return b + ((size_t)64 << 10) * 32;                                            // alignment slack
 }
@@ -604,9 +706,12 @@ bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t*
   int32_t* c_ar = a.hi_n<int32_t>(nchunks);
   LVG_CUDA(cudaMemsetAsync(dcount, 0, sizeof(uint32_t) * ((size_t)C + 1), s));
   ic_attributes();
+  int32_t* cvl = a.hi_n<int32_t>(E);
+  ic_cv_kernel<<<ic_grid(E), kIcFlat, 0, s>>>(g.dst, part, E, cvl);
+  LVG_LAUNCH();
   ic_chunk_kernel<<<(unsigned)nchunks, kIcThreads, sizeof(IcSmem), s>>>(
-      E, nchunks, Bb, mem, mcomm, mscan, cfirst, g.off, lscan, g.dst, g.w, part, tkey, tsum, dcount, firstrun,
-      c_runs, c_nl, c_nr, c_flags, c_ar);
+      E, nchunks, Bb, mem, mcomm, mscan, cfirst, g.off, lscan, cvl, g.w, tkey, tsum, dcount, firstrun, c_runs,
+      c_nl, c_nr, c_flags, c_ar);
   LVG_LAUNCH();
   // segments open across chunk boundaries
   uint32_t* newr = a.hi_n<uint32_t>(nchunks + 1);

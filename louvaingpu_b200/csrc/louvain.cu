@@ -157,7 +157,7 @@ __global__ void row_count_kernel(const int32_t* src, int64_t E, int64_t* rowcnt)
   if (seg_warp_last<int64_t>(u, valid)) atomicAdd((unsigned long long*)&rowcnt[u], (unsigned long long)n);
 }
 
-enum : uint32_t { kNotSorted = 1u, kNotSymmetric = 2u };
+enum : uint32_t { kNotSorted = 1u, kNotSymmetric = 2u, kBadEntry = 4u };
 
 // Sortedness (exact) and symmetry of the list in one coalesced pass.  The
 // symmetry test compares order-free fingerprints: the sums mod 2^64 of two
@@ -225,6 +225,101 @@ __global__ void csr_fast_emit_kernel(const int32_t* src, const int32_t* dst, con
   double dv = valid ? __dadd_rn((double)f, (double)f) : 0.0;
   double sum = seg_warp_sum<int64_t>(dv, u);
   if (seg_warp_last<int64_t>(u, valid)) atomicAdd(&k[u], sum);
+}
+
+// ---------------------------------------------------------- streamed level-0 build
+// The checks and CSR build of a list that arrives from the host chunk by
+// chunk, each chunk processed while later ones are still being copied.  The
+// CSR is the one build_csr_fast makes; it is kept only if the whole list
+// turns out strictly sorted and symmetric.
+
+__device__ __forceinline__ bool entry_ok(int32_t u, int32_t v, float x, int32_t V) {
+  return u >= 0 && u < V && v >= 0 && v < V && x >= 0.0f && !isinf(x);   // as validate_kernel
+}
+
+// One chunk [b, e_end): range/weight check, strict order against the previous
+// entry, the symmetry fingerprints of list_check_kernel, per-row counts of
+// non-loop entries (into cnt) and the chunk's non-loop flags (pos[b..e_end),
+// scanned next).  Grid covers the chunk in whole warps.
+__global__ void pre_chunk_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t b, int64_t e_end,
+                                 int32_t V, uint32_t* flags, unsigned long long* sums, unsigned long long* cnt,
+                                 uint32_t* pos) {
+  const uint64_t K1 = 0x243F6A8885A308D3ull, K2 = 0x13198A2E03707344ull;   // as list_check_kernel
+  const unsigned full = 0xffffffffu;
+  const int64_t e = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool in = e < e_end;
+  const int32_t u = in ? src[e] : 0, v = in ? dst[e] : 0;
+  const float x = in ? w[e] : 0.0f;
+  const bool ok = in && entry_ok(u, v, x, V);
+  bool unsorted = false;
+  if (in && e > 0) {
+    const int32_t u0 = src[e - 1], v0 = dst[e - 1];
+    unsorted = !(u > u0 || (u == u0 && v > v0));
+  }
+  uint64_t d1 = 0, d2 = 0;
+  if (ok && u != v) {
+    const uint32_t wb = __float_as_uint(x);
+    d1 = edge_hash((uint32_t)u, (uint32_t)v, wb, K1) - edge_hash((uint32_t)v, (uint32_t)u, wb, K1);
+    d2 = edge_hash((uint32_t)u, (uint32_t)v, wb, K2) - edge_hash((uint32_t)v, (uint32_t)u, wb, K2);
+  }
+  if (in) pos[e] = (ok && u != v) ? 1u : 0u;
+  const int64_t key = ok ? (int64_t)u : -1;
+  const double n = seg_warp_sum<int64_t>((ok && u != v) ? 1.0 : 0.0, key);
+  if (seg_warp_last<int64_t>(key, ok) && n > 0.0) atomicAdd(&cnt[u], (unsigned long long)n);
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    d1 += __shfl_down_sync(full, d1, o);
+    d2 += __shfl_down_sync(full, d2, o);
+  }
+  const bool any_bad = __any_sync(full, in && !ok), any_unsorted = __any_sync(full, unsorted);
+  if ((threadIdx.x & 31) == 0) {
+    if (d1) atomicAdd(&sums[0], (unsigned long long)d1);
+    if (d2) atomicAdd(&sums[1], (unsigned long long)d2);
+    if (any_unsorted) atomicOr(flags, kNotSorted);
+    if (any_bad) atomicOr(flags, kBadEntry);
+  }
+}
+
+// carry[i + 1] = carry[i] + (non-loop entries of chunk i)
+__global__ void pre_carry_kernel(uint32_t* carry, int64_t i, const uint32_t* chunk_total) {
+  carry[i + 1] = carry[i] + *chunk_total;
+}
+
+// The chunk's CSR entries, degrees and self loops, as csr_fast_emit_kernel
+// does for the whole list (positions: chunk scan + carry).  Entries that
+// failed the checks are skipped.  Grid covers the chunk in whole warps.
+__global__ void pre_emit_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t b, int64_t e_end,
+                                int32_t V, const uint32_t* pos, const uint32_t* carry, int32_t* col, float* cw,
+                                double* k, float* loopw, uint8_t* has_loop) {
+  const int64_t e = b + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool in = e < e_end;
+  const int32_t u = in ? src[e] : 0, v = in ? dst[e] : 0;
+  const float x = in ? w[e] : 0.0f;
+  const bool ok = in && entry_ok(u, v, x, V);
+  const bool loop = ok && u == v;
+  if (ok && !loop) {
+    const uint32_t p = pos[e] + *carry;
+    col[p] = v;
+    cw[p] = __double2float_rn(__dadd_rn((double)x, (double)x));
+  }
+  if (loop) { loopw[u] = x; has_loop[u] = 1; }
+  float f = x == 0.0f ? 1.0f : x;             // InitKernel.cu:165-170, both copies of the entry
+  if (loop) f *= 2.0f;
+  const double dv = ok ? __dadd_rn((double)f, (double)f) : 0.0;
+  const int64_t key = ok ? (int64_t)u : -1;
+  const double sum = seg_warp_sum<int64_t>(dv, key);
+  if (seg_warp_last<int64_t>(key, ok)) atomicAdd(&k[u], sum);
+}
+
+// Group partials of the fixed-tree sum of the weights (as tree_sum_f32's
+// first round; group b of the chunk starting at x).
+__global__ void __launch_bounds__(kRedThreads) pre_group_kernel(const float* x, int64_t n, double* out) {
+  __shared__ double ws[8];
+  const int64_t b = blockIdx.x;
+  int64_t len = n - b * kGroup;
+  if (len > kGroup) len = kGroup;
+  const double r = group_sum_block<float>(x + b * kGroup, len, ws);
+  if (threadIdx.x == 0) out[b] = r;
 }
 
 __global__ void row_off_kernel(const int64_t* rowstart, const uint32_t* pos, int32_t V, int64_t* off) {
@@ -1883,6 +1978,91 @@ bool validate_edges(const int32_t* src, const int32_t* dst, const float* w, int6
   return h == 0;
 }
 
+bool stream_load_level0(const int32_t* hsrc, const int32_t* hdst, const float* hw, int32_t* src, int32_t* dst,
+                        float* w, int64_t E, int32_t V, int64_t chunk, PreCsr& pre, std::vector<cudaEvent_t>& evs,
+                        Arena& a, cudaStream_t s, cudaStream_t copy) {
+  pre = PreCsr();
+  chunk = std::max<int64_t>(kGroup, (chunk + kGroup - 1) / kGroup * kGroup);
+  const int64_t nchunks = (E + chunk - 1) / chunk;
+  const size_t mark = a.lo;
+  pre.off = a.lo_n<int64_t>((int64_t)V + 1);
+  pre.col = a.lo_n<int32_t>(E);
+  pre.cw = a.lo_n<float>(E);
+  pre.k = a.lo_n<double>(V);
+  pre.loopw = a.lo_n<float>(V);
+  pre.has_loop = a.lo_n<uint8_t>(V);
+  bool valid = false, bad = false;
+  {
+    HiScope hs(a);
+    uint32_t* pos = a.hi_n<uint32_t>(E + 1);
+    const int64_t ngroups = (E + kGroup - 1) / kGroup;
+    double* gpart = a.hi_n<double>(ngroups);
+    double* d_m = a.hi_n<double>(1);
+    unsigned long long* chk = a.hi_n<unsigned long long>(3);   // flags, two fingerprint sums
+    uint32_t* carry = a.hi_n<uint32_t>(nchunks + 1);
+    LVG_CUDA(cudaMemsetAsync(pre.off, 0, sizeof(int64_t) * ((size_t)V + 1), s));
+    LVG_CUDA(cudaMemsetAsync(pre.k, 0, sizeof(double) * std::max<int32_t>(V, 1), s));
+    LVG_CUDA(cudaMemsetAsync(pre.loopw, 0, sizeof(float) * std::max<int32_t>(V, 1), s));
+    LVG_CUDA(cudaMemsetAsync(pre.has_loop, 0, std::max<int32_t>(V, 1), s));
+    LVG_CUDA(cudaMemsetAsync(chk, 0, 3 * sizeof(unsigned long long), s));
+    LVG_CUDA(cudaMemsetAsync(carry, 0, sizeof(uint32_t), s));
+    while ((int64_t)evs.size() < nchunks + 1) {
+      cudaEvent_t ev;
+      LVG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      evs.push_back(ev);
+    }
+    // the copies start once earlier work of the stream (which may still use
+    // this memory) is done; chunk i's kernels start once its copies are
+    LVG_CUDA(cudaEventRecord(evs[nchunks], s));
+    LVG_CUDA(cudaStreamWaitEvent(copy, evs[nchunks], 0));
+    // chunk i's copies are issued before chunk i-1's kernels, so that the
+    // kernels overlap the next copy even when a copy from pageable memory
+    // holds the host thread until it is staged
+    auto issue_copy = [&](int64_t i) {
+      const int64_t b = i * chunk, n = std::min(chunk, E - b);
+      LVG_CUDA(cudaMemcpyAsync(src + b, hsrc + b, sizeof(int32_t) * n, cudaMemcpyHostToDevice, copy));
+      LVG_CUDA(cudaMemcpyAsync(dst + b, hdst + b, sizeof(int32_t) * n, cudaMemcpyHostToDevice, copy));
+      LVG_CUDA(cudaMemcpyAsync(w + b, hw + b, sizeof(float) * n, cudaMemcpyHostToDevice, copy));
+      LVG_CUDA(cudaEventRecord(evs[i], copy));
+    };
+    issue_copy(0);
+    for (int64_t i = 0; i < nchunks; ++i) {
+      const int64_t b = i * chunk, n = std::min(chunk, E - b);
+      if (i + 1 < nchunks) issue_copy(i + 1);
+      LVG_CUDA(cudaStreamWaitEvent(s, evs[i], 0));
+      pre_chunk_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(src, dst, w, b, b + n, V, (uint32_t*)chk, chk + 1,
+                                                                   (unsigned long long*)pre.off, pos);
+      LVG_LAUNCH();
+      scan_u32(pos + b, pos + b, n, a, s);
+      pre_carry_kernel<<<1, 1, 0, s>>>(carry, i, pos + b + n);
+      LVG_LAUNCH();
+      pre_emit_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(src, dst, w, b, b + n, V, pos, carry + i, pre.col,
+                                                                  pre.cw, pre.k, pre.loopw, pre.has_loop);
+      LVG_LAUNCH();
+      pre_group_kernel<<<(unsigned)((n + kGroup - 1) / kGroup), kRedThreads, 0, s>>>(w + b, n, gpart + b / kGroup);
+      LVG_LAUNCH();
+    }
+    tree_finish(gpart, ngroups, d_m, a, s);
+    unsigned long long h[3] = {0, 0, 0};
+    LVG_CUDA(cudaMemcpyAsync(h, chk, sizeof h, cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaMemcpyAsync(&pre.m, d_m, sizeof(double), cudaMemcpyDeviceToHost, s));
+    LVG_CUDA(cudaStreamSynchronize(s));
+    bad = (h[0] & kBadEntry) != 0;
+    valid = !bad && h[0] == 0 && h[1] == 0 && h[2] == 0;
+    if (valid) {
+      scan_i64(pre.off, pre.off, V, a, s);   // non-loop entries before each row
+      LVG_CUDA(cudaMemcpyAsync(&pre.nnz, pre.off + V, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      LVG_CUDA(cudaStreamSynchronize(s));
+    }
+  }
+  if (!valid) {
+    a.lo = mark;   // the list is not in that form: the level build makes the CSR
+    pre = PreCsr();
+  }
+  pre.valid = valid;
+  return !bad;
+}
+
 // Sort-free CSR build; returns false (and builds nothing) unless the level
 // list is strictly sorted and symmetric.
 static void set_move_attributes();
@@ -1929,17 +2109,30 @@ void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s) {
   const int64_t n = 2 * E;
   if (n >= ((int64_t)1 << 32)) throw Error(LVG_ERR_CAPACITY, "doubled edge list exceeds 2^32-1 entries");
   // per-vertex arrays (low end, level lifetime)
-  g.off = a.lo_n<int64_t>(V + 1);
-  g.k = a.lo_n<double>(V);
+  const bool pre = g.pre && g.pre->valid;
   g.kfrac = a.lo_n<double>(V);
-  g.loopw = a.lo_n<float>(V);
-  g.has_loop = a.lo_n<uint8_t>(V);
   double* d_m = a.lo_n<double>(1);
-  LVG_CUDA(cudaMemsetAsync(g.k, 0, sizeof(double) * std::max<int32_t>(V, 1), s));
-  LVG_CUDA(cudaMemsetAsync(g.loopw, 0, sizeof(float) * std::max<int32_t>(V, 1), s));
-  LVG_CUDA(cudaMemsetAsync(g.has_loop, 0, std::max<int32_t>(V, 1), s));
-  tree_sum_f32(g.w, E, d_m, a, s);                                  // NeighbourCompute.cu:46
-  g.sorted_symmetric = E > 0 && build_csr_fast(g, a, s);
+  if (pre) {   // level 0 built while it streamed in (stream_load_level0)
+    g.off = g.pre->off;
+    g.col = g.pre->col;
+    g.cw = g.pre->cw;
+    g.k = g.pre->k;
+    g.loopw = g.pre->loopw;
+    g.has_loop = g.pre->has_loop;
+    g.nnz = g.pre->nnz;
+    LVG_CUDA(cudaMemcpyAsync(d_m, &g.pre->m, sizeof(double), cudaMemcpyHostToDevice, s));
+    g.sorted_symmetric = true;
+  } else {
+    g.off = a.lo_n<int64_t>(V + 1);
+    g.k = a.lo_n<double>(V);
+    g.loopw = a.lo_n<float>(V);
+    g.has_loop = a.lo_n<uint8_t>(V);
+    LVG_CUDA(cudaMemsetAsync(g.k, 0, sizeof(double) * std::max<int32_t>(V, 1), s));
+    LVG_CUDA(cudaMemsetAsync(g.loopw, 0, sizeof(float) * std::max<int32_t>(V, 1), s));
+    LVG_CUDA(cudaMemsetAsync(g.has_loop, 0, std::max<int32_t>(V, 1), s));
+    tree_sum_f32(g.w, E, d_m, a, s);                                  // NeighbourCompute.cu:46
+    g.sorted_symmetric = E > 0 && build_csr_fast(g, a, s);
+  }
   if (!g.sorted_symmetric) {
     HiScope hs(a);
     const int B = std::max(1, bits_for(V));

@@ -30,6 +30,22 @@ enum : uint32_t { kErrProbe = 1u };
 // Degree classes of the move kernels (see bucket_of).
 enum { kB4 = 0, kB8, kB16, kB32, kBTile, kBBlock, kBHub, kNumBuckets };
 
+// Level-0 CSR built while the list streamed in from the host
+// (stream_load_level0); valid only if the whole list was in range, strictly
+// sorted and symmetric.  Lives below the level region of the arena, so a
+// rerun from level 0 uses it again.
+struct PreCsr {
+  bool valid = false;
+  int64_t* off = nullptr;
+  int32_t* col = nullptr;
+  float* cw = nullptr;
+  double* k = nullptr;
+  float* loopw = nullptr;
+  uint8_t* has_loop = nullptr;
+  double m = 0.0;
+  int64_t nnz = 0;
+};
+
 // One level of the graph on the device.
 struct LevelGraph {
   int32_t V = 0;
@@ -47,6 +63,7 @@ struct LevelGraph {
   uint8_t* has_loop = nullptr;
   double m = 0.0;                 // sum of input weights (NeighbourCompute.cu:46)
   bool sorted_symmetric = false;  // CSR built without sorting (list sorted and symmetric)
+  const PreCsr* pre = nullptr;    // level 0 only: CSR built during the upload
   const double* gm = nullptr;     // batched runs: m of each graph (device)
   const int32_t* vgid = nullptr;  // batched runs: graph of each vertex (device)
   int32_t* blist = nullptr;       // vertices grouped by degree class, in index order inside a class
@@ -131,6 +148,15 @@ bool validate_edges(const int32_t* src, const int32_t* dst, const float* w, int6
 // Build the level CSR, degrees, loops and buckets (NeighbourCompute.cu:42-117,
 // InitKernel.cu:245-339).  Level arrays go to the arena's low end.
 void build_level(LevelGraph& g, const Tuning& t, Arena& a, cudaStream_t s);
+// Copies a host list into (src, dst, w) in chunks of `chunk` entries on
+// `copy` while kernels on `s` check each arrived chunk (ids in range, finite
+// non-negative weights, strict order, symmetry fingerprints) and build the
+// sorted-symmetric CSR into `pre`, allocated at the arena's low end (and
+// released again, pre.valid false, when the list is not in that form).
+// Returns false if an entry failed the range or weight check.
+bool stream_load_level0(const int32_t* hsrc, const int32_t* hdst, const float* hw, int32_t* src, int32_t* dst,
+                        float* w, int64_t E, int32_t V, int64_t chunk, PreCsr& pre, std::vector<cudaEvent_t>& evs,
+                        Arena& a, cudaStream_t s, cudaStream_t copy);
 
 // Allocate community state for g (low end) and set the singleton state
 // (InitKernel.cu:196-216, OneLevelKernel.cu:80-91); ctl->q_prev = Q(S0).

@@ -422,3 +422,35 @@ def test_partition_into_caller_buffers(Louvain, gen):
             lv.partition(out=np.zeros(n - 1, np.int32))
         with pytest.raises(ValueError):
             lv.partition(out=np.zeros(n, np.int64))
+
+
+@pytest.mark.parametrize("form", ["sorted_symmetric", "as_given"])
+def test_chunked_host_load(Louvain, oracle, gen, form):
+    """A host list copied in chunks (load_chunk_entries) while the level-0 CSR
+    is built from the chunks already on the device: the CSR, two whole runs
+    on one load, and the refusal of an out-of-range id or a negative weight in
+    a late chunk equal what the whole-list load gives.  A list that is not
+    sorted and symmetric falls back to the sorting build."""
+    from louvaingpu_b200._lib import LvgError
+    n, s, d, w = make_case(gen, "hub")
+    if form == "sorted_symmetric":
+        s, d, w = sorted_symmetric(oracle, n, s, d, w)
+    assert len(s) > 4 * 4096
+    oc = oracle.Csr(n, s, d, w)
+    orun = oracle.Run(n, s, d, w)
+    with Louvain(load_chunk_entries=4096) as lv:
+        lv.load_edges(s, d, w, n)
+        csr_equal(lv, oc)
+        for _ in range(2):
+            res = lv.run()
+            run_equal(lv, res, orun, n, s, d, w, oracle)
+        bad = d.copy()
+        bad[len(bad) * 2 // 3] = n
+        with pytest.raises(LvgError):
+            lv.load_edges(s, bad, w, n)
+        neg = w.copy()
+        neg[len(neg) - 5] = -1.0
+        with pytest.raises(LvgError):
+            lv.load_edges(s, d, neg, n)
+        lv.load_edges(s, d, w, n)
+        csr_equal(lv, oc)
