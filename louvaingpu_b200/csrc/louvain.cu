@@ -2736,20 +2736,28 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
 }
 
 // Kc and Ain of a list known to be symmetric (every (u, v, w) has its
-// (v, u, w)): the destination side of Kc equals the source side, so each
-// entry adds 2w to its source's community only -- one warp-aggregated update
-// per run of equal sources instead of a scattered update per entry -- and
-// 2w to Ain when both ends share a community.
+// (v, u, w)) and sorted by source: the destination side of Kc equals the
+// source side, so each entry adds 2w to its source's community only, and 2w
+// to Ain when both ends share a community.  Lanes holding entries of one
+// source row add them by a segmented warp scan; the last lane of each row
+// piece makes one atomic update of each sum -- a few updates per row instead
+// of one per entry, and no shuffle loop over all 32 lanes.  Grid-stride over
+// whole warps.
 __global__ void nm_accum_sym_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
                                     const int32_t* part, double* Kc, double* Ain) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t e0 = blockIdx.x * (int64_t)blockDim.x; e0 < E; e0 += stride) {
     const int64_t e = e0 + threadIdx.x;
     const bool ok = e < E;
+    const int32_t u = ok ? src[e] : -1;
     const double x = ok ? 2.0 * (double)w[e] : 0.0;
-    const int32_t a = ok ? part[src[e]] : -1, b = ok ? part[dst[e]] : -1;
-    warp_group_add(Kc, a, x);
-    warp_group_add(Ain, (a >= 0 && a == b) ? a : -1, x);
+    const int32_t a = ok ? part[u] : -1, b = ok ? part[dst[e]] : -1;
+    const double kin = seg_warp_sum<int32_t>(x, u);
+    const double ain = seg_warp_sum<int32_t>(a == b ? x : 0.0, u);
+    if (seg_warp_last<int32_t>(u, ok)) {
+      atomicAdd(&Kc[a], kin);
+      if (ain != 0.0) atomicAdd(&Ain[a], ain);
+    }
   }
 }
 
