@@ -81,6 +81,7 @@ struct lvg_ctx {
   int64_t move_passes = 0;
   std::vector<float> move_pass_ms;  // move kernels of each pass of the last one-level phase
   PreCsr pre0;                    // level-0 CSR built during a chunked host upload
+  PreCsr pre_next;                // CSR of the level just coarsened into, written by the coarsening
   cudaStream_t copy_stream = nullptr;   // host-list upload chunks (lvg_load_edges)
   std::vector<cudaEvent_t> load_ev;     // one per upload chunk
 };
@@ -361,16 +362,39 @@ void induce_level(lvg_ctx* c) {
   float* ow = nullptr;
   c->arena.hi = c->run_hi;
   LVG_CUDA(cudaEventRecord(c->pev[4], c->stream));
-  int64_t n = induce(c->g, c->d_part_cur, c->C_cur, &os, &od, &ow, c->arena, c->stream);
-  // the next level's list moves down to the start of the level region
+  PreCsr hi_csr;
+  int64_t n = induce(c->g, c->d_part_cur, c->C_cur, &os, &od, &ow, c->arena, c->stream, &hi_csr);
+  // the next level's list (and its CSR, when the coarsening wrote it) moves
+  // down to the start of the level region
   c->arena.lo = c->base_lo;
   int32_t* ns = c->arena.lo_n<int32_t>(n);
   int32_t* nd = c->arena.lo_n<int32_t>(n);
   float* nw = c->arena.lo_n<float>(n);
-  if (n > 0) {
-    LVG_CUDA(cudaMemcpyAsync(ns, os, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
-    LVG_CUDA(cudaMemcpyAsync(nd, od, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
-    LVG_CUDA(cudaMemcpyAsync(nw, ow, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+  auto down = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes) LVG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  };
+  down(ns, os, sizeof(int32_t) * n);
+  down(nd, od, sizeof(int32_t) * n);
+  down(nw, ow, sizeof(float) * n);
+  const int32_t C1 = c->C_cur;
+  c->pre_next = PreCsr();
+  if (hi_csr.valid) {
+    PreCsr& p = c->pre_next;
+    p.off = c->arena.lo_n<int64_t>((int64_t)C1 + 1);
+    p.col = c->arena.lo_n<int32_t>(hi_csr.nnz);
+    p.cw = c->arena.lo_n<float>(hi_csr.nnz);
+    p.k = c->arena.lo_n<double>(C1);
+    p.loopw = c->arena.lo_n<float>(C1);
+    p.has_loop = c->arena.lo_n<uint8_t>(C1);
+    down(p.off, hi_csr.off, sizeof(int64_t) * ((size_t)C1 + 1));
+    down(p.col, hi_csr.col, sizeof(int32_t) * hi_csr.nnz);
+    down(p.cw, hi_csr.cw, sizeof(float) * hi_csr.nnz);
+    down(p.k, hi_csr.k, sizeof(double) * C1);
+    down(p.loopw, hi_csr.loopw, sizeof(float) * C1);
+    down(p.has_loop, hi_csr.has_loop, C1);
+    p.m = hi_csr.m;
+    p.nnz = hi_csr.nnz;
+    p.valid = true;
   }
   LVG_CUDA(cudaEventRecord(c->pev[5], c->stream));
   sync(c);
@@ -386,6 +410,7 @@ void induce_level(lvg_ctx* c) {
   c->g.src = ns;
   c->g.dst = nd;
   c->g.w = nw;
+  c->g.pre = &c->pre_next;
   c->level += 1;
   prepare_level(c);
 }

@@ -204,7 +204,7 @@ static_assert(sizeof(uint32_t) * kIcHashSlots + sizeof(double) * kIcHashSlots <=
                   offsetof(IcSmem, wmax), "hash table fits below the block's scalars");
 
 __device__ __forceinline__ void ic_chunk_hash(IcSmem& S, unsigned char* raw, const uint64_t* k, const float* x,
-                                              int n, int64_t p0, uint64_t* tkey, double* tsum) {
+                                              int n, int64_t p0, uint64_t* tkey, double* tsum, uint32_t* hl) {
   const unsigned full = 0xffffffffu;
   const int t = threadIdx.x, lane = t & 31;
   const int32_t a0 = S.loc_a[0];
@@ -254,6 +254,7 @@ __device__ __forceinline__ void ic_chunk_hash(IcSmem& S, unsigned char* raw, con
     if (hk[slot] != kIcEmpty) {
       tkey[p0 + o] = ((uint64_t)(uint32_t)a0 << 32) | hk[slot];
       tsum[p0 + o] = hv[slot];
+      if (hk[slot] == (uint32_t)a0) hl[a0] = 1u;
       ++o;
     }
   }
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(kIcThreads, 2) ic_chunk_kernel(
     int64_t E, int64_t nchunks, int Bb, const int32_t* mem, const int32_t* mcomm, const int64_t* mscan,
     const int32_t* cfirst, const int64_t* off, const uint32_t* lscan, const int32_t* cvl, const float* lw,
     uint64_t* tkey, double* tsum, uint32_t* dcount, uint32_t* firstrun, uint32_t* c_runs,
-    uint32_t* c_nl, uint32_t* c_nr, uint32_t* c_flags, int32_t* c_ar) {
+    uint32_t* c_nl, uint32_t* c_nr, uint32_t* c_flags, int32_t* c_ar, uint32_t* hl, uint32_t* notint) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   IcSmem& S = *reinterpret_cast<IcSmem*>(smem_raw);
   const unsigned full = 0xffffffffu;
@@ -353,6 +354,7 @@ __global__ void __launch_bounds__(kIcThreads, 2) ic_chunk_kernel(
   // gather (warp-striped positions: q = w*256 + jj*32 + lane)
   uint64_t k[kIcItems];
   float x[kIcItems];
+  bool frac = false;   // a weight that is not an integer
   const uint64_t bmask = (Bb >= 64) ? ~0ull : ((1ull << Bb) - 1ull);
 #pragma unroll
   for (int jj = 0; jj < kIcItems; ++jj) {
@@ -366,14 +368,15 @@ __global__ void __launch_bounds__(kIcThreads, 2) ic_chunk_kernel(
       const float wv = __ldg(lw + e);
       k[jj] = ((uint64_t)(pk >> kIcRelBits) << Bb) | b;
       x[jj] = wv == 0.0f ? 1.0f : wv;     // InducedGraphKernel.cu:38-39
+      frac |= wv != truncf(wv);
     }
   }
-  __syncthreads();
+  if (__syncthreads_or(frac) && t == 0) atomicOr(notint, 1u);
   if (nloc == 1 && S.openL && S.openR) {
     // The chunk lies inside one segment that continues on both sides: its
     // runs all go on to the device-wide sort, so they need no order here.
     // Equal cv are summed in a shared-memory hash table instead of sorted.
-    ic_chunk_hash(S, smem_raw, k, x, n, p0, tkey, tsum);
+    ic_chunk_hash(S, smem_raw, k, x, n, p0, tkey, tsum, hl);
     if (t == 0) {
       const uint32_t runs = S.nloc;   // set by ic_chunk_hash
       c_runs[j] = runs;
@@ -486,6 +489,7 @@ __global__ void __launch_bounds__(kIcThreads, 2) ic_chunk_kernel(
         const int32_t a = S.loc_a[kk >> Bb];
         tkey[p0 + run] = ((uint64_t)(uint32_t)a << 32) | (kk & bmask);
         tsum[p0 + run] = acc;
+        if ((kk & bmask) == (uint64_t)(uint32_t)a) hl[a] = 1u;   // the community's self loop
       }
     }
   }
@@ -588,42 +592,123 @@ __global__ void ic_open_dcount_kernel(uint32_t n_open, const uint32_t* ofirst, c
 }
 
 // ------------------------------------------------------------------ placement
+// The next level's CSR, written with the list (what build_csr_fast would make
+// of it): a non-loop entry at list position p of row a goes to p - (loops in
+// rows before a) - (1 if row a's loop sorts before it); a loop sets the row's
+// loop weight; degrees k sum f = (w == 0 ? 1 : w), doubled, twice for a loop
+// (InitKernel.cu:154-194).
+struct IcCsrOut {
+  int32_t* col;
+  float* cw;
+  double* k;
+  float* loopw;
+  uint8_t* has_loop;
+  const uint32_t* hl;      // [C] 1: the coarse list has (a, a)
+  const uint32_t* loopx;   // [C + 1] exclusive scan of hl
+};
+
+__device__ __forceinline__ double ic_seg_sum(double v, int32_t seg) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double u = __shfl_up_sync(full, v, o);
+    const int32_t t = __shfl_up_sync(full, seg, o);
+    if (lane >= o && t == seg) v = __dadd_rn(v, u);
+  }
+  return v;
+}
+
+// One coarse entry (a, b, wf) at list position p (when `emit`) into the CSR,
+// and its row's degree: lanes of a warp with the same row add first.  All
+// lanes of the warp call it; `row` is a for every lane holding an entry of
+// the sorted order (emitting or not) and -1 past the end.
+__device__ __forceinline__ void ic_emit_csr(const IcCsrOut& O, bool emit, int32_t row, int32_t b, float wf,
+                                            uint64_t p) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const bool loop = emit && row == b;
+  if (emit && !loop) {
+    const uint64_t cp = p - O.loopx[row] - ((O.hl[row] && b > row) ? 1u : 0u);
+    O.col[cp] = b;
+    O.cw[cp] = __double2float_rn(__dadd_rn((double)wf, (double)wf));
+  }
+  if (loop) {
+    O.loopw[row] = wf;
+    O.has_loop[row] = 1;
+  }
+  float f = wf == 0.0f ? 1.0f : wf;
+  if (loop) f *= 2.0f;
+  const double sum = ic_seg_sum(emit ? __dadd_rn((double)f, (double)f) : 0.0, row);
+  const int32_t nx = __shfl_down_sync(full, row, 1);
+  if (row >= 0 && (lane == 31 || nx != row) && sum != 0.0) atomicAdd(&O.k[row], sum);
+}
+
 // Runs of the segments inside one chunk, to their final slots.  A block per chunk.
 __global__ void ic_final_closed_kernel(const uint32_t* c_runs, const uint32_t* c_nl, const uint32_t* c_nr,
                                        const uint32_t* c_flags, const uint64_t* tkey, const double* tsum,
                                        const uint32_t* segoff, const uint32_t* firstrun, int32_t* osrc,
-                                       int32_t* odst, float* ow) {
+                                       int32_t* odst, float* ow, IcCsrOut O) {
   const int64_t j = blockIdx.x;
   if (c_flags[j] & kSingle) return;
   const uint32_t lo = c_nl[j], hi = c_runs[j] - c_nr[j];
-  for (uint32_t r = lo + threadIdx.x; r < hi; r += blockDim.x) {
-    const uint64_t tt = (uint64_t)j * kIcChunk + r;
-    const uint64_t kk = tkey[tt];
-    const int32_t a = (int32_t)(kk >> 32);
-    const uint64_t p = (uint64_t)segoff[a] + (tt - firstrun[a]);
-    osrc[p] = a;
-    odst[p] = (int32_t)(uint32_t)kk;
-    ow[p] = __double2float_rn(tsum[tt]);
+  for (uint32_t r0 = lo; r0 < hi; r0 += blockDim.x) {   // whole warps every round
+    const uint32_t r = r0 + threadIdx.x;
+    const bool valid = r < hi;
+    int32_t a = -1, b = 0;
+    float wf = 0.0f;
+    uint64_t p = 0;
+    if (valid) {
+      const uint64_t tt = (uint64_t)j * kIcChunk + r;
+      const uint64_t kk = tkey[tt];
+      a = (int32_t)(kk >> 32);
+      b = (int32_t)(uint32_t)kk;
+      p = (uint64_t)segoff[a] + (tt - firstrun[a]);
+      wf = __double2float_rn(tsum[tt]);
+      osrc[p] = a;
+      odst[p] = b;
+      ow[p] = wf;
+    }
+    if (O.col) ic_emit_csr(O, valid, a, b, wf, p);
   }
 }
 
-// Distinct keys of the open segments, to their final slots.
+// Distinct keys of the open segments, to their final slots.  Grid-stride
+// over whole warps.
 __global__ void ic_final_open_kernel(const uint64_t* k, int64_t n, int Bb, const uint32_t* pos,
                                      const uint32_t* head, const uint32_t* ofirst, const int32_t* oa,
                                      const uint32_t* segoff, const double* osum, int32_t* osrc, int32_t* odst,
-                                     float* ow) {
+                                     float* ow, IcCsrOut O) {
   const uint64_t bmask = (1ull << Bb) - 1ull;
-  IC_FOR(i, n) {
-    if (!head[i]) continue;
-    const uint32_t g = pos[i];
-    const uint64_t kk = k[i];
-    const uint32_t o = (uint32_t)(kk >> Bb);
-    const int32_t a = oa[o];
-    const uint64_t p = (uint64_t)segoff[a] + (g - ofirst[o]);
-    osrc[p] = a;
-    odst[p] = (int32_t)(kk & bmask);
-    ow[p] = __double2float_rn(osum[g]);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += stride) {
+    const int64_t i = i0 + threadIdx.x;
+    const bool in = i < n;
+    const bool emit = in && head[i];
+    int32_t a = -1, b = 0;
+    float wf = 0.0f;
+    uint64_t p = 0;
+    if (in) {
+      const uint64_t kk = k[i];
+      const uint32_t o = (uint32_t)(kk >> Bb);
+      a = oa[o];
+      b = (int32_t)(kk & bmask);
+      if (emit) {
+        const uint32_t g = pos[i];
+        p = (uint64_t)segoff[a] + (g - ofirst[o]);
+        wf = __double2float_rn(osum[g]);
+        osrc[p] = a;
+        odst[p] = b;
+        ow[p] = wf;
+      }
+    }
+    if (O.col) ic_emit_csr(O, emit, a, b, wf, p);
   }
+}
+
+// CSR row offsets of the next level: list row start minus the loops before.
+__global__ void ic_csr_off_kernel(int32_t C, const uint32_t* segoff, const uint32_t* loopx, int64_t* off) {
+  IC_FOR(a, (int64_t)C + 1) off[a] = (int64_t)segoff[a] - (int64_t)loopx[a];
 }
 
 // Bytes of scratch induce_sorted may take, at most (the open runs can be all
@@ -633,7 +718,7 @@ size_t induce_sorted_scratch(int64_t V, int64_t E, int64_t C) {
   const int64_t slots = nchunks * kIcChunk;
   size_t b = 0;
   b += (size_t)V * (2 * 12 + 4 + 4 + 4 + 8) + 8 * 256 * (size_t)(V / 4096 + 2);   // member sort, scans
-  b += (size_t)E * 4 + (size_t)slots * 16 + (size_t)nchunks * 28 + (size_t)C * 12;   // cv, runs, chunk facts
+  b += (size_t)E * 4 + (size_t)slots * 16 + (size_t)nchunks * 28 + (size_t)C * 20;   // cv, runs, chunk facts
   b += (size_t)E * (2 * 12 + 4 + 4 + 8 + 4) + 8 * 256 * (size_t)(E / 4096 + 2); // open runs, worst case
   return b + ((size_t)64 << 10) * 32;                                            // alignment slack
 }
@@ -661,7 +746,7 @@ T read_back(const T* d, cudaStream_t s) {
 }  // namespace
 
 bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t* osrc, int32_t* odst, float* ow,
-                   int64_t* count, Arena& a, cudaStream_t s) {
+                   int64_t* count, PreCsr* next, Arena& a, cudaStream_t s) {
   const int32_t V = g.V;
   const int64_t E = g.E;
   if (!g.sorted_symmetric || V <= 0 || C <= 0) return false;
@@ -698,6 +783,9 @@ bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t*
   uint64_t* tkey = a.hi_n<uint64_t>(nchunks * kIcChunk);
   double* tsum = a.hi_n<double>(nchunks * kIcChunk);
   uint32_t* dcount = a.hi_n<uint32_t>((int64_t)C + 1);
+  uint32_t* hl = a.hi_n<uint32_t>((int64_t)C + 2);   // coarse self loops; [C + 1]: a weight not integral
+  uint32_t* notint = hl + C + 1;
+  LVG_CUDA(cudaMemsetAsync(hl, 0, sizeof(uint32_t) * ((size_t)C + 2), s));
   uint32_t* firstrun = a.hi_n<uint32_t>(C);
   uint32_t* c_runs = a.hi_n<uint32_t>(nchunks);
   uint32_t* c_nl = a.hi_n<uint32_t>(nchunks);
@@ -711,7 +799,7 @@ bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t*
   LVG_LAUNCH();
   ic_chunk_kernel<<<(unsigned)nchunks, kIcThreads, sizeof(IcSmem), s>>>(
       E, nchunks, Bb, mem, mcomm, mscan, cfirst, g.off, lscan, cvl, g.w, tkey, tsum, dcount, firstrun, c_runs,
-      c_nl, c_nr, c_flags, c_ar);
+      c_nl, c_nr, c_flags, c_ar, hl, notint);
   LVG_LAUNCH();
   // segments open across chunk boundaries
   uint32_t* newr = a.hi_n<uint32_t>(nchunks + 1);
@@ -721,6 +809,10 @@ bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t*
   scan_u32(newr, newr, nchunks, a, s);
   scan_u32(nopen, nopen, nchunks, a, s);
   const uint32_t n_open = read_back(newr + nchunks, s);
+  // The CSR is written only for integral weights: then every sum is exact,
+  // so the coarse list is exactly symmetric, as the CSR written from one
+  // direction assumes.
+  const bool int_weights = read_back(notint, s) == 0u;
   const int64_t n_orun = read_back(nopen + nchunks, s);
   uint64_t* okeys = nullptr;
   uint32_t *ohead = nullptr, *opos = nullptr, *ofirst = nullptr;
@@ -757,13 +849,32 @@ bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t*
   uint32_t* segoff = a.hi_n<uint32_t>((int64_t)C + 1);
   scan_u32(dcount, segoff, C, a, s);
   const int64_t cnt = read_back(segoff + C, s);
+  IcCsrOut O{};
+  uint32_t* loopx = a.hi_n<uint32_t>((int64_t)C + 1);
+  if (next && next->col && int_weights) {
+    scan_u32(hl, loopx, C, a, s);
+    LVG_CUDA(cudaMemsetAsync(next->k, 0, sizeof(double) * (size_t)C, s));
+    LVG_CUDA(cudaMemsetAsync(next->loopw, 0, sizeof(float) * (size_t)C, s));
+    LVG_CUDA(cudaMemsetAsync(next->has_loop, 0, (size_t)C, s));
+    O = IcCsrOut{next->col, next->cw, next->k, next->loopw, next->has_loop, hl, loopx};
+  }
   ic_final_closed_kernel<<<(unsigned)nchunks, kIcFlat, 0, s>>>(c_runs, c_nl, c_nr, c_flags, tkey, tsum, segoff,
-                                                               firstrun, osrc, odst, ow);
+                                                               firstrun, osrc, odst, ow, O);
   LVG_LAUNCH();
   if (n_orun > 0) {
     ic_final_open_kernel<<<ic_grid(n_orun), kIcFlat, 0, s>>>(okeys, n_orun, Bb, opos, ohead, ofirst, oa, segoff,
-                                                             osum, osrc, odst, ow);
+                                                             osum, osrc, odst, ow, O);
     LVG_LAUNCH();
+  }
+  if (O.col) {   // the rest of the next level's CSR: row offsets, entry count, m
+    ic_csr_off_kernel<<<ic_grid((int64_t)C + 1), kIcFlat, 0, s>>>(C, segoff, loopx, next->off);
+    LVG_LAUNCH();
+    double* d_m = a.hi_n<double>(1);
+    tree_sum_f32(ow, cnt, d_m, a, s);   // as build_level's m over the list (NeighbourCompute.cu:46)
+    LVG_CUDA(cudaMemcpyAsync(&next->m, d_m, sizeof(double), cudaMemcpyDeviceToHost, s));
+    const int64_t loops = read_back(loopx + C, s);
+    next->nnz = cnt - loops;
+    next->valid = true;
   }
   LVG_CUDA(cudaStreamSynchronize(s));
   *count = cnt;

@@ -2678,7 +2678,7 @@ int32_t renumber(const LevelGraph& g, const int32_t* comm, int32_t* part, Arena&
 }
 
 int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** out_src, int32_t** out_dst,
-               float** out_w, Arena& a, cudaStream_t s) {
+               float** out_w, Arena& a, cudaStream_t s, PreCsr* next) {
   const int64_t E = g.E;
   if (E >= ((int64_t)1 << 32)) throw Error(LVG_ERR_CAPACITY, "level edge list exceeds 2^32-1 entries");
   // the output stays in high scratch for the caller; temporaries are released below it
@@ -2686,7 +2686,18 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
   int32_t* odst = a.hi_n<int32_t>(E);
   float* ow = a.hi_n<float>(E);
   int64_t cnt = 0;
-  if (induce_sorted(g, part, C, osrc, odst, ow, &cnt, a, s)) {
+  if (next) {
+    *next = PreCsr();
+    if (g.sorted_symmetric) {
+      next->off = a.hi_n<int64_t>((int64_t)C + 1);
+      next->col = a.hi_n<int32_t>(E);
+      next->cw = a.hi_n<float>(E);
+      next->k = a.hi_n<double>(C);
+      next->loopw = a.hi_n<float>(C);
+      next->has_loop = a.hi_n<uint8_t>(C);
+    }
+  }
+  if (induce_sorted(g, part, C, osrc, odst, ow, &cnt, next, a, s)) {
     *out_src = osrc;
     *out_dst = odst;
     *out_w = ow;

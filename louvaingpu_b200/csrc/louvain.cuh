@@ -199,11 +199,16 @@ int32_t renumber(const LevelGraph& g, const int32_t* comm, int32_t* part, Arena&
 // sort of all its entries (induce.cu).  Writes the same list as the
 // sort-based path into osrc/odst/ow (capacity E) and its length into *count;
 // returns false, having done nothing, when the list is not in that form or
-// the arena lacks room.
+// the arena lacks room.  With `next` (arrays of capacity E entries / C rows
+// given), also writes the coarse list's CSR as build_csr_fast would build it
+// and marks it valid.
 bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t* osrc, int32_t* odst, float* ow,
-                   int64_t* count, Arena& a, cudaStream_t s);
+                   int64_t* count, PreCsr* next, Arena& a, cudaStream_t s);
+// Coarse list of the level under `part` (C communities), left at the arena's
+// high end.  With `next`: when the sort-free path runs, also the next level's
+// CSR (high end, next->valid set); otherwise next->valid stays false.
 int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** out_src, int32_t** out_dst,
-               float** out_w, Arena& a, cudaStream_t s);
+               float** out_w, Arena& a, cudaStream_t s, PreCsr* next = nullptr);
 
 // FP64 Newman modularity of part[] (values < C) over an input list (device).
 // symmetric: the list is known to hold (v, u, w) for every (u, v, w) (its
