@@ -60,6 +60,9 @@ typedef struct {
                               * while the level-0 CSR is built from the chunks already on the device
                               * (0: 2^25; rounded up to a multiple of 2048; lists of fewer than two
                               * chunks are copied whole, then built) */
+  int32_t coarsen_mode;    /* coarsening of a sorted symmetric level list (InducedGraphKernel.cu:50-113):
+                            * 0 automatic, 1 segment chunks, 2 by transposition, 3 sort of all keys;
+                            * every mode writes the same coarse list */
 } lvg_config;
 
 /* Per-level record of a run (the reference keeps one Partition per level,

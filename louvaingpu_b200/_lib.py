@@ -37,6 +37,7 @@ class LvgConfig(ctypes.Structure):
         ("use_graphs", ctypes.c_int32),
         ("l2_persist", ctypes.c_int32),
         ("load_chunk_entries", ctypes.c_int64),
+        ("coarsen_mode", ctypes.c_int32),
     ]
 
 

@@ -363,7 +363,7 @@ void induce_level(lvg_ctx* c) {
   c->arena.hi = c->run_hi;
   LVG_CUDA(cudaEventRecord(c->pev[4], c->stream));
   PreCsr hi_csr;
-  int64_t n = induce(c->g, c->d_part_cur, c->C_cur, &os, &od, &ow, c->arena, c->stream, &hi_csr);
+  int64_t n = induce(c->g, c->d_part_cur, c->C_cur, &os, &od, &ow, c->arena, c->stream, &hi_csr, c->tune.coarsen);
   // the next level's list (and its CSR, when the coarsening wrote it) moves
   // down to the start of the level region
   c->arena.lo = c->base_lo;
@@ -467,6 +467,9 @@ lvg_status lvg_create(const lvg_config* cfg, lvg_ctx** out) {
     c->tune.warp_max = c->cfg.tile_max_degree > 0 ? std::min(c->cfg.tile_max_degree, 512) : 512;
     c->tune.block_max = c->cfg.block_max_degree > 0 ? std::min(c->cfg.block_max_degree, 8192) : 4096;
     if (c->tune.block_max < c->tune.warp_max) c->tune.block_max = c->tune.warp_max;
+    require(c->cfg.coarsen_mode >= 0 && c->cfg.coarsen_mode <= 3, LVG_ERR_INVALID_ARG,
+            "coarsen_mode must be 0, 1, 2 or 3");
+    c->tune.coarsen = c->cfg.coarsen_mode;
     c->device = c->cfg.device;
     int n = 0;
     LVG_CUDA(cudaGetDeviceCount(&n));

@@ -743,7 +743,407 @@ T read_back(const T* d, cudaStream_t s) {
   return h;
 }
 
+// ------------------------------------------------------------ by transposition
+// The members' rows read in community order (the segment layout above) list
+// every entry (u, d) grouped by part[u], ascending.  The list is symmetric
+// with bitwise-equal weights, so (d, u, w) is an entry as well, and the same
+// positions therefore list every coarse key (part[d], part[u]) grouped by its
+// SECOND community, ascending.  One stable sort by the first community alone
+// then leaves the keys in (first, second) order with equal keys adjacent:
+// 8-bit passes over one community width instead of two, and no sort inside
+// the segments.
+constexpr int kTxThreads = 256;
+constexpr int kTxItems = kIcChunk / kTxThreads;   // 16 consecutive positions (entries) per thread
+
+// Per member of a chunk: start relative to the chunk (0 for the member
+// holding the chunk's first position), list index of its first position
+// minus its start, community.
+struct TxSmem {
+  int32_t rs[kIcChunk + 2];
+  int64_t eb[kIcChunk + 1];
+  int32_t yc[kIcChunk + 1];
+};
+
+// Keys (part[d] << Bb | part[u]) and weights (0 counted as 1) of the entries
+// in segment order, a block per 4096 positions.  The chunk's members are
+// staged in shared memory; a thread takes 16 consecutive positions, finds
+// the member of the first by a binary search and walks on, then issues all
+// 16 list loads and all 16 community gathers before it uses any of them.
+__global__ void __launch_bounds__(kTxThreads) tx_layout_kernel(
+    int64_t E, int32_t nz, int Bb, const int32_t* mem, const int32_t* mcomm, const int64_t* mscan,
+    const int32_t* cfirst, const int64_t* off, const uint32_t* lscan, const int32_t* ldst, const float* lw,
+    const int32_t* part, uint64_t* keys, float* vals, uint32_t* notint) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TxSmem& S = *reinterpret_cast<TxSmem*>(smem_raw);
+  const int64_t c = blockIdx.x;
+  const int64_t p0 = c * (int64_t)kIcChunk;
+  const int n = (int)min((int64_t)kIcChunk, E - p0);
+  // members j0 .. jend - 1 cover [p0, p0 + n); at most kIcChunk of them start
+  // inside the chunk, so nm <= kIcChunk + 1
+  const int32_t j0 = cfirst[c];
+  const int32_t jend = min(cfirst[c + 1] + 1, nz);
+  const int nm = jend - j0;
+  for (int t = threadIdx.x; t <= nm; t += kTxThreads) {
+    const int64_t st = mscan[j0 + t] - p0;
+    S.rs[t] = (int32_t)(st < 0 ? 0 : (st > kIcChunk ? kIcChunk : st));
+    if (t < nm) {
+      const int32_t u = mem[j0 + t];
+      S.eb[t] = off[u] + (int64_t)lscan[u] - mscan[j0 + t];
+      S.yc[t] = mcomm[j0 + t];
+    }
+  }
+  __syncthreads();
+  const int q0 = threadIdx.x * kTxItems;
+  bool frac = false;
+  if (q0 < n) {
+    int lo = 0, hi = nm - 1;   // last member starting at or before q0
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (S.rs[mid] <= q0) lo = mid; else hi = mid - 1;
+    }
+    int64_t e[kTxItems];
+    int32_t y[kTxItems];
+#pragma unroll
+    for (int i = 0; i < kTxItems; ++i) {
+      const int q = q0 + i;
+      e[i] = 0;
+      y[i] = 0;
+      if (q < n) {
+        while (S.rs[lo + 1] <= q) ++lo;   // rs[nm] >= n > q ends the walk
+        e[i] = S.eb[lo] + p0 + q;
+        y[i] = S.yc[lo];
+      }
+    }
+    int32_t d[kTxItems];
+    float wv[kTxItems];
+#pragma unroll
+    for (int i = 0; i < kTxItems; ++i) {
+      const bool ok = q0 + i < n;
+      d[i] = ok ? __ldg(ldst + e[i]) : 0;
+      wv[i] = ok ? __ldg(lw + e[i]) : 1.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < kTxItems; ++i) d[i] = __ldg(part + d[i]);
+    uint64_t* kp = keys + p0 + q0;
+    float* vp = vals + p0 + q0;
+    if (q0 + kTxItems <= n) {
+#pragma unroll
+      for (int i = 0; i < kTxItems; i += 2) {
+        ulonglong2 kk;
+        kk.x = ((uint64_t)(uint32_t)d[i] << Bb) | (uint32_t)y[i];
+        kk.y = ((uint64_t)(uint32_t)d[i + 1] << Bb) | (uint32_t)y[i + 1];
+        reinterpret_cast<ulonglong2*>(kp)[i / 2] = kk;
+      }
+#pragma unroll
+      for (int i = 0; i < kTxItems; i += 4) {
+        float4 vv;
+        vv.x = wv[i] == 0.0f ? 1.0f : wv[i];   // InducedGraphKernel.cu:38-39
+        vv.y = wv[i + 1] == 0.0f ? 1.0f : wv[i + 1];
+        vv.z = wv[i + 2] == 0.0f ? 1.0f : wv[i + 2];
+        vv.w = wv[i + 3] == 0.0f ? 1.0f : wv[i + 3];
+        reinterpret_cast<float4*>(vp)[i / 4] = vv;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < kTxItems; ++i) {
+        if (q0 + i < n) {
+          kp[i] = ((uint64_t)(uint32_t)d[i] << Bb) | (uint32_t)y[i];
+          vp[i] = wv[i] == 0.0f ? 1.0f : wv[i];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kTxItems; ++i) frac |= wv[i] != truncf(wv[i]);
+  }
+  if (__syncthreads_or(frac) && threadIdx.x == 0) atomicOr(notint, 1u);
+}
+
+// The 16 sorted keys and weights of a thread (16-byte loads when whole).
+__device__ __forceinline__ int tx_load16(const uint64_t* k, const float* v, int64_t i0, int64_t n,
+                                         uint64_t (&kk)[kTxItems], float (&vv)[kTxItems]) {
+  const int m = (int)max((int64_t)0, min((int64_t)kTxItems, n - i0));
+  if (m == kTxItems) {
+#pragma unroll
+    for (int i = 0; i < kTxItems; i += 2) {
+      const ulonglong2 x = reinterpret_cast<const ulonglong2*>(k + i0)[i / 2];
+      kk[i] = x.x;
+      kk[i + 1] = x.y;
+    }
+    if (v) {
+#pragma unroll
+      for (int i = 0; i < kTxItems; i += 4) {
+        const float4 x = reinterpret_cast<const float4*>(v + i0)[i / 4];
+        vv[i] = x.x; vv[i + 1] = x.y; vv[i + 2] = x.z; vv[i + 3] = x.w;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < kTxItems; ++i) {
+      kk[i] = i < m ? k[i0 + i] : ~0ull;
+      if (v) vv[i] = i < m ? v[i0 + i] : 0.0f;
+    }
+  }
+  return m;
+}
+
+// Runs of equal keys: the number of run heads (first entries) in every
+// 4096-entry tile of the sorted keys.
+__global__ void __launch_bounds__(kTxThreads) tx_count_kernel(const uint64_t* k, int64_t n, uint32_t* tcount) {
+  const int64_t i0 = blockIdx.x * (int64_t)kIcChunk + (int64_t)threadIdx.x * kTxItems;
+  uint64_t kk[kTxItems];
+  float unused[kTxItems];
+  const int m = tx_load16(k, nullptr, i0, n, kk, unused);
+  uint64_t prev = (i0 > 0 && m > 0) ? k[i0 - 1] : ~0ull;
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int i = 0; i < kTxItems; ++i) {
+    cnt += (i < m && (i0 + i == 0 || kk[i] != prev)) ? 1u : 0u;
+    prev = kk[i];
+  }
+  uint32_t tot;
+  block_exclusive_scan256<uint32_t>(cnt, &tot);
+  if (threadIdx.x == 0) tcount[blockIdx.x] = tot;
+}
+
+// Each run of equal keys once: its key to (osrc, odst) at its distinct index
+// r, its weights summed in FP64 in entry order to wsum[r], the coarse self
+// loops (hl) and the distinct entries of every coarse row (dcount).  A block
+// per 4096-entry tile, 16 consecutive entries per thread; a run that spans
+// threads is finished by the thread that holds its head, which adds the
+// leading pieces of the threads after it.  A run still open at the tile's
+// end (or continuing one from an earlier tile) adds into wsum (zeroed
+// beforehand) with an atomic; every other run is stored once.
+__global__ void __launch_bounds__(kTxThreads) tx_emit_kernel(const uint64_t* k, const float* v, int64_t n, int Bb,
+                                                             const uint32_t* tbase, int32_t* osrc, int32_t* odst,
+                                                             double* wsum, uint32_t* hl, uint32_t* dcount) {
+  __shared__ double lead[kTxThreads];     // sum of the entries before the thread's first head
+  __shared__ uint8_t anyhead[kTxThreads];
+  const uint64_t mask = (1ull << Bb) - 1ull;
+  const int t = threadIdx.x;
+  const int64_t i0 = blockIdx.x * (int64_t)kIcChunk + (int64_t)t * kTxItems;
+  uint64_t kk[kTxItems];
+  float vv[kTxItems];
+  const int m = tx_load16(k, v, i0, n, kk, vv);
+  uint64_t prev = (i0 > 0 && m > 0) ? k[i0 - 1] : ~0ull;
+  uint32_t hmask = 0;
+#pragma unroll
+  for (int i = 0; i < kTxItems; ++i) {
+    if (i < m && (i0 + i == 0 || kk[i] != prev)) hmask |= 1u << i;
+    prev = kk[i];
+  }
+  uint32_t tot;
+  const uint32_t excl = block_exclusive_scan256<uint32_t>((uint32_t)__popc(hmask), &tot);
+  const int64_t rbase = (int64_t)tbase[blockIdx.x] + excl;   // distinct index of this thread's first head
+  // leading piece, complete runs, trailing run
+  double s = 0.0;
+  int64_t r = rbase - 1;
+  int32_t rowa = -1;
+  uint32_t rowcnt = 0;
+  bool started = false;
+#pragma unroll
+  for (int i = 0; i < kTxItems; ++i) {
+    if (i < m) {
+      if ((hmask >> i) & 1u) {
+        if (started) wsum[r] = s;                         // a run that began and ended in this thread
+        else lead[t] = s;
+        started = true;
+        ++r;
+        s = (double)vv[i];
+        const int32_t a = (int32_t)(kk[i] >> Bb), b = (int32_t)(kk[i] & mask);
+        osrc[r] = a;
+        odst[r] = b;
+        if (a == b) hl[a] = 1u;
+        if (a != rowa) {
+          if (rowcnt) atomicAdd(&dcount[rowa], rowcnt);
+          rowa = a;
+          rowcnt = 0;
+        }
+        ++rowcnt;
+      } else {
+        s = __dadd_rn(s, (double)vv[i]);
+      }
+    }
+  }
+  if (rowcnt) atomicAdd(&dcount[rowa], rowcnt);
+  if (!started) lead[t] = s;
+  anyhead[t] = started ? 1 : 0;
+  __syncthreads();
+  // thread 0: entries before the tile's first head continue a run of an
+  // earlier tile; they and the leading pieces after them add to it
+  if (t == 0 && m > 0 && !(hmask & 1u)) {
+    double x = 0.0;
+    for (int u = 0; u < kTxThreads; ++u) {
+      x = __dadd_rn(x, lead[u]);
+      if (anyhead[u]) break;
+    }
+    atomicAdd(&wsum[(int64_t)tbase[blockIdx.x] - 1], x);
+  }
+  // the trailing run of this thread takes the leading pieces of the threads
+  // after it, up to the next thread with a head
+  if (started) {
+    double x = s;
+    bool open = true;
+    for (int u = t + 1; u < kTxThreads; ++u) {
+      x = __dadd_rn(x, lead[u]);
+      if (anyhead[u]) { open = false; break; }
+    }
+    if (open) atomicAdd(&wsum[r], x);
+    else wsum[r] = x;
+  }
+}
+
+// Float weight of every distinct entry and, with a CSR to write, its CSR
+// entry and its row's degree (list position = distinct index).  Four
+// entries per thread in flight; grid-stride over whole warps.
+__global__ void tx_out_kernel(int64_t n, const int32_t* osrc, const int32_t* odst, const double* wsum, float* ow,
+                              IcCsrOut O) {
+  constexpr int U = 4;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x * U;
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x * U; i0 < n; i0 += stride) {
+    int32_t a[U], b[U];
+    float wf[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = i0 + (int64_t)u * blockDim.x + threadIdx.x;
+      const bool valid = i < n;
+      a[u] = valid ? osrc[i] : -1;
+      b[u] = valid ? odst[i] : 0;
+      wf[u] = valid ? __double2float_rn(wsum[i]) : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = i0 + (int64_t)u * blockDim.x + threadIdx.x;
+      if (i < n) ow[i] = wf[u];
+      if (O.col) ic_emit_csr(O, i < n, a[u], b[u], wf[u], (uint64_t)i);
+    }
+  }
+}
+
+void tx_attributes() {
+  constexpr int kDevs = 64;
+  static std::mutex mu;
+  static bool done[kDevs] = {};
+  int dev = 0;
+  LVG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < kDevs && done[dev]) return;
+  LVG_CUDA(cudaFuncSetAttribute(tx_layout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TxSmem)));
+  if (dev >= 0 && dev < kDevs) done[dev] = true;
+}
+
 }  // namespace
+
+// Bytes of scratch induce_transposed may take, at most.
+size_t induce_transposed_scratch(int64_t V, int64_t E, int64_t C) {
+  const int64_t nchunks = (E + kIcChunk - 1) / kIcChunk;
+  size_t b = 0;
+  b += (size_t)V * (2 * 12 + 4 + 4 + 4 + 8) + 8 * 256 * (size_t)(V / 4096 + 2);   // member sort, scans
+  b += (size_t)(nchunks + 1) * 4;                                                  // chunk first members
+  b += (size_t)E * (2 * 12) + 8 * 256 * (size_t)(E / 4096 + 2);                   // keys, weights, look-back
+  b += (size_t)E * 8 + 16 * (size_t)(E / 2048 + 2);                              // run sums, tile counts
+  b += (size_t)C * 16 + 64;                                                        // loops, counts, offsets
+  return b + ((size_t)64 << 10) * 32;                                              // alignment slack
+}
+
+bool induce_transposed(const LevelGraph& g, const int32_t* part, int32_t C, int32_t* osrc, int32_t* odst, float* ow,
+                       int64_t* count, PreCsr* next, Arena& a, cudaStream_t s) {
+  const int32_t V = g.V;
+  const int64_t E = g.E;
+  if (!g.sorted_symmetric || V <= 0 || C <= 0) return false;
+  if (E + 2 * (int64_t)kIcChunk >= ((int64_t)1 << 32)) return false;   // heads and positions are 32-bit
+  if (a.hi < a.lo || a.hi - a.lo < induce_transposed_scratch(V, E, C)) return false;
+  if (E == 0) { *count = 0; return true; }
+  HiScope hs(a);
+  const int64_t nchunks = (E + kIcChunk - 1) / kIcChunk;
+  const int Bb = std::max(1, bits_for(C));
+  // members in community order (stable: vertex order inside a community)
+  uint64_t* mk0 = a.hi_n<uint64_t>(V);
+  float* mv0 = a.hi_n<float>(V);
+  uint64_t* mk1 = a.hi_n<uint64_t>(V);
+  float* mv1 = a.hi_n<float>(V);
+  uint32_t* lscan = a.hi_n<uint32_t>(V + 1);
+  ic_member_keys_kernel<<<ic_grid(V), kIcFlat, 0, s>>>(V, g.off, g.has_loop, part, C, mk0, mv0, lscan);
+  LVG_LAUNCH();
+  const int which = radix_sort_pairs(mk0, mv0, mk1, mv1, V, bits_for((int64_t)C + 1), a, s);
+  scan_u32(lscan, lscan, V, a, s);   // self loops before each vertex: list row start = off + lscan
+  int32_t* mem = a.hi_n<int32_t>(V);
+  int32_t* mcomm = a.hi_n<int32_t>(V);
+  int64_t* mscan = a.hi_n<int64_t>(V + 1);
+  int32_t* nz = a.hi_n<int32_t>(1);
+  LVG_CUDA(cudaMemsetAsync(nz, 0, sizeof(int32_t), s));
+  ic_member_len_kernel<<<ic_grid(V), kIcFlat, 0, s>>>(V, which ? mk1 : mk0, which ? mv1 : mv0, g.off, g.has_loop,
+                                                      C, mem, mcomm, mscan, nz);
+  LVG_LAUNCH();
+  scan_i64(mscan, mscan, V, a, s);
+  if (read_back(mscan + V, s) != E) throw Error(LVG_ERR_CUDA, "coarsening: list rows disagree with the CSR");
+  const int32_t h_nz = read_back(nz, s);
+  int32_t* cfirst = a.hi_n<int32_t>(nchunks + 1);
+  ic_chunk_first_kernel<<<ic_grid(V), kIcFlat, 0, s>>>(mscan, nz, cfirst, nchunks);
+  LVG_LAUNCH();
+  // keys in segment order, then one stable sort by the first community
+  uint64_t* k0 = a.hi_n<uint64_t>(E);
+  float* v0 = a.hi_n<float>(E);
+  uint64_t* k1 = a.hi_n<uint64_t>(E);
+  float* v1 = a.hi_n<float>(E);
+  uint32_t* flags = a.hi_n<uint32_t>(1);   // a weight not integral
+  LVG_CUDA(cudaMemsetAsync(flags, 0, sizeof(uint32_t), s));
+  tx_attributes();
+  tx_layout_kernel<<<(unsigned)nchunks, kTxThreads, sizeof(TxSmem), s>>>(E, h_nz, Bb, mem, mcomm, mscan, cfirst,
+                                                                         g.off, lscan, g.dst, g.w, part, k0, v0,
+                                                                         flags);
+  LVG_LAUNCH();
+  const int w2 = radix_sort_pairs_range(k0, v0, k1, v1, E, Bb, Bb, a, s);
+  const uint64_t* keys = w2 ? k1 : k0;
+  const float* vals = w2 ? v1 : v0;
+  // runs of equal keys: heads per 4096-entry tile, their scan, every run once
+  uint32_t* tcount = a.hi_n<uint32_t>(nchunks + 1);
+  tx_count_kernel<<<(unsigned)nchunks, kTxThreads, 0, s>>>(keys, E, tcount);
+  LVG_LAUNCH();
+  scan_u32(tcount, tcount, nchunks, a, s);
+  const int64_t cnt = read_back(tcount + nchunks, s);
+  const bool int_weights = read_back(flags, s) == 0u;
+  double* wsum = a.hi_n<double>(cnt);
+  uint32_t* hl = a.hi_n<uint32_t>((int64_t)C + 1);
+  uint32_t* dcount = a.hi_n<uint32_t>((int64_t)C + 1);
+  LVG_CUDA(cudaMemsetAsync(wsum, 0, sizeof(double) * (size_t)cnt, s));
+  LVG_CUDA(cudaMemsetAsync(hl, 0, sizeof(uint32_t) * ((size_t)C + 1), s));
+  LVG_CUDA(cudaMemsetAsync(dcount, 0, sizeof(uint32_t) * ((size_t)C + 1), s));
+  tx_emit_kernel<<<(unsigned)nchunks, kTxThreads, 0, s>>>(keys, vals, E, Bb, tcount, osrc, odst, wsum, hl, dcount);
+  LVG_LAUNCH();
+  // The CSR is written only for integral weights: then every sum is exact,
+  // so the coarse list is exactly symmetric, as the CSR written from one
+  // direction assumes.
+  IcCsrOut O{};
+  uint32_t* segoff = nullptr;
+  uint32_t* loopx = nullptr;
+  if (next && next->col && int_weights) {
+    segoff = a.hi_n<uint32_t>((int64_t)C + 1);
+    loopx = a.hi_n<uint32_t>((int64_t)C + 1);
+    scan_u32(dcount, segoff, C, a, s);
+    scan_u32(hl, loopx, C, a, s);
+    LVG_CUDA(cudaMemsetAsync(next->k, 0, sizeof(double) * (size_t)C, s));
+    LVG_CUDA(cudaMemsetAsync(next->loopw, 0, sizeof(float) * (size_t)C, s));
+    LVG_CUDA(cudaMemsetAsync(next->has_loop, 0, (size_t)C, s));
+    O = IcCsrOut{next->col, next->cw, next->k, next->loopw, next->has_loop, hl, loopx};
+  }
+  if (cnt > 0) {
+    tx_out_kernel<<<ic_grid((cnt + 3) / 4), kIcFlat, 0, s>>>(cnt, osrc, odst, wsum, ow, O);
+    LVG_LAUNCH();
+  }
+  if (O.col) {   // the rest of the next level's CSR: row offsets, entry count, m
+    ic_csr_off_kernel<<<ic_grid((int64_t)C + 1), kIcFlat, 0, s>>>(C, segoff, loopx, next->off);
+    LVG_LAUNCH();
+    double* d_m = a.hi_n<double>(1);
+    tree_sum_f32(ow, cnt, d_m, a, s);   // as build_level's m over the list (NeighbourCompute.cu:46)
+    LVG_CUDA(cudaMemcpyAsync(&next->m, d_m, sizeof(double), cudaMemcpyDeviceToHost, s));
+    const int64_t loops = read_back(loopx + C, s);
+    next->nnz = cnt - loops;
+    next->valid = true;
+  }
+  LVG_CUDA(cudaStreamSynchronize(s));
+  *count = cnt;
+  return true;
+}
 
 bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t* osrc, int32_t* odst, float* ow,
                    int64_t* count, PreCsr* next, Arena& a, cudaStream_t s) {

@@ -2678,7 +2678,7 @@ int32_t renumber(const LevelGraph& g, const int32_t* comm, int32_t* part, Arena&
 }
 
 int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** out_src, int32_t** out_dst,
-               float** out_w, Arena& a, cudaStream_t s, PreCsr* next) {
+               float** out_w, Arena& a, cudaStream_t s, PreCsr* next, int32_t mode) {
   const int64_t E = g.E;
   if (E >= ((int64_t)1 << 32)) throw Error(LVG_ERR_CAPACITY, "level edge list exceeds 2^32-1 entries");
   // the output stays in high scratch for the caller; temporaries are released below it
@@ -2697,7 +2697,9 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
       next->has_loop = a.hi_n<uint8_t>(C);
     }
   }
-  if (induce_sorted(g, part, C, osrc, odst, ow, &cnt, next, a, s)) {
+  const bool by_tx = mode == kCoarsenTransposed;
+  if (mode != kCoarsenSort && (by_tx ? induce_transposed(g, part, C, osrc, odst, ow, &cnt, next, a, s)
+                                     : induce_sorted(g, part, C, osrc, odst, ow, &cnt, next, a, s))) {
     *out_src = osrc;
     *out_dst = odst;
     *out_w = ow;
@@ -2752,22 +2754,65 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
 // to Ain when both ends share a community.  Lanes holding entries of one
 // source row add them by a segmented warp scan; the last lane of each row
 // piece makes one atomic update of each sum -- a few updates per row instead
-// of one per entry, and no shuffle loop over all 32 lanes.  Grid-stride over
-// whole warps.
-__global__ void nm_accum_sym_kernel(const int32_t* src, const int32_t* dst, const float* w, int64_t E,
-                                    const int32_t* part, double* Kc, double* Ain) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e0 = blockIdx.x * (int64_t)blockDim.x; e0 < E; e0 += stride) {
-    const int64_t e = e0 + threadIdx.x;
+// of one per entry, and no shuffle loop over all 32 lanes.
+//
+// The row pieces then add into a small block-private table of communities in
+// shared memory (open addressing, a few probes; a community that finds no
+// slot adds to the global sums directly), flushed once per block.  The last
+// levels leave a few very large communities, and one global atomic per row
+// piece into those few addresses would serialise at the L2: with the table
+// each block makes one global update per large community.  Each block takes
+// one contiguous range of the list (whole 256-entry steps, so every warp
+// stays converged), whose rows meet the same large communities again and
+// again.
+constexpr int kNmHotLog = 9;        // 512 slots: 10 KB, eight blocks per SM
+constexpr int kNmHot = 1 << kNmHotLog;
+constexpr int kNmHotProbes = 8;
+constexpr int kNmSymBlocksPerSm = 8;
+
+__device__ __forceinline__ void nm_hot_add(int32_t* hk, double* hK, double* hA, double* Kc, double* Ain, int32_t a,
+                                           double kin, double ain) {
+  uint32_t h = hash_c(a, kNmHotLog);
+  for (int p = 0; p < kNmHotProbes; ++p) {
+    const int32_t prev = atomicCAS(&hk[h], -1, a);
+    if (prev == -1 || prev == a) {
+      atomicAdd(&hK[h], kin);
+      if (ain != 0.0) atomicAdd(&hA[h], ain);
+      return;
+    }
+    h = (h + 1) & (kNmHot - 1);
+  }
+  atomicAdd(&Kc[a], kin);
+  if (ain != 0.0) atomicAdd(&Ain[a], ain);
+}
+
+__global__ void __launch_bounds__(kThreads) nm_accum_sym_kernel(const int32_t* src, const int32_t* dst,
+                                                                const float* w, int64_t E, const int32_t* part,
+                                                                double* Kc, double* Ain) {
+  __shared__ int32_t hk[kNmHot];
+  __shared__ double hK[kNmHot], hA[kNmHot];
+  for (int x = threadIdx.x; x < kNmHot; x += kThreads) { hk[x] = -1; hK[x] = 0.0; hA[x] = 0.0; }
+  __syncthreads();
+  const int64_t steps = (E + kThreads - 1) / kThreads;
+  const int64_t per = (steps + gridDim.x - 1) / gridDim.x;
+  const int64_t s0 = (int64_t)blockIdx.x * per;
+  const int64_t s1 = min(steps, s0 + per);
+  for (int64_t st = s0; st < s1; ++st) {
+    const int64_t e = st * kThreads + threadIdx.x;
     const bool ok = e < E;
     const int32_t u = ok ? src[e] : -1;
     const double x = ok ? 2.0 * (double)w[e] : 0.0;
     const int32_t a = ok ? part[u] : -1, b = ok ? part[dst[e]] : -1;
     const double kin = seg_warp_sum<int32_t>(x, u);
     const double ain = seg_warp_sum<int32_t>(a == b ? x : 0.0, u);
-    if (seg_warp_last<int32_t>(u, ok)) {
-      atomicAdd(&Kc[a], kin);
-      if (ain != 0.0) atomicAdd(&Ain[a], ain);
+    if (seg_warp_last<int32_t>(u, ok)) nm_hot_add(hk, hK, hA, Kc, Ain, a, kin, ain);
+  }
+  __syncthreads();
+  for (int x = threadIdx.x; x < kNmHot; x += kThreads) {
+    const int32_t a = hk[x];
+    if (a >= 0) {
+      atomicAdd(&Kc[a], hK[x]);
+      if (hA[x] != 0.0) atomicAdd(&Ain[a], hA[x]);
     }
   }
 }
@@ -2814,7 +2859,8 @@ double modularity_fp64(const int32_t* src, const int32_t* dst, const float* w, i
   LVG_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * std::max(C, 1), s));
   LVG_CUDA(cudaMemsetAsync(Ain, 0, sizeof(double) * std::max(C, 1), s));
   if (symmetric && E > 0 && C > kNmSmemMax) {
-    nm_accum_sym_kernel<<<sm_grid(E, kThreads), kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
+    const unsigned grid = std::min<unsigned>(grid_for(E, kThreads), (unsigned)(sm_count() * kNmSymBlocksPerSm));
+    nm_accum_sym_kernel<<<grid, kThreads, 0, s>>>(src, dst, w, E, part, Kc, Ain);
     LVG_LAUNCH();
   } else {
     nm_accum(src, dst, w, E, C, part, Kc, Ain, nullptr, s);   // ids checked on the host

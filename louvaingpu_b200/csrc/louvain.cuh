@@ -139,7 +139,11 @@ struct CommState {
 struct Tuning {
   int32_t warp_max = 512;         // largest degree packed into tiles
   int32_t block_max = 4096;       // largest degree with a block-private table
+  int32_t coarsen = 0;            // coarsening method (kCoarsen*)
 };
+
+// Coarsening methods of a level (lvg_config.coarsen_mode).
+enum : int32_t { kCoarsenAuto = 0, kCoarsenChunks = 1, kCoarsenTransposed = 2, kCoarsenSort = 3 };
 
 // Validate an input list on the device: ids in range, weights finite >= 0.
 bool validate_edges(const int32_t* src, const int32_t* dst, const float* w, int64_t E, int32_t V,
@@ -204,11 +208,16 @@ int32_t renumber(const LevelGraph& g, const int32_t* comm, int32_t* part, Arena&
 // and marks it valid.
 bool induce_sorted(const LevelGraph& g, const int32_t* part, int32_t C, int32_t* osrc, int32_t* odst, float* ow,
                    int64_t* count, PreCsr* next, Arena& a, cudaStream_t s);
+// The same list (and CSR) by transposition (induce.cu): the keys listed in
+// segment order of the second community, then one stable sort by the first.
+// Same preconditions and return value as induce_sorted.
+bool induce_transposed(const LevelGraph& g, const int32_t* part, int32_t C, int32_t* osrc, int32_t* odst,
+                       float* ow, int64_t* count, PreCsr* next, Arena& a, cudaStream_t s);
 // Coarse list of the level under `part` (C communities), left at the arena's
 // high end.  With `next`: when the sort-free path runs, also the next level's
 // CSR (high end, next->valid set); otherwise next->valid stays false.
 int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** out_src, int32_t** out_dst,
-               float** out_w, Arena& a, cudaStream_t s, PreCsr* next = nullptr);
+               float** out_w, Arena& a, cudaStream_t s, PreCsr* next = nullptr, int32_t mode = kCoarsenAuto);
 
 // FP64 Newman modularity of part[] (values < C) over an input list (device).
 // symmetric: the list is known to hold (v, u, w) for every (u, v, w) (its

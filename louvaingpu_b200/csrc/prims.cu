@@ -7,6 +7,7 @@
 // in shared memory (warp __match_any_sync multisplit), learns the counts of
 // its digits in all earlier tiles by decoupled look-back (bounded spin, error
 // flag), and writes its keys out digit run by digit run.
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 
@@ -113,13 +114,13 @@ constexpr int kRadix = 256;
 // One pass over the keys gives the global histogram of every digit position.
 constexpr int kRsMaxPasses = 8;
 
-__global__ void __launch_bounds__(kRsThreads) rs_upfront_kernel(const uint64_t* keys, int64_t n, int npass,
+__global__ void __launch_bounds__(kRsThreads) rs_upfront_kernel(const uint64_t* keys, int64_t n, int lo, int npass,
                                                                 uint32_t* ghist) {
   __shared__ uint32_t h[kRsMaxPasses][kRadix];
   for (int i = threadIdx.x; i < kRsMaxPasses * kRadix; i += kRsThreads) (&h[0][0])[i] = 0;
   __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)kRsThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kRsThreads) {
-    const uint64_t k = keys[i];
+    const uint64_t k = keys[i] >> lo;
     for (int p = 0; p < npass; ++p) atomicAdd(&h[p][(unsigned)(k >> (8 * p)) & (kRadix - 1)], 1u);
   }
   __syncthreads();
@@ -301,14 +302,21 @@ void tree_finish(const double* partials, int64_t n, double* d_out, Arena& a, cud
 
 int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n, int bits, Arena& a,
                      cudaStream_t s) {
+  return radix_sort_pairs_range(k0, v0, k1, v1, n, 0, bits, a, s);
+}
+
+int radix_sort_pairs_range(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n, int lo, int bits, Arena& a,
+                           cudaStream_t s) {
   if (n >= ((int64_t)1 << 32)) throw Error(LVG_ERR_CAPACITY, "radix sort limited to 2^32-1 entries");
+  if (lo < 0 || lo >= 64) throw Error(LVG_ERR_INVALID_ARG, "radix sort: first key bit out of range");
+  bits = std::min(bits, 64 - lo);
   if (n <= 1 || bits <= 0) return 0;
   static std::once_flag attr_once;
   std::call_once(attr_once, [] {
     LVG_CUDA(cudaFuncSetAttribute(rs_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sizeof(RsSmem)));
   });
-  const int npass = (std::min(bits, 64) + 7) / 8;
+  const int npass = (bits + 7) / 8;
   HiScope hs(a);
   const int64_t ntiles = (n + kRsTile - 1) / kRsTile;
   unsigned long long* look = a.hi_n<unsigned long long>(ntiles * kRadix);
@@ -318,7 +326,7 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
   LVG_CUDA(cudaMemsetAsync(look, 0, sizeof(unsigned long long) * ntiles * kRadix, s));
   LVG_CUDA(cudaMemsetAsync(ghist, 0, sizeof(uint32_t) * (kRsMaxPasses * kRadix + kRsMaxPasses + 1), s));
   const int64_t ublocks = std::min<int64_t>((n + kRsThreads - 1) / kRsThreads, 148 * 8);
-  rs_upfront_kernel<<<(unsigned)ublocks, kRsThreads, 0, s>>>(k0, n, npass, ghist);
+  rs_upfront_kernel<<<(unsigned)ublocks, kRsThreads, 0, s>>>(k0, n, lo, npass, ghist);
   LVG_LAUNCH();
   rs_gscan_kernel<<<1, kRsThreads, 0, s>>>(ghist, npass);
   LVG_LAUNCH();
@@ -327,7 +335,7 @@ int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n
   float* Vv[2] = {v0, v1};
   for (int p = 0; p < npass; ++p) {
     rs_onesweep_kernel<<<(unsigned)ntiles, kRsThreads, sizeof(RsSmem), s>>>(
-        K[cur], Vv[cur], K[cur ^ 1], Vv[cur ^ 1], n, 8 * p, p, ghist + p * kRadix, look, counters + p, err,
+        K[cur], Vv[cur], K[cur ^ 1], Vv[cur ^ 1], n, lo + 8 * p, p, ghist + p * kRadix, look, counters + p, err,
         g_rs_spin_limit.load(), g_rs_hold_tile.load());
     LVG_LAUNCH();
     cur ^= 1;

@@ -23,5 +23,9 @@ void tree_finish(const double* partials, int64_t n, double* d_out, Arena& a, cud
 // the result (0 or 1).  Requires n < 2^32.
 int radix_sort_pairs(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n, int bits, Arena& a,
                      cudaStream_t s);
+// The same, by key bits [lo, lo + bits): the bits below lo ride along, the
+// bits from lo + bits up must be zero (the last 8-bit digit reads them).
+int radix_sort_pairs_range(uint64_t* k0, float* v0, uint64_t* k1, float* v1, int64_t n, int lo, int bits, Arena& a,
+                           cudaStream_t s);
 
 }  // namespace lvg

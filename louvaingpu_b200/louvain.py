@@ -81,7 +81,7 @@ def pack_graphs(graphs):
 class Louvain:
     def __init__(self, device=0, pass_min_gain=1e-7, level_min_gain=1e-7, max_passes=-1, max_levels=-1,
                  arena_bytes=0, tile_max_degree=0, block_max_degree=0, passes_per_sync=0, use_graphs=True, l2_persist=True,
-                 load_chunk_entries=0):
+                 load_chunk_entries=0, coarsen_mode=0):
         L = _lib.load()
         cfg = _lib.LvgConfig()
         L.lvg_config_default(ctypes.byref(cfg))
@@ -100,6 +100,7 @@ class Louvain:
         cfg.use_graphs = 1 if use_graphs else 0
         cfg.l2_persist = 1 if l2_persist else 0
         cfg.load_chunk_entries = int(load_chunk_entries)
+        cfg.coarsen_mode = int(coarsen_mode)
         self._L = L
         h = ctypes.c_void_p()
         _lib.check(None, L.lvg_create(ctypes.byref(cfg), ctypes.byref(h)))

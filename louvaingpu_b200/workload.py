@@ -52,12 +52,16 @@ def main(argv=None):
     ap.add_argument("--phase", choices=["load", "passes", "coarsen", "run"], default="run")
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--thresholds", default="256,4096", help="tile,block maximum degrees")
+    ap.add_argument("--coarsen", type=int, default=0,
+                    help="coarsening of sorted symmetric levels: 0 automatic, 1 segment chunks, 2 by transposition, "
+                         "3 sort of all keys")
+    ap.add_argument("--levels", action="store_true", help="print each level's sizes and phase times after a run")
     a = ap.parse_args(argv)
     import torch
     torch.cuda.set_device(0)
     keep, args = _graph(a.graph)
     tile, block = (int(x) for x in a.thresholds.split(","))
-    lv = Louvain(tile_max_degree=tile, block_max_degree=block)
+    lv = Louvain(tile_max_degree=tile, block_max_degree=block, coarsen_mode=a.coarsen)
 
     def sync_time():
         torch.cuda.synchronize()
@@ -87,6 +91,11 @@ def main(argv=None):
                 t1 = sync_time()
                 extra = f" communities {C}"
         print(f"{a.graph} {a.phase} repeat {r}: {1e3 * (t1 - t0):.1f} ms{extra}", flush=True)
+        if a.levels and a.phase == "run":
+            for l in range(res.n_levels):
+                x = lv.level_info(l)
+                print(f"  level {l}: V {x.n_vertices} E {x.n_entries} C {x.n_comms} build {x.ms_build:.2f} "
+                      f"passes {x.ms_passes:.2f} renumber {x.ms_renumber:.2f} induce {x.ms_induce:.2f} ms", flush=True)
     lv.close()
     del keep
 

@@ -204,12 +204,15 @@ def test_step_api_matches_run(Louvain, oracle, gen):
         assert (q1, p1) == (orun.levels[1].q, orun.levels[1].passes)
 
 
-def test_lfr_full_size(Louvain, oracle, gen):
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_lfr_full_size(Louvain, oracle, gen, mode):
     """LFR-style n=2^20 config: the dendrogram matches the oracle bit for bit
-    and the final Q lies within 1e-3."""
+    and the final Q lies within 1e-3, whichever method coarsens the sorted
+    symmetric levels (0 automatic, 1 segment chunks, 2 by transposition, 3
+    sort of all keys)."""
     n, s, d, w = gen.lfr()
     orun = oracle.Run(n, s, d, w)
-    with Louvain() as lv:
+    with Louvain(coarsen_mode=mode) as lv:
         lv.load_edges(s, d, w, n)
         res = lv.run()
         run_equal(lv, res, orun, n, s, d, w, oracle)
@@ -353,20 +356,22 @@ def sorted_symmetric(oracle, n, s, d, w):
     return ss, sd, sw
 
 
-@pytest.mark.parametrize("form", ["as_given", "sorted_symmetric"])
+@pytest.mark.parametrize("form,mode", [("as_given", 0), ("sorted_symmetric", 1), ("sorted_symmetric", 2),
+                                       ("sorted_symmetric", 3)])
 @pytest.mark.parametrize("case", ["weighted", "loops_zeros_isolated", "odd_sizes", "hub", "lfr"])
-def test_coarsening_bit_exact(Louvain, oracle, gen, case, form):
+def test_coarsening_bit_exact(Louvain, oracle, gen, case, form, mode):
     """renumber + induce from a given partition: the vertex map
     (RenumberKernel.cu:121-133), the coarse list -- one entry per distinct
     (cu, cv) key in key order, weight 0 counted as 1 (InducedGraphKernel.cu:28-48)
     and equal keys summed (:84-101) -- and the CSR built from it equal the
     oracle's entry for entry.  A list given strictly sorted and symmetric is
     coarsened without the device-wide sort (communities of up to ~10^5 entries
-    here, so segments cross many 4096-entry chunks)."""
+    here, so segments cross many 4096-entry chunks) by each coarsening method:
+    segment chunks (1), by transposition (2) and the sort of all keys (3)."""
     n, s, d, w = gen.lfr() if case == "lfr" else make_case(gen, case)
     if form == "sorted_symmetric":
         s, d, w = sorted_symmetric(oracle, n, s, d, w)
-    with Louvain() as lv:
+    with Louvain(coarsen_mode=mode) as lv:
         for comm in coarsening_partitions(oracle, gen, case, n, s, d, w):
             lv.load_edges(s, d, w, n)
             lv.set_communities(comm)
