@@ -766,9 +766,9 @@ struct TxSmem {
 
 // Keys (part[d] << Bb | part[u]) and weights (0 counted as 1) of the entries
 // in segment order, a block per 4096 positions.  The chunk's members are
-// staged in shared memory; a thread takes 16 consecutive positions, finds
-// the member of the first by a binary search and walks on, then issues all
-// 16 list loads and all 16 community gathers before it uses any of them.
+// staged in shared memory; a thread takes 16 positions 256 apart, finds the
+// member of each by a binary search, then issues all 16 list loads and all
+// 16 community gathers before it uses any of them.
 __global__ void __launch_bounds__(kTxThreads) tx_layout_kernel(
     int64_t E, int32_t nz, int Bb, const int32_t* mem, const int32_t* mcomm, const int64_t* mscan,
     const int32_t* cfirst, const int64_t* off, const uint32_t* lscan, const int32_t* ldst, const float* lw,
@@ -783,77 +783,73 @@ __global__ void __launch_bounds__(kTxThreads) tx_layout_kernel(
   const int32_t j0 = cfirst[c];
   const int32_t jend = min(cfirst[c + 1] + 1, nz);
   const int nm = jend - j0;
-  for (int t = threadIdx.x; t <= nm; t += kTxThreads) {
-    const int64_t st = mscan[j0 + t] - p0;
-    S.rs[t] = (int32_t)(st < 0 ? 0 : (st > kIcChunk ? kIcChunk : st));
-    if (t < nm) {
-      const int32_t u = mem[j0 + t];
-      S.eb[t] = off[u] + (int64_t)lscan[u] - mscan[j0 + t];
-      S.yc[t] = mcomm[j0 + t];
+  {   // stage the members: every thread's loads issued before any is used
+    constexpr int kStage = (kIcChunk + 2 + kTxThreads - 1) / kTxThreads;
+    int64_t st[kStage];
+    int32_t uu[kStage], yy[kStage];
+#pragma unroll
+    for (int x = 0; x < kStage; ++x) {
+      const int t = threadIdx.x + x * kTxThreads;
+      st[x] = t <= nm ? mscan[j0 + t] : 0;
+      uu[x] = t < nm ? mem[j0 + t] : 0;
+      yy[x] = t < nm ? mcomm[j0 + t] : 0;
+    }
+    int64_t ob[kStage];
+#pragma unroll
+    for (int x = 0; x < kStage; ++x) {
+      const int t = threadIdx.x + x * kTxThreads;
+      ob[x] = t < nm ? off[uu[x]] + (int64_t)lscan[uu[x]] : 0;
+    }
+#pragma unroll
+    for (int x = 0; x < kStage; ++x) {
+      const int t = threadIdx.x + x * kTxThreads;
+      if (t <= nm) {
+        const int64_t r = st[x] - p0;
+        S.rs[t] = (int32_t)(r < 0 ? 0 : (r > kIcChunk ? kIcChunk : r));
+      }
+      if (t < nm) {
+        S.eb[t] = ob[x] - st[x];
+        S.yc[t] = yy[x];
+      }
     }
   }
   __syncthreads();
-  const int q0 = threadIdx.x * kTxItems;
+  // position q = i * 256 + thread: a warp's loads and stores are contiguous
+  // along the rows; the member of each position by a branch-free binary
+  // search over the staged starts (all 16 searches independent)
   bool frac = false;
-  if (q0 < n) {
-    int lo = 0, hi = nm - 1;   // last member starting at or before q0
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (S.rs[mid] <= q0) lo = mid; else hi = mid - 1;
+  int64_t e[kTxItems];
+  int32_t y[kTxItems];
+#pragma unroll
+  for (int i = 0; i < kTxItems; ++i) {
+    const int q = i * kTxThreads + threadIdx.x;
+    int lo = 0;
+#pragma unroll
+    for (int b = 12; b >= 0; --b) {   // nm <= kIcChunk + 1 < 2^13
+      const int cand = lo + (1 << b);
+      if (cand < nm && S.rs[cand] <= q) lo = cand;
     }
-    int64_t e[kTxItems];
-    int32_t y[kTxItems];
+    e[i] = q < n ? S.eb[lo] + p0 + q : 0;
+    y[i] = S.yc[lo];
+  }
+  int32_t d[kTxItems];
+  float wv[kTxItems];
 #pragma unroll
-    for (int i = 0; i < kTxItems; ++i) {
-      const int q = q0 + i;
-      e[i] = 0;
-      y[i] = 0;
-      if (q < n) {
-        while (S.rs[lo + 1] <= q) ++lo;   // rs[nm] >= n > q ends the walk
-        e[i] = S.eb[lo] + p0 + q;
-        y[i] = S.yc[lo];
-      }
+  for (int i = 0; i < kTxItems; ++i) {
+    const bool ok = i * kTxThreads + (int)threadIdx.x < n;
+    d[i] = ok ? __ldg(ldst + e[i]) : 0;
+    wv[i] = ok ? __ldg(lw + e[i]) : 1.0f;
+  }
+#pragma unroll
+  for (int i = 0; i < kTxItems; ++i) d[i] = __ldg(part + d[i]);
+#pragma unroll
+  for (int i = 0; i < kTxItems; ++i) {
+    const int q = i * kTxThreads + threadIdx.x;
+    if (q < n) {
+      keys[p0 + q] = ((uint64_t)(uint32_t)d[i] << Bb) | (uint32_t)y[i];
+      vals[p0 + q] = wv[i] == 0.0f ? 1.0f : wv[i];   // InducedGraphKernel.cu:38-39
+      frac |= wv[i] != truncf(wv[i]);
     }
-    int32_t d[kTxItems];
-    float wv[kTxItems];
-#pragma unroll
-    for (int i = 0; i < kTxItems; ++i) {
-      const bool ok = q0 + i < n;
-      d[i] = ok ? __ldg(ldst + e[i]) : 0;
-      wv[i] = ok ? __ldg(lw + e[i]) : 1.0f;
-    }
-#pragma unroll
-    for (int i = 0; i < kTxItems; ++i) d[i] = __ldg(part + d[i]);
-    uint64_t* kp = keys + p0 + q0;
-    float* vp = vals + p0 + q0;
-    if (q0 + kTxItems <= n) {
-#pragma unroll
-      for (int i = 0; i < kTxItems; i += 2) {
-        ulonglong2 kk;
-        kk.x = ((uint64_t)(uint32_t)d[i] << Bb) | (uint32_t)y[i];
-        kk.y = ((uint64_t)(uint32_t)d[i + 1] << Bb) | (uint32_t)y[i + 1];
-        reinterpret_cast<ulonglong2*>(kp)[i / 2] = kk;
-      }
-#pragma unroll
-      for (int i = 0; i < kTxItems; i += 4) {
-        float4 vv;
-        vv.x = wv[i] == 0.0f ? 1.0f : wv[i];   // InducedGraphKernel.cu:38-39
-        vv.y = wv[i + 1] == 0.0f ? 1.0f : wv[i + 1];
-        vv.z = wv[i + 2] == 0.0f ? 1.0f : wv[i + 2];
-        vv.w = wv[i + 3] == 0.0f ? 1.0f : wv[i + 3];
-        reinterpret_cast<float4*>(vp)[i / 4] = vv;
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < kTxItems; ++i) {
-        if (q0 + i < n) {
-          kp[i] = ((uint64_t)(uint32_t)d[i] << Bb) | (uint32_t)y[i];
-          vp[i] = wv[i] == 0.0f ? 1.0f : wv[i];
-        }
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < kTxItems; ++i) frac |= wv[i] != truncf(wv[i]);
   }
   if (__syncthreads_or(frac) && threadIdx.x == 0) atomicOr(notint, 1u);
 }
@@ -886,135 +882,223 @@ __device__ __forceinline__ int tx_load16(const uint64_t* k, const float* v, int6
   return m;
 }
 
-// Runs of equal keys: the number of run heads (first entries) in every
-// 4096-entry tile of the sorted keys.
-__global__ void __launch_bounds__(kTxThreads) tx_count_kernel(const uint64_t* k, int64_t n, uint32_t* tcount) {
+// Runs of equal keys, per 4096-entry tile of the sorted keys: the number of
+// run heads (first entries; low 32 bits) and of heads that are coarse self
+// loops (high 32 bits), so that one scan gives every run its distinct index
+// and the self loops before it.
+__global__ void __launch_bounds__(kTxThreads) tx_count_kernel(const uint64_t* k, int64_t n, int Bb,
+                                                              int64_t* tcount) {
+  const uint64_t mask = (1ull << Bb) - 1ull;
   const int64_t i0 = blockIdx.x * (int64_t)kIcChunk + (int64_t)threadIdx.x * kTxItems;
   uint64_t kk[kTxItems];
   float unused[kTxItems];
   const int m = tx_load16(k, nullptr, i0, n, kk, unused);
   uint64_t prev = (i0 > 0 && m > 0) ? k[i0 - 1] : ~0ull;
-  uint32_t cnt = 0;
+  unsigned long long cnt = 0;
 #pragma unroll
   for (int i = 0; i < kTxItems; ++i) {
-    cnt += (i < m && (i0 + i == 0 || kk[i] != prev)) ? 1u : 0u;
+    if (i < m && (i0 + i == 0 || kk[i] != prev)) cnt += ((kk[i] >> Bb) == (kk[i] & mask)) ? (1ull << 32) + 1ull : 1ull;
     prev = kk[i];
   }
-  uint32_t tot;
-  block_exclusive_scan256<uint32_t>(cnt, &tot);
-  if (threadIdx.x == 0) tcount[blockIdx.x] = tot;
+  unsigned long long tot;
+  block_exclusive_scan256<unsigned long long>(cnt, &tot);
+  if (threadIdx.x == 0) tcount[blockIdx.x] = (int64_t)tot;
 }
 
-// Each run of equal keys once: its key to (osrc, odst) at its distinct index
-// r, its weights summed in FP64 in entry order to wsum[r], the coarse self
-// loops (hl) and the distinct entries of every coarse row (dcount).  A block
-// per 4096-entry tile, 16 consecutive entries per thread; a run that spans
-// threads is finished by the thread that holds its head, which adds the
-// leading pieces of the threads after it.  A run still open at the tile's
-// end (or continuing one from an earlier tile) adds into wsum (zeroed
-// beforehand) with an atomic; every other run is stored once.
+__device__ __forceinline__ double tx_seg_sum(double v, int64_t seg) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double u = __shfl_up_sync(full, v, o);
+    const int64_t t = __shfl_up_sync(full, seg, o);
+    if (lane >= o && t == seg) v = __dadd_rn(v, u);
+  }
+  return v;
+}
+
+__device__ __forceinline__ bool tx_seg_last(int64_t seg, bool valid) {
+  const unsigned full = 0xffffffffu;
+  const int64_t nx = __shfl_down_sync(full, seg, 1);
+  const bool nvalid = __shfl_down_sync(full, valid, 1);
+  return valid && ((threadIdx.x & 31) == 31 || !nvalid || nx != seg);
+}
+
+struct TxEmitSmem {
+  uint64_t key[kIcChunk];     // key of the tile's i-th distinct entry
+  double sum[kIcChunk];       // its summed weight; -1: the run is still open at the tile's end
+  uint16_t lp[kIcChunk];      // coarse self loops among the tile's distinct entries before it
+  double lead[kTxThreads];    // sum of a thread's entries before its first head
+  uint8_t anyhead[kTxThreads];
+};
+
+__device__ __forceinline__ uint32_t tx_lo(int64_t x) { return (uint32_t)((uint64_t)x & 0xffffffffull); }
+__device__ __forceinline__ uint32_t tx_hi(int64_t x) { return (uint32_t)((uint64_t)x >> 32); }
+
+// One coarse entry (row a, column b, float weight wf) at distinct index r
+// with `lb` self loops before it into the next level's CSR: a loop sets the
+// row's loop weight, any other entry goes to position r - lb (weight doubled:
+// the merged doubled list holds each entry twice).  The row's degree, summed
+// over the lanes of the warp with the same row, is added by the caller.
+__device__ __forceinline__ double tx_csr_entry(const IcCsrOut& O, int32_t a, int32_t b, float wf, int64_t r,
+                                               int64_t lb) {
+  const bool loop = a == b;
+  if (loop) {
+    O.loopw[a] = wf;
+    O.has_loop[a] = 1;
+  } else {
+    O.col[r - lb] = b;
+    O.cw[r - lb] = __double2float_rn(__dadd_rn((double)wf, (double)wf));
+  }
+  float f = wf == 0.0f ? 1.0f : wf;   // InitKernel.cu:154-179: weight 0 counts 1, a loop twice
+  if (loop) f *= 2.0f;
+  return __dadd_rn((double)f, (double)f);
+}
+
+// Each run of equal keys once, a block per 4096-entry tile, 16 consecutive
+// entries per thread.  A thread sums the runs that start in its entries in
+// entry order (FP64); a run that goes on past the thread is finished by the
+// thread holding its head, which adds the leading pieces of the threads after
+// it.  The tile's distinct entries are staged in shared memory and written in
+// order: (osrc, odst), the float weight, the coarse self loops (hl), the
+// distinct entries per row (dcount) and, with O.col, the next level's CSR
+// entry and the row degrees.  The tile's last run, when it goes on into the
+// next tiles, is summed with atomics into opensum[tile] (its continuations
+// find the tile by a binary search) and finished by tx_open_kernel.
 __global__ void __launch_bounds__(kTxThreads) tx_emit_kernel(const uint64_t* k, const float* v, int64_t n, int Bb,
-                                                             const uint32_t* tbase, int32_t* osrc, int32_t* odst,
-                                                             double* wsum, uint32_t* hl, uint32_t* dcount) {
-  __shared__ double lead[kTxThreads];     // sum of the entries before the thread's first head
-  __shared__ uint8_t anyhead[kTxThreads];
+                                                             const int64_t* tscan, int32_t* osrc, int32_t* odst,
+                                                             float* ow, double* opensum, uint32_t* openflag,
+                                                             uint32_t* hl, uint32_t* dcount, IcCsrOut O) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TxEmitSmem& S = *reinterpret_cast<TxEmitSmem*>(smem_raw);
   const uint64_t mask = (1ull << Bb) - 1ull;
   const int t = threadIdx.x;
-  const int64_t i0 = blockIdx.x * (int64_t)kIcChunk + (int64_t)t * kTxItems;
+  const int64_t tile = blockIdx.x;
+  const int64_t i0 = tile * kIcChunk + (int64_t)t * kTxItems;
   uint64_t kk[kTxItems];
   float vv[kTxItems];
   const int m = tx_load16(k, v, i0, n, kk, vv);
   uint64_t prev = (i0 > 0 && m > 0) ? k[i0 - 1] : ~0ull;
-  uint32_t hmask = 0;
+  uint32_t hmask = 0, nloop = 0;
 #pragma unroll
   for (int i = 0; i < kTxItems; ++i) {
-    if (i < m && (i0 + i == 0 || kk[i] != prev)) hmask |= 1u << i;
+    if (i < m && (i0 + i == 0 || kk[i] != prev)) {
+      hmask |= 1u << i;
+      nloop += (kk[i] >> Bb) == (kk[i] & mask) ? 1u : 0u;
+    }
     prev = kk[i];
   }
-  uint32_t tot;
-  const uint32_t excl = block_exclusive_scan256<uint32_t>((uint32_t)__popc(hmask), &tot);
-  const int64_t rbase = (int64_t)tbase[blockIdx.x] + excl;   // distinct index of this thread's first head
-  // leading piece, complete runs, trailing run
+  unsigned long long both;
+  const unsigned long long ex =
+      block_exclusive_scan256<unsigned long long>(((unsigned long long)nloop << 32) | (uint32_t)__popc(hmask), &both);
+  const uint32_t tot = (uint32_t)both;
+  int loc = (int)(uint32_t)ex - 1;
+  uint32_t lc = (uint32_t)(ex >> 32);   // self loops among the tile's distinct entries before the next head
   double s = 0.0;
-  int64_t r = rbase - 1;
-  int32_t rowa = -1;
-  uint32_t rowcnt = 0;
   bool started = false;
 #pragma unroll
   for (int i = 0; i < kTxItems; ++i) {
     if (i < m) {
       if ((hmask >> i) & 1u) {
-        if (started) wsum[r] = s;                         // a run that began and ended in this thread
-        else lead[t] = s;
+        if (started) S.sum[loc] = s;   // a run that began and ended in this thread
+        else S.lead[t] = s;
         started = true;
-        ++r;
+        ++loc;
+        S.key[loc] = kk[i];
+        S.lp[loc] = (uint16_t)lc;
+        lc += (kk[i] >> Bb) == (kk[i] & mask) ? 1u : 0u;
         s = (double)vv[i];
-        const int32_t a = (int32_t)(kk[i] >> Bb), b = (int32_t)(kk[i] & mask);
-        osrc[r] = a;
-        odst[r] = b;
-        if (a == b) hl[a] = 1u;
-        if (a != rowa) {
-          if (rowcnt) atomicAdd(&dcount[rowa], rowcnt);
-          rowa = a;
-          rowcnt = 0;
-        }
-        ++rowcnt;
       } else {
         s = __dadd_rn(s, (double)vv[i]);
       }
     }
   }
-  if (rowcnt) atomicAdd(&dcount[rowa], rowcnt);
-  if (!started) lead[t] = s;
-  anyhead[t] = started ? 1 : 0;
+  if (!started) S.lead[t] = s;
+  S.anyhead[t] = started ? 1 : 0;
   __syncthreads();
-  // thread 0: entries before the tile's first head continue a run of an
-  // earlier tile; they and the leading pieces after them add to it
+  const int64_t tb = tx_lo(tscan[tile]);
   if (t == 0 && m > 0 && !(hmask & 1u)) {
+    // entries before the tile's first head continue the last run of an
+    // earlier tile h: the run with distinct index tb - 1
     double x = 0.0;
     for (int u = 0; u < kTxThreads; ++u) {
-      x = __dadd_rn(x, lead[u]);
-      if (anyhead[u]) break;
+      x = __dadd_rn(x, S.lead[u]);
+      if (S.anyhead[u]) break;
     }
-    atomicAdd(&wsum[(int64_t)tbase[blockIdx.x] - 1], x);
+    int64_t lo = tile - 1, hi = tile - 1;   // last tile whose first distinct index is <= tb - 1
+    if ((int64_t)tx_lo(tscan[lo]) > tb - 1) lo = 0;   // the previous tile holds no head: search
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if ((int64_t)tx_lo(tscan[mid]) <= tb - 1) lo = mid; else hi = mid - 1;
+    }
+    atomicAdd(&opensum[lo], x);
   }
-  // the trailing run of this thread takes the leading pieces of the threads
-  // after it, up to the next thread with a head
-  if (started) {
+  if (started) {   // the thread's last run takes the leading pieces after it
     double x = s;
     bool open = true;
     for (int u = t + 1; u < kTxThreads; ++u) {
-      x = __dadd_rn(x, lead[u]);
-      if (anyhead[u]) { open = false; break; }
+      x = __dadd_rn(x, S.lead[u]);
+      if (S.anyhead[u]) { open = false; break; }
     }
-    if (open) atomicAdd(&wsum[r], x);
-    else wsum[r] = x;
+    if (open && i0 + kIcChunk - (int64_t)t * kTxItems < n) {   // goes on into the next tile
+      atomicAdd(&opensum[tile], x);
+      openflag[tile] = 1u;
+      S.sum[loc] = -1.0;
+    } else {
+      S.sum[loc] = x;
+    }
+  }
+  __syncthreads();
+  // the tile's distinct entries, in order
+  const int64_t lt = tx_hi(tscan[tile]);
+  const int lane = t & 31;
+  for (uint32_t l0 = 0; l0 < tot; l0 += kTxThreads) {
+    const uint32_t l = l0 + t;
+    const bool valid = l < tot;
+    const int64_t r = tb + l;
+    int32_t a = -1, b = 0;
+    double x = -1.0;
+    if (valid) {
+      const uint64_t key = S.key[l];
+      a = (int32_t)(key >> Bb);
+      b = (int32_t)(key & mask);
+      x = S.sum[l];
+      osrc[r] = a;
+      odst[r] = b;
+      if (a == b) hl[a] = 1u;
+    }
+    const bool closed = valid && x >= 0.0;
+    const float wf = closed ? __double2float_rn(x) : 0.0f;
+    if (closed) ow[r] = wf;
+    // distinct entries per row: lanes of one row are consecutive
+    const int32_t ap = __shfl_up_sync(0xffffffffu, a, 1);
+    const unsigned starts = __ballot_sync(0xffffffffu, valid && (lane == 0 || ap != a));
+    const bool last = tx_seg_last(a, valid);
+    if (last) {
+      const int first = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
+      atomicAdd(&dcount[a], (uint32_t)(lane - first + 1));
+    }
+    if (O.col) {
+      const double kd = closed ? tx_csr_entry(O, a, b, wf, r, lt + (valid ? S.lp[l] : 0)) : 0.0;
+      const double ks = tx_seg_sum(kd, a);
+      if (last && ks != 0.0) atomicAdd(&O.k[a], ks);
+    }
   }
 }
 
-// Float weight of every distinct entry and, with a CSR to write, its CSR
-// entry and its row's degree (list position = distinct index).  Four
-// entries per thread in flight; grid-stride over whole warps.
-__global__ void tx_out_kernel(int64_t n, const int32_t* osrc, const int32_t* odst, const double* wsum, float* ow,
-                              IcCsrOut O) {
-  constexpr int U = 4;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x * U;
-  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x * U; i0 < n; i0 += stride) {
-    int32_t a[U], b[U];
-    float wf[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t i = i0 + (int64_t)u * blockDim.x + threadIdx.x;
-      const bool valid = i < n;
-      a[u] = valid ? osrc[i] : -1;
-      b[u] = valid ? odst[i] : 0;
-      wf[u] = valid ? __double2float_rn(wsum[i]) : 0.0f;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t i = i0 + (int64_t)u * blockDim.x + threadIdx.x;
-      if (i < n) ow[i] = wf[u];
-      if (O.col) ic_emit_csr(O, i < n, a[u], b[u], wf[u], (uint64_t)i);
+// The runs left open at a tile's end: their final sums, float weights and
+// CSR entries (one thread per tile).
+__global__ void tx_open_kernel(int64_t ntiles, const int64_t* tscan, const double* opensum, const uint32_t* openflag,
+                               const int32_t* osrc, const int32_t* odst, float* ow, IcCsrOut O) {
+  IC_FOR(h, ntiles) {
+    if (!openflag[h]) continue;
+    const int64_t r = (int64_t)tx_lo(tscan[h + 1]) - 1;   // the tile's last run
+    const float wf = __double2float_rn(opensum[h]);
+    ow[r] = wf;
+    if (O.col) {
+      const int32_t a = osrc[r], b = odst[r];
+      const int64_t lb = (int64_t)tx_hi(tscan[h + 1]) - (a == b ? 1 : 0);
+      atomicAdd(&O.k[a], tx_csr_entry(O, a, b, wf, r, lb));
     }
   }
 }
@@ -1028,6 +1112,8 @@ void tx_attributes() {
   std::lock_guard<std::mutex> lock(mu);
   if (dev >= 0 && dev < kDevs && done[dev]) return;
   LVG_CUDA(cudaFuncSetAttribute(tx_layout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TxSmem)));
+  LVG_CUDA(cudaFuncSetAttribute(tx_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TxEmitSmem)));
   if (dev >= 0 && dev < kDevs) done[dev] = true;
 }
 
@@ -1040,7 +1126,7 @@ size_t induce_transposed_scratch(int64_t V, int64_t E, int64_t C) {
   b += (size_t)V * (2 * 12 + 4 + 4 + 4 + 8) + 8 * 256 * (size_t)(V / 4096 + 2);   // member sort, scans
   b += (size_t)(nchunks + 1) * 4;                                                  // chunk first members
   b += (size_t)E * (2 * 12) + 8 * 256 * (size_t)(E / 4096 + 2);                   // keys, weights, look-back
-  b += (size_t)E * 8 + 16 * (size_t)(E / 2048 + 2);                              // run sums, tile counts
+  b += 32 * (size_t)(E / 4096 + 2);                                                // tile counts, open runs
   b += (size_t)C * 16 + 64;                                                        // loops, counts, offsets
   return b + ((size_t)64 << 10) * 32;                                              // alignment slack
 }
@@ -1095,42 +1181,43 @@ bool induce_transposed(const LevelGraph& g, const int32_t* part, int32_t C, int3
   const int w2 = radix_sort_pairs_range(k0, v0, k1, v1, E, Bb, Bb, a, s);
   const uint64_t* keys = w2 ? k1 : k0;
   const float* vals = w2 ? v1 : v0;
-  // runs of equal keys: heads per 4096-entry tile, their scan, every run once
-  uint32_t* tcount = a.hi_n<uint32_t>(nchunks + 1);
-  tx_count_kernel<<<(unsigned)nchunks, kTxThreads, 0, s>>>(keys, E, tcount);
+  // runs of equal keys: heads (and self-loop heads) per 4096-entry tile,
+  // their scan, then every run once
+  int64_t* tscan = a.hi_n<int64_t>(nchunks + 1);
+  tx_count_kernel<<<(unsigned)nchunks, kTxThreads, 0, s>>>(keys, E, Bb, tscan);
   LVG_LAUNCH();
-  scan_u32(tcount, tcount, nchunks, a, s);
-  const int64_t cnt = read_back(tcount + nchunks, s);
+  scan_i64(tscan, tscan, nchunks, a, s);
+  const int64_t cnt = (int64_t)((uint64_t)read_back(tscan + nchunks, s) & 0xffffffffull);
   const bool int_weights = read_back(flags, s) == 0u;
-  double* wsum = a.hi_n<double>(cnt);
+  double* opensum = a.hi_n<double>(nchunks);
+  uint32_t* openflag = a.hi_n<uint32_t>(nchunks);
   uint32_t* hl = a.hi_n<uint32_t>((int64_t)C + 1);
   uint32_t* dcount = a.hi_n<uint32_t>((int64_t)C + 1);
-  LVG_CUDA(cudaMemsetAsync(wsum, 0, sizeof(double) * (size_t)cnt, s));
+  LVG_CUDA(cudaMemsetAsync(opensum, 0, sizeof(double) * (size_t)nchunks, s));
+  LVG_CUDA(cudaMemsetAsync(openflag, 0, sizeof(uint32_t) * (size_t)nchunks, s));
   LVG_CUDA(cudaMemsetAsync(hl, 0, sizeof(uint32_t) * ((size_t)C + 1), s));
   LVG_CUDA(cudaMemsetAsync(dcount, 0, sizeof(uint32_t) * ((size_t)C + 1), s));
-  tx_emit_kernel<<<(unsigned)nchunks, kTxThreads, 0, s>>>(keys, vals, E, Bb, tcount, osrc, odst, wsum, hl, dcount);
-  LVG_LAUNCH();
   // The CSR is written only for integral weights: then every sum is exact,
   // so the coarse list is exactly symmetric, as the CSR written from one
   // direction assumes.
   IcCsrOut O{};
-  uint32_t* segoff = nullptr;
-  uint32_t* loopx = nullptr;
-  if (next && next->col && int_weights) {
-    segoff = a.hi_n<uint32_t>((int64_t)C + 1);
-    loopx = a.hi_n<uint32_t>((int64_t)C + 1);
-    scan_u32(dcount, segoff, C, a, s);
-    scan_u32(hl, loopx, C, a, s);
+  const bool csr = next && next->col && int_weights;
+  if (csr) {
     LVG_CUDA(cudaMemsetAsync(next->k, 0, sizeof(double) * (size_t)C, s));
     LVG_CUDA(cudaMemsetAsync(next->loopw, 0, sizeof(float) * (size_t)C, s));
     LVG_CUDA(cudaMemsetAsync(next->has_loop, 0, (size_t)C, s));
-    O = IcCsrOut{next->col, next->cw, next->k, next->loopw, next->has_loop, hl, loopx};
+    O = IcCsrOut{next->col, next->cw, next->k, next->loopw, next->has_loop, hl, nullptr};
   }
-  if (cnt > 0) {
-    tx_out_kernel<<<ic_grid((cnt + 3) / 4), kIcFlat, 0, s>>>(cnt, osrc, odst, wsum, ow, O);
-    LVG_LAUNCH();
-  }
-  if (O.col) {   // the rest of the next level's CSR: row offsets, entry count, m
+  tx_emit_kernel<<<(unsigned)nchunks, kTxThreads, sizeof(TxEmitSmem), s>>>(keys, vals, E, Bb, tscan, osrc, odst, ow,
+                                                                           opensum, openflag, hl, dcount, O);
+  LVG_LAUNCH();
+  tx_open_kernel<<<ic_grid(nchunks), kIcFlat, 0, s>>>(nchunks, tscan, opensum, openflag, osrc, odst, ow, O);
+  LVG_LAUNCH();
+  if (csr) {   // the rest of the next level's CSR: row offsets, entry count, m
+    uint32_t* segoff = a.hi_n<uint32_t>((int64_t)C + 1);
+    uint32_t* loopx = a.hi_n<uint32_t>((int64_t)C + 1);
+    scan_u32(dcount, segoff, C, a, s);
+    scan_u32(hl, loopx, C, a, s);
     ic_csr_off_kernel<<<ic_grid((int64_t)C + 1), kIcFlat, 0, s>>>(C, segoff, loopx, next->off);
     LVG_LAUNCH();
     double* d_m = a.hi_n<double>(1);
