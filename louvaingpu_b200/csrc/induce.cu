@@ -764,7 +764,9 @@ struct TxSmem {
   int32_t yc[kIcChunk + 1];
 };
 
-// Keys (part[d] << Bb | part[u]) and weights (0 counted as 1) of the entries
+// Keys (dense community of d << Bb | community of u: the caller passes the
+// dense ids of the vertices as `part`) and weights (0 counted as 1) of the
+// entries
 // in segment order, a block per 4096 positions.  The chunk's members are
 // staged in shared memory; a thread takes 16 positions 256 apart, finds the
 // member of each by a binary search, then issues all 16 list loads and all
@@ -882,12 +884,13 @@ __device__ __forceinline__ int tx_load16(const uint64_t* k, const float* v, int6
   return m;
 }
 
-// Runs of equal keys, per 4096-entry tile of the sorted keys: the number of
-// run heads (first entries; low 32 bits) and of heads that are coarse self
-// loops (high 32 bits), so that one scan gives every run its distinct index
-// and the self loops before it.
+// Runs of equal keys (dense first community << Bb | second community), per
+// 4096-entry tile of the sorted keys: the number of run heads (first entries;
+// low 32 bits) and of heads that are coarse self loops (high 32 bits), so
+// that one scan gives every run its distinct index and the self loops before
+// it.
 __global__ void __launch_bounds__(kTxThreads) tx_count_kernel(const uint64_t* k, int64_t n, int Bb,
-                                                              int64_t* tcount) {
+                                                              const int32_t* und, int64_t* tcount) {
   const uint64_t mask = (1ull << Bb) - 1ull;
   const int64_t i0 = blockIdx.x * (int64_t)kIcChunk + (int64_t)threadIdx.x * kTxItems;
   uint64_t kk[kTxItems];
@@ -897,7 +900,8 @@ __global__ void __launch_bounds__(kTxThreads) tx_count_kernel(const uint64_t* k,
   unsigned long long cnt = 0;
 #pragma unroll
   for (int i = 0; i < kTxItems; ++i) {
-    if (i < m && (i0 + i == 0 || kk[i] != prev)) cnt += ((kk[i] >> Bb) == (kk[i] & mask)) ? (1ull << 32) + 1ull : 1ull;
+    if (i < m && (i0 + i == 0 || kk[i] != prev))
+      cnt += ((uint64_t)und[(int32_t)(kk[i] >> Bb)] == (kk[i] & mask)) ? (1ull << 32) + 1ull : 1ull;
     prev = kk[i];
   }
   unsigned long long tot;
@@ -955,7 +959,8 @@ __device__ __forceinline__ double tx_csr_entry(const IcCsrOut& O, int32_t a, int
   return __dadd_rn((double)f, (double)f);
 }
 
-// Each run of equal keys once, a block per 4096-entry tile, 16 consecutive
+// Each run of equal keys (dense first community, mapped back by und; the
+// second community as it is) once, a block per 4096-entry tile, 16 consecutive
 // entries per thread.  A thread sums the runs that start in its entries in
 // entry order (FP64); a run that goes on past the thread is finished by the
 // thread holding its head, which adds the leading pieces of the threads after
@@ -966,9 +971,10 @@ __device__ __forceinline__ double tx_csr_entry(const IcCsrOut& O, int32_t a, int
 // next tiles, is summed with atomics into opensum[tile] (its continuations
 // find the tile by a binary search) and finished by tx_open_kernel.
 __global__ void __launch_bounds__(kTxThreads) tx_emit_kernel(const uint64_t* k, const float* v, int64_t n, int Bb,
-                                                             const int64_t* tscan, int32_t* osrc, int32_t* odst,
-                                                             float* ow, double* opensum, uint32_t* openflag,
-                                                             uint32_t* hl, uint32_t* dcount, IcCsrOut O) {
+                                                             const int64_t* tscan, const int32_t* und,
+                                                             int32_t* osrc, int32_t* odst, float* ow, double* opensum,
+                                                             uint32_t* openflag, uint32_t* hl, uint32_t* dcount,
+                                                             IcCsrOut O) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TxEmitSmem& S = *reinterpret_cast<TxEmitSmem*>(smem_raw);
   const uint64_t mask = (1ull << Bb) - 1ull;
@@ -984,7 +990,7 @@ __global__ void __launch_bounds__(kTxThreads) tx_emit_kernel(const uint64_t* k, 
   for (int i = 0; i < kTxItems; ++i) {
     if (i < m && (i0 + i == 0 || kk[i] != prev)) {
       hmask |= 1u << i;
-      nloop += (kk[i] >> Bb) == (kk[i] & mask) ? 1u : 0u;
+      nloop += (uint64_t)und[(int32_t)(kk[i] >> Bb)] == (kk[i] & mask) ? 1u : 0u;
     }
     prev = kk[i];
   }
@@ -1006,7 +1012,7 @@ __global__ void __launch_bounds__(kTxThreads) tx_emit_kernel(const uint64_t* k, 
         ++loc;
         S.key[loc] = kk[i];
         S.lp[loc] = (uint16_t)lc;
-        lc += (kk[i] >> Bb) == (kk[i] & mask) ? 1u : 0u;
+        lc += (uint64_t)und[(int32_t)(kk[i] >> Bb)] == (kk[i] & mask) ? 1u : 0u;
         s = (double)vv[i];
       } else {
         s = __dadd_rn(s, (double)vv[i]);
@@ -1060,7 +1066,7 @@ __global__ void __launch_bounds__(kTxThreads) tx_emit_kernel(const uint64_t* k, 
     double x = -1.0;
     if (valid) {
       const uint64_t key = S.key[l];
-      a = (int32_t)(key >> Bb);
+      a = und[(int32_t)(key >> Bb)];
       b = (int32_t)(key & mask);
       x = S.sum[l];
       osrc[r] = a;
@@ -1103,6 +1109,31 @@ __global__ void tx_open_kernel(int64_t ntiles, const int64_t* tscan, const doubl
   }
 }
 
+// Dense ids of the communities that have entries (members 0 .. nz - 1 are
+// sorted by community), mapped both ways.
+// Sorting by dense ids needs bits for these communities only; the first
+// level of a graph with many isolated vertices has far fewer of them than
+// communities.
+__global__ void tx_dense_flag_kernel(int32_t nz, const int32_t* mcomm, uint32_t* flag) {
+  IC_FOR(i, nz) flag[i] = (i == 0 || mcomm[i] != mcomm[i - 1]) ? 1u : 0u;
+}
+
+__global__ void tx_dense_kernel(int32_t nz, const int32_t* mcomm, const uint32_t* ex, int32_t* dn, int32_t* und) {
+  IC_FOR(i, nz) {
+    if (i == 0 || mcomm[i] != mcomm[i - 1]) {
+      dn[mcomm[i]] = (int32_t)ex[i];
+      und[ex[i]] = mcomm[i];
+    }
+  }
+}
+
+// Dense community id of every vertex with entries (the only vertices that
+// appear as a neighbour); 0 for the others, which are never read.
+__global__ void tx_vdense_kernel(int32_t V, const int32_t* part, const int64_t* off, const uint8_t* has_loop,
+                                 const int32_t* dn, int32_t* pd) {
+  IC_FOR(v, V) pd[v] = (off[v + 1] > off[v] || has_loop[v]) ? dn[part[v]] : 0;
+}
+
 void tx_attributes() {
   constexpr int kDevs = 64;
   static std::mutex mu;
@@ -1127,6 +1158,7 @@ size_t induce_transposed_scratch(int64_t V, int64_t E, int64_t C) {
   b += (size_t)(nchunks + 1) * 4;                                                  // chunk first members
   b += (size_t)E * (2 * 12) + 8 * 256 * (size_t)(E / 4096 + 2);                   // keys, weights, look-back
   b += 32 * (size_t)(E / 4096 + 2);                                                // tile counts, open runs
+  b += (size_t)V * 16 + (size_t)C * 8;                                             // dense community ids
   b += (size_t)C * 16 + 64;                                                        // loops, counts, offsets
   return b + ((size_t)64 << 10) * 32;                                              // alignment slack
 }
@@ -1141,7 +1173,6 @@ bool induce_transposed(const LevelGraph& g, const int32_t* part, int32_t C, int3
   if (E == 0) { *count = 0; return true; }
   HiScope hs(a);
   const int64_t nchunks = (E + kIcChunk - 1) / kIcChunk;
-  const int Bb = std::max(1, bits_for(C));
   // members in community order (stable: vertex order inside a community)
   uint64_t* mk0 = a.hi_n<uint64_t>(V);
   float* mv0 = a.hi_n<float>(V);
@@ -1166,6 +1197,21 @@ bool induce_transposed(const LevelGraph& g, const int32_t* part, int32_t C, int3
   int32_t* cfirst = a.hi_n<int32_t>(nchunks + 1);
   ic_chunk_first_kernel<<<ic_grid(V), kIcFlat, 0, s>>>(mscan, nz, cfirst, nchunks);
   LVG_LAUNCH();
+  // dense ids of the communities with entries: the sort needs their bits only
+  uint32_t* dflag = a.hi_n<uint32_t>(h_nz + 1);
+  int32_t* dn = a.hi_n<int32_t>(C);
+  int32_t* und = a.hi_n<int32_t>(C);
+  int32_t* pd = a.hi_n<int32_t>(V);
+  tx_dense_flag_kernel<<<ic_grid(h_nz), kIcFlat, 0, s>>>(h_nz, mcomm, dflag);
+  LVG_LAUNCH();
+  scan_u32(dflag, dflag, h_nz, a, s);
+  tx_dense_kernel<<<ic_grid(h_nz), kIcFlat, 0, s>>>(h_nz, mcomm, dflag, dn, und);
+  LVG_LAUNCH();
+  tx_vdense_kernel<<<ic_grid(V), kIcFlat, 0, s>>>(V, part, g.off, g.has_loop, dn, pd);
+  LVG_LAUNCH();
+  const int64_t ndense = read_back(dflag + h_nz, s);
+  const int Bb = std::max(1, bits_for(C));            // second community, as it is
+  const int Bd = std::max(1, bits_for(ndense));       // first community, dense: the sort key
   // keys in segment order, then one stable sort by the first community
   uint64_t* k0 = a.hi_n<uint64_t>(E);
   float* v0 = a.hi_n<float>(E);
@@ -1175,16 +1221,16 @@ bool induce_transposed(const LevelGraph& g, const int32_t* part, int32_t C, int3
   LVG_CUDA(cudaMemsetAsync(flags, 0, sizeof(uint32_t), s));
   tx_attributes();
   tx_layout_kernel<<<(unsigned)nchunks, kTxThreads, sizeof(TxSmem), s>>>(E, h_nz, Bb, mem, mcomm, mscan, cfirst,
-                                                                         g.off, lscan, g.dst, g.w, part, k0, v0,
+                                                                         g.off, lscan, g.dst, g.w, pd, k0, v0,
                                                                          flags);
   LVG_LAUNCH();
-  const int w2 = radix_sort_pairs_range(k0, v0, k1, v1, E, Bb, Bb, a, s);
+  const int w2 = radix_sort_pairs_range(k0, v0, k1, v1, E, Bb, Bd, a, s);
   const uint64_t* keys = w2 ? k1 : k0;
   const float* vals = w2 ? v1 : v0;
   // runs of equal keys: heads (and self-loop heads) per 4096-entry tile,
   // their scan, then every run once
   int64_t* tscan = a.hi_n<int64_t>(nchunks + 1);
-  tx_count_kernel<<<(unsigned)nchunks, kTxThreads, 0, s>>>(keys, E, Bb, tscan);
+  tx_count_kernel<<<(unsigned)nchunks, kTxThreads, 0, s>>>(keys, E, Bb, und, tscan);
   LVG_LAUNCH();
   scan_i64(tscan, tscan, nchunks, a, s);
   const int64_t cnt = (int64_t)((uint64_t)read_back(tscan + nchunks, s) & 0xffffffffull);
@@ -1208,8 +1254,9 @@ bool induce_transposed(const LevelGraph& g, const int32_t* part, int32_t C, int3
     LVG_CUDA(cudaMemsetAsync(next->has_loop, 0, (size_t)C, s));
     O = IcCsrOut{next->col, next->cw, next->k, next->loopw, next->has_loop, hl, nullptr};
   }
-  tx_emit_kernel<<<(unsigned)nchunks, kTxThreads, sizeof(TxEmitSmem), s>>>(keys, vals, E, Bb, tscan, osrc, odst, ow,
-                                                                           opensum, openflag, hl, dcount, O);
+  tx_emit_kernel<<<(unsigned)nchunks, kTxThreads, sizeof(TxEmitSmem), s>>>(keys, vals, E, Bb, tscan, und, osrc,
+                                                                           odst, ow, opensum, openflag, hl, dcount,
+                                                                           O);
   LVG_LAUNCH();
   tx_open_kernel<<<ic_grid(nchunks), kIcFlat, 0, s>>>(nchunks, tscan, opensum, openflag, osrc, odst, ow, O);
   LVG_LAUNCH();
