@@ -110,10 +110,21 @@ def make_case(gen, case):
         hd = np.concatenate([leaves, np.zeros(12000, np.int32), mid, np.full(600, 12500, np.int32)])
         hw = np.ones(len(hs), np.float32) * 2
         return n, np.concatenate([s, hs]), np.concatenate([d, hd]), np.concatenate([w, hw])
+    if case == "bighub":
+        # a hub of degree 400,000 (512 aggregation buckets: a thread per
+        # bucket slice) over leaves on a ring, integer weights 1..3
+        n = 450000
+        rng = np.random.default_rng(8)
+        leaves = np.arange(1, 400001, dtype=np.int32)
+        ring = np.roll(leaves, 1)
+        u = np.concatenate([np.zeros(len(leaves), np.int32), leaves])
+        v = np.concatenate([leaves, ring])
+        w = rng.integers(1, 4, len(u)).astype(np.float32)
+        return n, np.concatenate([u, v]), np.concatenate([v, u]), np.concatenate([w, w])
     raise ValueError(case)
 
 
-@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "odd_sizes", "hub"])
+@pytest.mark.parametrize("case", ["sbm_small", "weighted", "loops_zeros_isolated", "odd_sizes", "hub", "bighub"])
 def test_move_decisions_bit_exact(Louvain, oracle, gen, case):
     n, s, d, w = make_case(gen, case)
     oc = oracle.Csr(n, s, d, w)
