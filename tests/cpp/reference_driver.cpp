@@ -2,6 +2,9 @@
 // and generate_dendogram do (LouvainCPP.cpp:209-553, 739-806).
 //   reference_driver <dir> run    -> whole dendrogram through generate_dendogram
 //   reference_driver <dir> steps  -> the phase functions called one by one
+//   reference_driver <dir> float  -> the same through the shim's float phase
+//                                    functions, as a relinked reference driver
+//                                    calls them (LouvainCPP.cpp:356-470)
 // Reads <dir>/nodes.txt and <dir>/edges.txt; prints one line per level:
 //   level <l> <count> then "node:community" pairs, and "communities <n>".
 #include <cstdio>
@@ -31,6 +34,33 @@ int main(int argc, char** argv) {
   if (std::strcmp(argv[2], "run") == 0) {
     std::map<int, std::pair<int, float>> init;
     dendogram = generate_dendogram(graph, init);
+  } else if (std::strcmp(argv[2], "float") == 0) {
+    // modularity values as floats end to end: the floor handed to each
+    // one-level phase and the level break are the float ones
+    StatusCUDA status;
+    CUDAGraph cuGraph;
+    CUDPPHandle handle = nullptr;
+    AllocateMemory(status, graph, cuGraph);
+    handle = status.ctx;
+    CalculateNeighbour(status, cuGraph);
+    initCUDA(status, cuGraph);
+    float mod = modularityCUDA(status, graph.getNodeSize());
+    float next = oneLevelCUDA(status, cuGraph.nodesSize, cuGraph.nrOfAllNeighbours, cuGraph.edgeSize * 2, mod);
+    Partition first = renumberCUDA(handle, status);
+    dendogram.push_back(first);
+    mod = next;
+    inducedGraphCUDA(handle, status, cuGraph, first);
+    for (;;) {
+      CalculateNeighbour(status, cuGraph);
+      initCUDA(status, cuGraph);
+      next = oneLevelCUDA(status, cuGraph.nodesSize, cuGraph.nrOfAllNeighbours, cuGraph.edgeSize * 2, mod);
+      Partition p = renumberCUDA(handle, status);
+      dendogram.push_back(p);
+      if (next - mod < 1e-7f) break;
+      mod = next;
+      inducedGraphCUDA(handle, status, cuGraph, p);
+    }
+    DeAllocateMemory(status);
   } else {
     // LouvainCPP.cpp:334-507 with the reference's call sequence
     StatusCUDA status;

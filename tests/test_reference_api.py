@@ -84,9 +84,13 @@ def test_reference_driver_run_and_steps(tmp_path, oracle, gen):
     exe = build_driver(tmp_path)
     out_run = subprocess.check_output([exe, str(tmp_path), "run"], text=True)
     out_steps = subprocess.check_output([exe, str(tmp_path), "steps"], text=True)
+    out_float = subprocess.check_output([exe, str(tmp_path), "float"], text=True)
     lv_run, c_run = parse(out_run)
     lv_steps, c_steps = parse(out_steps)
     assert lv_run == lv_steps and c_run == c_steps
+    # the shim's float phase functions, called as the reference's level loop
+    # calls them, give the same dendrogram on this graph
+    assert parse(out_float) == (lv_run, c_run)
     orun = oracle.Run(n, s, d, w)
     assert len(lv_run) == len(orun.levels)
     # level 0 pairs: node ids grouped by the pre-renumbering label, index order inside a group
