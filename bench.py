@@ -184,25 +184,21 @@ class Clocks:
 
 
 def phase_roofline(levels, peak):
-    """Algorithmic bytes and achieved GB/s of the level phases of one run:
-    build 2*(8+4) B per doubled-list entry read and written + 8 B per vertex;
-    coarsening 12 B per entry read + 16 B per entry per radix pass + 12 B per
-    coarse entry written; renumbering 12 B per vertex."""
-    def bits(x):
-        b = 0
-        while (1 << b) < x:
-            b += 1
-        return b
+    """Algorithmic bytes and achieved GB/s of the level phases of one run, on
+    the least traffic each phase needs: the CSR build reads the level list
+    (12 B per entry) and writes the CSR (8 B per entry) and the per-vertex
+    offsets and degrees (16 B); the coarsening reads the level list (12 B per
+    entry) and writes the coarse list (12 B per coarse entry) and its CSR
+    (8 B per coarse entry); renumbering reads and writes 12 B per vertex."""
     tot = {"build": 0.0, "induce": 0.0, "renumber": 0.0}
     ms = {"build": 0.0, "induce": 0.0, "renumber": 0.0}
     for l, x in enumerate(levels):
-        tot["build"] += 24.0 * 2 * x.n_entries + 8.0 * x.n_vertices
+        tot["build"] += 20.0 * x.n_entries + 16.0 * x.n_vertices
         ms["build"] += x.ms_build
         tot["renumber"] += 12.0 * x.n_vertices
         ms["renumber"] += x.ms_renumber
         if l + 1 < len(levels):
-            passes = (2 * max(1, bits(x.n_comms)) + 7) // 8
-            tot["induce"] += 12.0 * x.n_entries + 16.0 * x.n_entries * passes + 12.0 * levels[l + 1].n_entries
+            tot["induce"] += 12.0 * x.n_entries + 20.0 * levels[l + 1].n_entries
             ms["induce"] += x.ms_induce
     out = {}
     for k in tot:
