@@ -164,6 +164,8 @@ void prepare_level(lvg_ctx* c) {
   drop_graphs(c);
   LVG_CUDA(cudaEventRecord(c->pev[0], c->stream));
   build_level(c->g, c->tune, c->arena, c->stream);
+  c->st.gid = nullptr;     // one graph (a batch that failed part-way may have left its maps)
+  c->st.gdone = nullptr;
   alloc_state(c->g, c->st, c->arena);
   init_state(c->g, c->st, 0.0, c->cfg.pass_min_gain, c->cfg.max_passes, c->arena, c->stream);
   LVG_CUDA(cudaEventRecord(c->pev[1], c->stream));   // read once the stream has synchronised

@@ -435,7 +435,36 @@ struct MoveArgs {
   const int32_t* k32;    // degrees as int32 (integral weights), else nullptr: the singleton tot
   const int32_t* gid;    // batched runs: graph of each vertex (nullptr for one graph)
   const int32_t* gdone;  // batched runs: 1 once a graph's level loop has stopped
+  unsigned long long* queue;   // batched runs: work counter of this launch (nullptr: grid-stride)
 };
+
+// Work items of the block-per-item kernels (block, tile and hub-bucket
+// classes).  Without a queue (one graph) a block takes items blockIdx.x,
+// blockIdx.x + gridDim.x, ...  With one (batched runs, whose graphs and rows
+// are of very uneven sizes) the blocks are persistent and pull kQueueGrab
+// consecutive items at a time from a device counter, so that a block that
+// finishes early takes more.  Every thread of the block calls these; the
+// decisions are the same whichever block takes an item.
+constexpr int kQueueGrab = 8;
+struct WorkQueue {
+  int64_t base, end;
+};
+__device__ __forceinline__ int64_t work_take(unsigned long long* q, WorkQueue& w) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    w.base = (int64_t)atomicAdd(q, (unsigned long long)kQueueGrab);
+    w.end = w.base + kQueueGrab;
+  }
+  __syncthreads();
+  return w.base;
+}
+__device__ __forceinline__ int64_t work_begin(unsigned long long* q, WorkQueue& w) {
+  return q ? work_take(q, w) : (int64_t)blockIdx.x;
+}
+__device__ __forceinline__ int64_t work_advance(unsigned long long* q, int64_t item, WorkQueue& w) {
+  if (!q) return item + gridDim.x;
+  return item + 1 < w.end ? item + 1 : work_take(q, w);
+}
 
 // Candidate order: higher gain first, then lower community id
 // (OneLevelKernel.cu:330,358).  Only strictly positive gains are candidates.
@@ -565,7 +594,8 @@ __global__ void __launch_bounds__(NT) move_block_kernel(MoveArgs P, int maxLog, 
   for (int s = threadIdx.x; s < Tmax; s += NT) { keys[s] = -1; vals[s] = Acc(0); }
   __syncthreads();
   bool overflow = false;
-  for (int64_t item = blockIdx.x; item < P.n; item += gridDim.x) {
+  __shared__ WorkQueue wq;
+  for (int64_t item = work_begin(P.queue, wq); item < P.n; item = work_advance(P.queue, item, wq)) {
     int32_t i = P.list[item];
     int64_t beg = P.off[i], end = P.off[i + 1];
     if (end - beg <= dlo || end - beg > dhi) continue;   // another band takes this degree
@@ -1126,7 +1156,8 @@ __global__ void __launch_bounds__(kThreads) move_tile_packed_kernel(MoveArgs P, 
   for (int sl = threadIdx.x; sl < kTileSlots; sl += kThreads) S.slot[sl] = kPackedEmpty;
   if (threadIdx.x == 0) S.nclaimed = 0;
   bool overflow = false;
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  __shared__ WorkQueue wq;
+  for (int64_t t = work_begin(P.queue, wq); t < ntiles; t = work_advance(P.queue, t, wq)) {
     const int vb = tile_start[t];
     const int nv = tile_start[t + 1] - vb;
     int deg = 0;
@@ -1590,7 +1621,8 @@ __global__ void __launch_bounds__(kThreads) hub_agg_kernel(MoveArgs P, HubArgs H
   AggCtl& S = *reinterpret_cast<AggCtl*>(smem + sizeof(AggTable<PACKED>));
   if (P.ctl->done) return;
   agg_init(T, S);
-  for (int64_t gb = blockIdx.x; gb < H.nbucket; gb += gridDim.x) {
+  __shared__ WorkQueue wq;
+  for (int64_t gb = work_begin(P.queue, wq); gb < H.nbucket; gb = work_advance(P.queue, gb, wq)) {
     const int32_t h = H.bucket_hub[gb];
     const int32_t b = (int32_t)(gb - H.hub_bb0[h]);
     const int32_t c0 = H.hub_cb0[h], K = H.hub_cb0[h + 1] - c0;
@@ -1957,6 +1989,7 @@ MoveArgs move_args(const LevelGraph& g, CommState& st) {
   P.k32 = g.k32;
   P.gid = st.gid;
   P.gdone = st.gdone;
+  P.queue = nullptr;
   return P;
 }
 
@@ -2386,6 +2419,7 @@ void alloc_state(const LevelGraph& g, CommState& st, Arena& a) {
   st.partials = a.lo_n<double>(st.ngroups);
   st.partials2 = a.lo_n<double>((st.ngroups + kGroup - 1) / kGroup);
   st.ctl = a.lo_n<PassCtl>(1);
+  st.queue = a.lo_n<unsigned long long>(kQueueSlots);
 }
 
 // Q of the committed state through the fixed tree into *dst.
@@ -2487,6 +2521,10 @@ static void launch_thread(const LevelGraph& g, MoveArgs P, int bucket, cudaStrea
 // classes run on side streams, forked from and joined back into `s`.
 void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const SideStreams* ss) {
   MoveArgs P = move_args(g, st);
+  // batched runs: the block-per-item kernels are persistent and pull their
+  // items from device counters (one per launch), zeroed before the fork
+  unsigned long long* q = (st.gid && st.queue) ? st.queue : nullptr;
+  if (q) LVG_CUDA(cudaMemsetAsync(q, 0, sizeof(unsigned long long) * kQueueSlots, s));
   cudaStream_t sh = s, sb = s, st2 = s;
   if (ss) {
     LVG_CUDA(cudaEventRecord(ss->fork, s));
@@ -2506,8 +2544,10 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     const size_t smem = g.int_acc ? agg_smem_bytes<true>() : agg_smem_bytes<false>();
     const int per_sm = std::max(1, std::min(8, (int)((227u * 1024u) / (smem + 1024))));
     const int64_t grid = std::min<int64_t>(g.nhub_bucket, (int64_t)sm_count() * per_sm);
-    if (g.int_acc) hub_agg_kernel<true><<<(unsigned)grid, kThreads, smem, sh>>>(P, H);
-    else hub_agg_kernel<false><<<(unsigned)grid, kThreads, smem, sh>>>(P, H);
+    MoveArgs PA = P;
+    PA.queue = q ? q + 0 : nullptr;
+    if (g.int_acc) hub_agg_kernel<true><<<(unsigned)grid, kThreads, smem, sh>>>(PA, H);
+    else hub_agg_kernel<false><<<(unsigned)grid, kThreads, smem, sh>>>(PA, H);
     LVG_LAUNCH();
     hub_decide_kernel<<<grid_for(nhub, 128), 128, 0, sh>>>(P, H, nhub);
     LVG_LAUNCH();
@@ -2518,7 +2558,9 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     Q.n = g.nbucket[kBBlock];
     // degree bands (lo, hi], hi = 1024, 2048, ..., each with a table of 2 hi slots
     int64_t lo = 0;
-    for (int64_t hi = 1024; lo < g.block_max; hi *= 2) {
+    int band = 0;
+    for (int64_t hi = 1024; lo < g.block_max; hi *= 2, ++band) {
+      Q.queue = q ? q + 2 + std::min(band, kQueueSlots - 3) : nullptr;
       const int64_t h = std::min<int64_t>(hi, g.block_max);
       int lg = 5;
       while (((int64_t)1 << lg) < 2 * h) ++lg;
@@ -2539,6 +2581,7 @@ void launch_moves(const LevelGraph& g, CommState& st, cudaStream_t s, const Side
     Q.list = g.blist + g.bstart[kBTile];
     Q.n = g.nbucket[kBTile];
     if (g.int_acc && g.V <= kTilePackedMaxComm) {
+      Q.queue = q ? q + 1 : nullptr;
       const size_t smem = sizeof(TilePackedSmem);
       const int per_sm = std::max(1, std::min(8, (int)((227u * 1024u) / (smem + 1024))));
       const int64_t grid = std::min<int64_t>(g.ntiles, (int64_t)sm_count() * per_sm);

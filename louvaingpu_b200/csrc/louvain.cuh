@@ -134,7 +134,9 @@ struct CommState {
   size_t hot_bytes = 0;           // tot | comm | size, contiguous from tot
   const int32_t* gid = nullptr;   // batched runs: graph of each vertex
   int32_t* gdone = nullptr;       // batched runs: per-graph stop flags
+  unsigned long long* queue = nullptr;   // work counters of the persistent move kernels (batched runs)
 };
+constexpr int kQueueSlots = 8;    // hub buckets, tiles, up to six block-class degree bands
 
 struct Tuning {
   int32_t warp_max = 512;         // largest degree packed into tiles

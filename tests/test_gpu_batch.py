@@ -67,6 +67,19 @@ def test_batch_equals_single_runs(Louvain, gen):
         assert b.q_final[g] == res.q_final, g          # same fixed tree: bit-identical
 
 
+def test_batch_persistent_kernels_at_low_thresholds(Louvain, gen):
+    """Tile, block and hub thresholds of 32 / 64 send most rows of the batch
+    to the persistent block-per-item kernels (items pulled from device
+    counters); every graph still gets its own run's result bit for bit."""
+    graphs = mixed_graphs(gen)
+    ref = single_runs(Louvain, graphs, tile_max_degree=32, block_max_degree=64)
+    with Louvain(tile_max_degree=32, block_max_degree=64) as lv:
+        b = lv.run_batch(graphs)
+    for g, (res, part, status, nlev) in enumerate(ref):
+        np.testing.assert_array_equal(b.part(g), part, err_msg=f"graph {g}")
+        assert b.q_final[g] == res.q_final, g
+
+
 def test_batch_matches_oracle(Louvain, oracle, gen):
     graphs = mixed_graphs(gen)
     with Louvain() as lv:
