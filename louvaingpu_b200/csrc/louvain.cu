@@ -1808,9 +1808,18 @@ __global__ void clear_deltas_kernel(int32_t V, Delta* delta, int32_t* cand) {
 }
 
 // ------------------------------------------------------------------ renumber
+// Smallest member of every community.  Lanes of a warp with the same
+// community leave the update to the lowest of them (the smallest index):
+// large communities would otherwise serialise on their counter.
 __global__ void min_member_kernel(int32_t V, const int32_t* comm, int32_t* minidx) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < V; i += (int64_t)gridDim.x * blockDim.x)
-    atomicMin(&minidx[comm[i]], (int32_t)i);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x; b < V; b += stride) {   // whole warps
+    const int64_t i = b + threadIdx.x;
+    const bool ok = i < V;
+    const int32_t c = ok ? comm[i] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    if (ok && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicMin(&minidx[c], (int32_t)i);
+  }
 }
 
 // Head flag of each community's smallest member.
@@ -2743,9 +2752,10 @@ int64_t induce(const LevelGraph& g, const int32_t* part, int32_t C, int32_t** ou
   // automatic: by transposition (measured on one B200, R-MAT scale 25: level 0
   // 1.05 G -> 0.68 G entries 156 -> 106 ms; level 1, where most entries merge,
   // 46 -> 48 ms; the LFR n = 2^20 levels 2.2 -> 1.9 and 1.7 -> 1.5 ms)
+  // (a sort-free method that lacks arena room declines, and the next one is tried)
   const bool by_tx = mode == kCoarsenTransposed || mode == kCoarsenAuto;
-  if (mode != kCoarsenSort && (by_tx ? induce_transposed(g, part, C, osrc, odst, ow, &cnt, next, a, s)
-                                     : induce_sorted(g, part, C, osrc, odst, ow, &cnt, next, a, s))) {
+  if ((by_tx && induce_transposed(g, part, C, osrc, odst, ow, &cnt, next, a, s)) ||
+      (mode != kCoarsenSort && induce_sorted(g, part, C, osrc, odst, ow, &cnt, next, a, s))) {
     *out_src = osrc;
     *out_dst = odst;
     *out_w = ow;
