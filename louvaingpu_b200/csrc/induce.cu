@@ -1192,8 +1192,12 @@ bool induce_transposed(const LevelGraph& g, const int32_t* part, int32_t C, int3
                                                       C, mem, mcomm, mscan, nz);
   LVG_LAUNCH();
   scan_i64(mscan, mscan, V, a, s);
-  if (read_back(mscan + V, s) != E) throw Error(LVG_ERR_CUDA, "coarsening: list rows disagree with the CSR");
-  const int32_t h_nz = read_back(nz, s);
+  int64_t h_rows = 0;
+  int32_t h_nz = 0;
+  LVG_CUDA(cudaMemcpyAsync(&h_rows, mscan + V, sizeof h_rows, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaMemcpyAsync(&h_nz, nz, sizeof h_nz, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));   // both values with one wait
+  if (h_rows != E) throw Error(LVG_ERR_CUDA, "coarsening: list rows disagree with the CSR");
   int32_t* cfirst = a.hi_n<int32_t>(nchunks + 1);
   ic_chunk_first_kernel<<<ic_grid(V), kIcFlat, 0, s>>>(mscan, nz, cfirst, nchunks);
   LVG_LAUNCH();
@@ -1233,8 +1237,13 @@ bool induce_transposed(const LevelGraph& g, const int32_t* part, int32_t C, int3
   tx_count_kernel<<<(unsigned)nchunks, kTxThreads, 0, s>>>(keys, E, Bb, und, tscan);
   LVG_LAUNCH();
   scan_i64(tscan, tscan, nchunks, a, s);
-  const int64_t cnt = (int64_t)((uint64_t)read_back(tscan + nchunks, s) & 0xffffffffull);
-  const bool int_weights = read_back(flags, s) == 0u;
+  int64_t h_tot = 0;
+  uint32_t h_frac = 0;
+  LVG_CUDA(cudaMemcpyAsync(&h_tot, tscan + nchunks, sizeof h_tot, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaMemcpyAsync(&h_frac, flags, sizeof h_frac, cudaMemcpyDeviceToHost, s));
+  LVG_CUDA(cudaStreamSynchronize(s));   // both values with one wait
+  const int64_t cnt = (int64_t)((uint64_t)h_tot & 0xffffffffull);
+  const bool int_weights = h_frac == 0u;
   double* opensum = a.hi_n<double>(nchunks);
   uint32_t* openflag = a.hi_n<uint32_t>(nchunks);
   uint32_t* hl = a.hi_n<uint32_t>((int64_t)C + 1);
