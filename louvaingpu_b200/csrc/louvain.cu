@@ -1808,21 +1808,39 @@ __global__ void clear_deltas_kernel(int32_t V, Delta* delta, int32_t* cand) {
 }
 
 // ------------------------------------------------------------------ renumber
-// Smallest member of every community.  Lanes of a warp with the same
-// community leave the update to the lowest of them (the smallest index):
-// large communities would otherwise serialise on their counter.
-__global__ void min_member_kernel(int32_t V, const int32_t* comm, int32_t* minidx) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x; b < V; b += stride) {   // whole warps
-    const int64_t i = b + threadIdx.x;
-    const bool ok = i < V;
-    const int32_t c = ok ? comm[i] : -1;
-    const unsigned peers = __match_any_sync(0xffffffffu, c);
-    if (ok && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicMin(&minidx[c], (int32_t)i);
+// Smallest member of every community.  A block takes one contiguous range
+// of vertices and keeps the minimum of the communities it meets in a small
+// shared table (open addressing, a few probes; a community that finds no
+// slot updates the global minimum directly), flushed once: the few very
+// large communities would otherwise serialise atomics on their counter.
+constexpr int kMinHotLog = 9;
+constexpr int kMinHot = 1 << kMinHotLog;
+__global__ void __launch_bounds__(kThreads) min_member_kernel(int32_t V, const int32_t* comm, int32_t* minidx) {
+  __shared__ int32_t hk[kMinHot], hv[kMinHot];
+  for (int x = threadIdx.x; x < kMinHot; x += kThreads) { hk[x] = -1; hv[x] = 0x7fffffff; }
+  __syncthreads();
+  const int64_t per = ((int64_t)V + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * per;
+  const int64_t i1 = min((int64_t)V, i0 + per);
+  for (int64_t i = i0 + threadIdx.x; i < i1; i += kThreads) {
+    const int32_t c = comm[i];
+    uint32_t h = hash_c(c, kMinHotLog);
+    bool done = false;
+    for (int p = 0; p < 8 && !done; ++p) {
+      const int32_t prev = atomicCAS(&hk[h], -1, c);
+      if (prev == -1 || prev == c) {
+        atomicMin(&hv[h], (int32_t)i);
+        done = true;
+      }
+      h = (h + 1) & (kMinHot - 1);
+    }
+    if (!done) atomicMin(&minidx[c], (int32_t)i);
   }
+  __syncthreads();
+  for (int x = threadIdx.x; x < kMinHot; x += kThreads)
+    if (hk[x] >= 0) atomicMin(&minidx[hk[x]], hv[x]);
 }
 
-// Head flag of each community's smallest member.
 __global__ void head_flag_kernel(int32_t V, const int32_t* comm, const int32_t* minidx, uint32_t* flag) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < V) flag[i] = minidx[comm[i]] == (int32_t)i ? 1u : 0u;
